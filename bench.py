@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the TREE force path: particle-steps/s at N = 1,048,576.
+
+One step = VVerletNotemp1 -> Force (octree build + upward pass + tree walk)
+-> VVerletNotemp2, the loop body of main.f90:123-131 of hpjeonGIT/TREE, on a
+seeded synthetic ultracold-plasma cloud (isotropic Gaussian of ions at peak
+density 1e15 m^-3 with each electron starting on its ion, T_e = 50 K,
+T_i = 1 mK, dt = 1e-11 s).  The inputs (positions, velocities, trees) are far
+larger than the 126 MB L2 and every step rebuilds the trees from scratch.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the CPU restatement of the reference algorithm
+(pointer octree, serial insertion, recursive OpenMP walks in FP64 with the
+reference pair laws) on the host cores, on a bounded sample of each step.
+With N > 1 GPUs every rank runs an independent replica of the workload (the
+path has no exchange step); value = all particles x steps / max rank time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at N=1,048,576 (force path: build + upward + walk + KDK)"
+UNIT = "particle-steps/s"
+
+# Algorithmic flops per interaction, counted from the kernels' formulas
+# (divisions, square roots and exponentials count as one flop each).
+FLOPS_M2P_REF = 194   # tree.f90:736-779 evaluated literally (FP64 path)
+FLOPS_P2P_REF = 30    # leaf laws of tree.f90 / erf-Kelbg with the x^2>40 shortcut
+FLOPS_M2P_MIXED = 52  # FP32 quadrupole about the charge centre (walk_mixed.cu)
+FLOPS_P2P_MIXED = 24  # FP32 erf-Kelbg pair with compensated accumulation
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1048576)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--mac", choices=["fixed", "learned"], default="fixed")
+    ap.add_argument("--physics", choices=["kelbg", "ref"], default="kelbg")
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--te", type=float, default=50.0)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--audit", type=int, default=16384,
+                    help="targets of the FP64 direct-sum accuracy audit")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-stride", type=int, default=0,
+                    help="walk every k-th target in the CPU sample (0: auto)")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# --------------------------------------------------------------- helpers ----
+def make_workload(n, seed, te):
+    from tree_b200 import cloud
+    return cloud.make_cloud(n, seed=seed, te_k=te, ti_k=1e-3)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return json.load(open(path)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path)).get(kernel)
+    return d
+
+
+def fp_peak_tflops(sm_mhz, fp64):
+    """CUDA-core peak of this GPU at the sampled SM clock: SMs x lanes x 2."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    lanes = 64 if fp64 else 128
+    return sms * lanes * 2 * sm_mhz * 1e6 / 1e12
+
+
+def cpu_sample(c_state, args, stride):
+    """Times the oracle on the same state: full tree build, walk of every
+    stride-th target; returns (particle-steps/s estimate, details)."""
+    import oracle
+    from tree_b200 import units
+    lam = units.kelbg_lambdas(args.te)
+    p = oracle.make_params(theta=args.theta, rs=lam[1], lambdas=lam,
+                           physics=oracle.PHYS_REF)
+    x_el, x_ion = c_state["x_el"], c_state["x_ion"]
+    n = len(x_el) + len(x_ion)
+    t0 = time.perf_counter()
+    r = oracle.force(x_el, x_ion, p, rdf=True, stride=stride)
+    wall = time.perf_counter() - t0
+    st = r["stats"]
+    xe, ve = x_el.copy(), c_state["v_el"].copy()
+    t1 = time.perf_counter()
+    oracle.kdk1(xe, ve, r["f_el"], units.dt_code(1e-11), units.M_ELECTRON_AMU)
+    oracle.kdk2(ve, r["f_el"], units.dt_code(1e-11), units.M_ELECTRON_AMU)
+    t_kdk = (time.perf_counter() - t1) * n / max(len(xe), 1)
+    t_step = st["t_build"] + st["t_walk"] * stride + t_kdk
+    return n / t_step, dict(t_build=st["t_build"], t_walk_sample=st["t_walk"],
+                            t_kdk=t_kdk, stride=stride, wall=wall,
+                            t_step_est=t_step)
+
+
+def auto_stride(n):
+    # about 3-6 s of sampled walking on ~8-100 host cores at N = 1M
+    return max(1, int(round(n / 16384)))
+
+
+# ----------------------------------------------------------- reference arm ----
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    c = make_workload(args.n, args.seed, args.te)
+    rng = np.random.Generator(np.random.Philox(args.seed + 1))
+    # the state a few steps after t = 0: each electron near its ion
+    state = dict(x_el=c.x_ion + rng.standard_normal(c.x_ion.shape) * 0.3,
+                 x_ion=c.x_ion, v_el=c.v_el)
+    stride = args.cpu_stride or auto_stride(args.n)
+    for _ in range(args.warmup):
+        cpu_sample(state, args, stride * 4)
+    vals, det = [], None
+    for _ in range(args.steps):
+        v, det = cpu_sample(state, args, stride)
+        vals.append(v)
+    value = float(np.median(vals))
+    cores = oracle.max_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * args.n / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian UCP cloud)",
+        "config": {"workload": f"UCP cloud N={args.n}, theta={args.theta}, "
+                               f"T_e={args.te} K, reference pair laws, FP64",
+                   "n_particles": args.n, "theta": args.theta},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                         "kind": "port",
+                         "sample": f"full build of both trees + walk of every "
+                                   f"{stride}th target, walk time x{stride}; "
+                                   f"median of {args.steps} samples",
+                         "detail": det},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours ----
+def run_ours(args, rank, world, dist):
+    import torch
+
+    from tree_b200 import api, units
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    torch.cuda.init()
+    prec = api.PREC_MIXED if args.precision == "mixed" else api.PREC_FP64
+    phys = api.PHYS_KELBG if args.physics == "kelbg" else api.PHYS_REF
+    mac = api.MAC_LEARNED if args.mac == "learned" else api.MAC_FIXED
+    cfg = api.Config(theta=args.theta, te=args.te, physics=phys, precision=prec,
+                     mac=mac)
+    dt = units.dt_code(1e-11)
+    c = make_workload(args.n, args.seed + rank, args.te)
+    n_el, n_ion = len(c.x_el), len(c.x_ion)
+    n = n_el + n_ion
+    stream = torch.cuda.Stream()
+    tf = api.TreeForce(n_el, n_ion, cfg)
+    tf.set_stream(stream.cuda_stream)
+    tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
+    tf.step(dt, max(args.warmup, 3))  # warm-up; e-i pairs separate
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    # ---- timed region: device-resident state, K steps in one call ----
+    t_before = tf.timings()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    diag = tf.step(dt, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t_after = tf.timings()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * world * args.steps / (ms / 1e3)
+    walk_ms = (t_after.ms_walk - t_before.ms_walk) / args.steps
+    build_ms = (t_after.ms_build - t_before.ms_build) / args.steps
+    launches = t_after.launches - t_before.launches
+    n_m2p, n_p2p = t_after.n_m2p, t_after.n_p2p
+
+    # ---- end to end: full state host->device, one step, state back ----
+    e2e = None
+    if not args.no_e2e:
+        st = tf.get_state()
+        pin = {k: torch.from_numpy(v).pin_memory() for k, v in st.items()}
+        ptr = {k: v.data_ptr() for k, v in pin.items()}
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        k2 = max(1, min(args.steps, 5))
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(k2):
+            tf.load_state(ptr["x_el"], ptr["v_el"], ptr["f_el"], ptr["x_ion"],
+                          ptr["v_ion"], ptr["f_ion"])
+            tf.step(dt, 1)
+            tf.get_state_ptr(ptr["x_el"], ptr["v_el"], ptr["f_el"],
+                             ptr["x_ion"], ptr["v_ion"], ptr["f_ion"])
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ems = a0.elapsed_time(a1)
+        if dist:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": n * world * k2 / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n,
+               "steps": k2,
+               "path": "tree_gpu_load_state(x,v,f pinned host) + tree_gpu_step(1) "
+                       "+ tree_gpu_get_state(x,v,f pinned host)"}
+
+    # ---- accuracy audit: FP64 direct sum on a seeded subsample ----
+    accuracy = None
+    if args.audit > 0:
+        st = tf.get_state()
+        rng = np.random.default_rng(args.seed + 17)
+        tsel = np.sort(rng.choice(n, min(args.audit, n), replace=False))
+        fd, _ = tf.direct(tsel)
+        fw = np.vstack([st["f_el"], st["f_ion"]])[tsel]
+        err = np.linalg.norm(fw - fd, axis=1) / np.linalg.norm(fd, axis=1)
+        accuracy = {"targets": int(len(tsel)), "rms_rel_err": float(np.sqrt(np.mean(err**2))),
+                    "max_rel_err": float(err.max()),
+                    "judge": "FP64 O(N^2) direct sum on the GPU (tree_gpu_direct), same pair laws"}
+
+    # ---- roofline of the dominant kernel (the walk) ----
+    fp64 = prec == api.PREC_FP64
+    fm2p = FLOPS_M2P_REF if fp64 else FLOPS_M2P_MIXED
+    fp2p = FLOPS_P2P_REF if fp64 else FLOPS_P2P_MIXED
+    flops = n_m2p * fm2p + n_p2p * fp2p
+    achieved = flops / (walk_ms / 1e3) / 1e12 if walk_ms > 0 else 0.0
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    peak = fp_peak_tflops(sm_mhz, fp64)
+    kname = "k_walk64" if fp64 else "k_walk_mixed"
+    roofline = {"bound": "fp64" if fp64 else "fp32", "kernel": kname,
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None,
+                "traffic": profile_traffic(kname),
+                "peak_source": f"CUDA-core {'FP64' if fp64 else 'FP32'} peak = SMs x "
+                               f"{64 if fp64 else 128} lanes x 2 x median SM clock "
+                               f"{sm_mhz:.0f} MHz sampled during the run (the walk is "
+                               "not a contraction; MEASURED_PEAKS.json has no CUDA-core figure)",
+                "flops_per_launch": flops, "walk_ms": walk_ms,
+                "n_m2p": n_m2p, "n_p2p": n_p2p,
+                "flops_per_m2p": fm2p, "flops_per_p2p": fp2p}
+    pk, pk_kind = peaks()
+    # build phase vs HBM: ~250 B per particle algorithmic
+    build_bytes = 250 * n
+    build_roof = {"bound": "hbm", "achieved": build_bytes / (build_ms / 1e3) / 1e9 if build_ms else None,
+                  "peak": pk.get("hbm_gbs"), "unit": "GB/s",
+                  "peak_source": pk_kind, "ms": build_ms,
+                  "bytes_per_particle": 250}
+    if build_roof["achieved"] and build_roof["peak"]:
+        build_roof["frac"] = build_roof["achieved"] / build_roof["peak"]
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        st = tf.get_state()
+        stride = args.cpu_stride or auto_stride(n)
+        v, det = cpu_sample(st, args, stride)
+        cpu = {"value": v, "unit": UNIT, "cores": oracle.max_threads(),
+               "kind": "port",
+               "sample": f"oracle REF1 (reference algorithm, FP64, reference pair laws) "
+                         f"on this state: full build + walk of every {stride}th target, "
+                         f"walk time x{stride}",
+               "detail": det}
+
+    tf.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if fp64 else "f32 (walk) + f64 (positions, Verlet, top cells)",
+        "data": "synthetic (seeded Gaussian UCP cloud, electrons start on ions)",
+        "config": {"workload": f"UCP cloud N={n} per GPU, T_e={args.te} K, T_i=1 mK, "
+                               f"theta={args.theta}, dt=1e-11 s",
+                   "n_particles": n, "theta": args.theta, "te_k": args.te,
+                   "physics": args.physics, "precision": args.precision,
+                   "mac": args.mac,
+                   "l2": "inputs larger than L2 (x,v,f 72 MB + trees >150 MB, rebuilt every step)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk, "e2e": e2e, "gpu_launches": launches,
+        "phases_ms_per_step": {"build": build_ms, "walk": walk_ms,
+                               "other": ms / args.steps - build_ms - walk_ms},
+        "roofline": roofline, "roofline_build": build_roof,
+        "accuracy": accuracy, "cpu_baseline": cpu,
+        "diag": {"epot_e": diag.epot_e, "epot_i": diag.epot_i,
+                 "mv2_el": diag.mv2_el, "mv2_ion": diag.mv2_ion},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

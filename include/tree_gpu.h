@@ -1,0 +1,180 @@
+/* tree_gpu.h -- C ABI of the B200 force path for TREE (hpjeonGIT/TREE).
+ *
+ * The reference computes forces in SUBROUTINE Force(NS, qel, qion, param,
+ * ttime) (main.f90:506-701), an internal procedure of PROGRAM OCTREE_HYBRID
+ * that builds one octree per species (tree.f90:39-100), computes one-level
+ * multipole moments (tree.f90:450-659) and walks both trees for every target
+ * (tree.f90:662-1133).  Velocity Verlet is VVerletNotemp1/2 (vverlet.f90:9-112).
+ * This header is the drop-in boundary that replaces those calls: plain C
+ * types, caller-owned host buffers, library-owned device memory, int status.
+ *
+ * Arrays of positions/velocities/forces are AoS xyz triples of double
+ * (x0,y0,z0,x1,...), the layout of TYPE(GS) (data.f90:54-56) after the
+ * Fortran caller packs TYPE(PT)%xx into a REAL(C_DOUBLE) array.
+ *
+ * Threading: one handle belongs to one host thread and one CUDA stream; calls
+ * on a handle are not reentrant.
+ */
+#ifndef TREE_GPU_H
+#define TREE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (0 = ok) */
+#define TREE_GPU_OK 0
+#define TREE_GPU_ERR_ARG -1        /* bad argument / size */
+#define TREE_GPU_ERR_DEPTH -2      /* two same-species particles share the
+                                      deepest (21-level) cell; the reference
+                                      recurses forever here (tree.f90:128-273) */
+#define TREE_GPU_ERR_NONFINITE -3  /* NaN/Inf position */
+#define TREE_GPU_ERR_CAPACITY -4   /* internal node capacity exceeded */
+#define TREE_GPU_ERR_CUDA -5       /* CUDA runtime error (see last_error) */
+#define TREE_GPU_ERR_WALK -6       /* walk guard tripped (corrupt tree) */
+#define TREE_GPU_ERR_STATE -7      /* call order (e.g. step before set_state) */
+
+/* physics: which pair laws the leaves use */
+#define TREE_GPU_PHYS_REF 0    /* reference laws: Coulomb e-e/i-i with the
+                                  r^2 > 0.01 um^2 cutoff (tree.f90:806,1115),
+                                  exp-screened e-i "Kelbg" with length rs
+                                  (tree.f90:905-913) */
+#define TREE_GPU_PHYS_KELBG 1  /* erf-Kelbg for every pair,
+                                  lambda_ij = hbar/sqrt(2 mu_ij k T_e) */
+
+/* precision / walk form */
+#define TREE_GPU_PREC_FP64 0   /* per-target walk in FP64, the reference's
+                                  visiting order (parity path) */
+#define TREE_GPU_PREC_MIXED 1  /* warp-group walk, FP32 cell-relative
+                                  arithmetic, compensated sums */
+
+/* multipole acceptance criterion */
+#define TREE_GPU_MAC_FIXED 0   /* s/theta + dx < r (tree.f90:743) */
+#define TREE_GPU_MAC_LEARNED 1 /* learned acceptance, fixed-theta fallback */
+
+#define TREE_GPU_RDF_BINS 10001 /* Ndist + 1 (data.f90:38) */
+
+typedef struct tree_gpu_params {
+  double theta;    /* param%sd_ratio (opening criterion) */
+  double rs;       /* param%rs, reference e-i screening length (um) */
+  double te;       /* electron temperature for lambda_ij (K) */
+  double xm_el;    /* param%xm(1), amu */
+  double xm_ion;   /* param%xm(2), amu */
+  double dx_ei;    /* NS%dx_ei, RDF bin width (um) */
+  double dx_ii;    /* NS%dx_ii */
+  int32_t physics;   /* TREE_GPU_PHYS_* */
+  int32_t precision; /* TREE_GPU_PREC_* */
+  int32_t mac;       /* TREE_GPU_MAC_* */
+  int32_t group;     /* targets per group in the mixed walk (0 = default 32) */
+} tree_gpu_params;
+
+typedef struct tree_gpu_diag {
+  double epot_e;   /* sys%Epot_e: ee + ie + ei potential energy (eV) */
+  double epot_i;   /* sys%Epot_i: ii */
+  double mv2_el;   /* sys%mv2el = sum m v^2 (vverlet.f90:86-88) */
+  double mv2_ion;  /* sys%mv2ion */
+  double rad_el;   /* sys%Te_rad = sum m (x.v)^2/|x|^2 (vverlet.f90:89-91) */
+  double rad_ion;  /* sys%Ti_rad */
+  int64_t steps_done;
+} tree_gpu_diag;
+
+typedef struct tree_gpu_timing {
+  double ms_build;   /* bbox + keys + sort + topology + upward pass */
+  double ms_walk;    /* tree walk */
+  double ms_kdk;     /* kick-drift-kick */
+  double ms_total;
+  int64_t n_m2p;     /* accepted cells (far-field evaluations), last call */
+  int64_t n_p2p;     /* leaf pair evaluations, last call */
+  int64_t n_nodes;   /* nodes of both trees, last build */
+  int64_t calls;
+  int64_t launches;  /* kernels this library launched (cumulative) */
+} tree_gpu_timing;
+
+typedef struct tree_gpu_handle tree_gpu_handle;
+
+/* Creates a handle for n_el electrons and n_ion ions on the current CUDA
+ * device.  Replaces the set-up that Init (main.f90:196-426) and the automatic
+ * arrays of Force (main.f90:521-522) did.  */
+int tree_gpu_create(const tree_gpu_params* params, int64_t n_el,
+                    int64_t n_ion, tree_gpu_handle** out);
+
+/* Changes the parameters (theta, physics, precision, ...) of a handle. */
+int tree_gpu_set_params(tree_gpu_handle* h, const tree_gpu_params* params);
+
+/* Force-only drop-in for CALL Force(NS, qel, qion, param, ttime)
+ * (main.f90:130, 777, 821).  In: x_el (3*n_el), x_ion (3*n_ion).  Out:
+ * f_el, f_ion overwritten (the local part zeroes them, tree.f90:675-680);
+ * *epot_e, *epot_i overwritten (sys%Epot_e/_i); rdf_ei, rdf_ii (10001 bins
+ * each, may be NULL) are ACCUMULATED like NS%RDF_ei/_ii.  Host buffers; the
+ * copies happen inside the call, which returns after the stream synchronises. */
+int tree_gpu_force(tree_gpu_handle* h, const double* x_el, const double* x_ion,
+                   double* f_el, double* f_ion, double* epot_e,
+                   double* epot_i, int64_t* rdf_ei, int64_t* rdf_ii);
+
+/* Loads positions and velocities (host) into the device-resident state and
+ * computes the initial forces (what Vinit/Vinit_REST do, main.f90:777/821). */
+int tree_gpu_set_state(tree_gpu_handle* h, const double* x_el,
+                       const double* v_el, const double* x_ion,
+                       const double* v_ion);
+
+/* Loads a full particle state (positions, velocities AND forces, e.g. from a
+ * restart or from the caller's own previous step) without computing forces;
+ * the next tree_gpu_step starts from it.  Counterpart of the state TYPE(PT)
+ * carries between steps (data.f90:47-50). */
+int tree_gpu_load_state(tree_gpu_handle* h, const double* x_el,
+                        const double* v_el, const double* f_el,
+                        const double* x_ion, const double* v_ion,
+                        const double* f_ion);
+
+/* Step drop-in for the loop body main.f90:125-131 + VVerletNotemp2: nsteps x
+ * (VVerletNotemp1 -> Force -> VVerletNotemp2) on the device with no host
+ * traffic.  Kinetic sums are sampled on the last step; `out` may be NULL. */
+int tree_gpu_step(tree_gpu_handle* h, double dt, int32_t nsteps,
+                  tree_gpu_diag* out);
+
+/* Copies the device-resident state to host buffers (any may be NULL), for
+ * Restart/RDF/TEMPORAL steps (print.f90:5-109, sample.f90). */
+int tree_gpu_get_state(tree_gpu_handle* h, double* x_el, double* v_el,
+                       double* f_el, double* x_ion, double* v_ion,
+                       double* f_ion);
+
+/* FP64 O(N^2) direct sum (the accuracy judge): forces on the listed targets
+ * from every particle at the current device positions, with the handle's
+ * pair laws and no tree (the theta -> 0 limit of Search_Tree_*,
+ * tree.f90:721-1133).  targets: global indices (electrons 0..n_el-1, ions
+ * n_el..n_el+n_ion-1).  Out (host): f (3*nt), epot (nt; 0.5*sum of V per
+ * target).  Allocates its device scratch per call. */
+int tree_gpu_direct(tree_gpu_handle* h, const int64_t* targets, int64_t nt,
+                    double* f, double* epot);
+
+/* Debug/parity: copies one species tree (0 electrons, 1 ions) of the last
+ * build in pre-order (children 1..8, the reference's visiting order).
+ * Per node: centre[3] (charge centre, or the particle for leaves), moments[10]
+ * (qeff, D[3], Q[3], QQ[3]), rcrit (s/theta + dx; -1 for leaves), level,
+ * skip (pre-order index past the subtree, tree-local), pt (particle index
+ * for leaves, -1 for twigs).  Pass NULL buffers to query *n_nodes only. */
+int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
+                       double* centre, double* moments, double* rcrit,
+                       int32_t* level, int64_t* skip, int64_t* pt,
+                       int64_t* n_nodes);
+
+/* Runs all later work of the handle on `stream` (a cudaStream_t; NULL
+ * restores the handle's own stream).  No counterpart in the reference (its
+ * work is on host threads); lets a caller order the force path with its own
+ * device work and time it with events on the same stream. */
+int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
+
+int tree_gpu_timings(tree_gpu_handle* h, tree_gpu_timing* out);
+const char* tree_gpu_last_error(tree_gpu_handle* h);
+int tree_gpu_destroy(tree_gpu_handle* h);
+
+/* Library build identifier (sm_100a + git describe at build time). */
+const char* tree_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TREE_GPU_H */

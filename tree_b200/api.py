@@ -1,0 +1,282 @@
+"""Python mirror of the force boundary (ctypes over libtree_b200.so).
+
+The reference's interface is ``SUBROUTINE Force(NS, qel, qion, param, ttime)``
+(main.f90:506-701 of hpjeonGIT/TREE) plus the velocity-Verlet calls of its step
+loop (main.f90:125-131, vverlet.f90:9-112).  ``TreeForce.force`` mirrors Force:
+positions in, forces and potential energies out, RDF histograms accumulated.
+``TreeForce.set_state / step / get_state`` mirror the step loop with the state
+resident on the GPU.  Every call goes through the C ABI of include/tree_gpu.h;
+there is no CPU fallback: a missing library raises ImportError.
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import units
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtree_b200.so")
+
+OK = 0
+ERR = {-1: "ARG", -2: "DEPTH", -3: "NONFINITE", -4: "CAPACITY", -5: "CUDA",
+       -6: "WALK", -7: "STATE"}
+PHYS_REF, PHYS_KELBG = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+MAC_FIXED, MAC_LEARNED = 0, 1
+RDF_BINS = 10001
+
+# Every symbol include/tree_gpu.h declares.
+EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
+           "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step", "tree_gpu_get_state",
+           "tree_gpu_direct", "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_timings",
+           "tree_gpu_last_error",
+           "tree_gpu_destroy", "tree_gpu_version")
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("theta", ctypes.c_double), ("rs", ctypes.c_double),
+                ("te", ctypes.c_double), ("xm_el", ctypes.c_double),
+                ("xm_ion", ctypes.c_double), ("dx_ei", ctypes.c_double),
+                ("dx_ii", ctypes.c_double), ("physics", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("mac", ctypes.c_int32),
+                ("group", ctypes.c_int32)]
+
+
+class Diag(ctypes.Structure):
+    _fields_ = [("epot_e", ctypes.c_double), ("epot_i", ctypes.c_double),
+                ("mv2_el", ctypes.c_double), ("mv2_ion", ctypes.c_double),
+                ("rad_el", ctypes.c_double), ("rad_ion", ctypes.c_double),
+                ("steps_done", ctypes.c_int64)]
+
+
+class Timing(ctypes.Structure):
+    _fields_ = [("ms_build", ctypes.c_double), ("ms_walk", ctypes.c_double),
+                ("ms_kdk", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("n_m2p", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
+                ("n_nodes", ctypes.c_int64), ("calls", ctypes.c_int64),
+                ("launches", ctypes.c_int64)]
+
+
+class TreeGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"tree_gpu error {code} ({ERR.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libtree_b200.so; raises ImportError when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} not built: run `python -m tree_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, dp, lp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)
+    L.tree_gpu_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int64,
+                                  ctypes.c_int64, ctypes.POINTER(vp)]
+    L.tree_gpu_set_params.argtypes = [vp, ctypes.POINTER(Params)]
+    L.tree_gpu_force.argtypes = [vp, dp, dp, dp, dp, dp, dp, lp, lp]
+    L.tree_gpu_set_state.argtypes = [vp, dp, dp, dp, dp]
+    L.tree_gpu_load_state.argtypes = [vp, dp, dp, dp, dp, dp, dp]
+    L.tree_gpu_step.argtypes = [vp, ctypes.c_double, ctypes.c_int32,
+                                ctypes.POINTER(Diag)]
+    L.tree_gpu_get_state.argtypes = [vp, dp, dp, dp, dp, dp, dp]
+    L.tree_gpu_tree_dump.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, dp,
+                                     dp, dp, ctypes.POINTER(ctypes.c_int32),
+                                     lp, lp, lp]
+    L.tree_gpu_direct.argtypes = [vp, lp, ctypes.c_int64, dp, dp]
+    L.tree_gpu_set_stream.argtypes = [vp, vp]
+    L.tree_gpu_timings.argtypes = [vp, ctypes.POINTER(Timing)]
+    L.tree_gpu_last_error.argtypes = [vp]
+    L.tree_gpu_last_error.restype = ctypes.c_char_p
+    L.tree_gpu_destroy.argtypes = [vp]
+    L.tree_gpu_version.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int
+    _lib = L
+    return L
+
+
+def _dp(a):
+    if a is None:
+        return None
+    if isinstance(a, int):  # raw address (e.g. pinned host memory)
+        return ctypes.cast(a, ctypes.POINTER(ctypes.c_double))
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c3(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, 3))
+
+
+@dataclass
+class Config:
+    """Arguments of the force path (the fields of TYPE(PM)/TYPE(NM) the walk
+    reads).  rs defaults to lambda_ei, the recommended REF screening length."""
+    theta: float = 0.5
+    te: float = 50.0
+    rs: float | None = None
+    xm_el: float = units.M_ELECTRON_AMU
+    xm_ion: float = units.M_ION_AMU
+    dx_ei: float = 0.01
+    dx_ii: float = 0.1
+    physics: int = PHYS_REF
+    precision: int = PREC_FP64
+    mac: int = MAC_FIXED
+    group: int = 0
+
+    def to_c(self) -> Params:
+        rs = self.rs if self.rs is not None else units.kelbg_lambdas(
+            self.te, self.xm_el, self.xm_ion)[1]
+        return Params(self.theta, rs, self.te, self.xm_el, self.xm_ion,
+                      self.dx_ei, self.dx_ii, self.physics, self.precision,
+                      self.mac, self.group)
+
+
+class TreeForce:
+    """One device-resident force path for n_el electrons and n_ion ions."""
+
+    def __init__(self, n_el: int, n_ion: int, config: Config | None = None):
+        self.lib = load_library()
+        self.n_el, self.n_ion = int(n_el), int(n_ion)
+        self.config = config or Config()
+        self._p = self.config.to_c()
+        h = ctypes.c_void_p()
+        rc = self.lib.tree_gpu_create(ctypes.byref(self._p), self.n_el,
+                                      self.n_ion, ctypes.byref(h))
+        if rc != OK:
+            raise TreeGpuError(rc, "tree_gpu_create failed")
+        self.h = h
+
+    def _check(self, rc):
+        if rc != OK:
+            msg = self.lib.tree_gpu_last_error(self.h)
+            raise TreeGpuError(rc, msg.decode() if msg else "")
+
+    def set_config(self, config: Config):
+        self.config = config
+        self._p = config.to_c()
+        self._check(self.lib.tree_gpu_set_params(self.h, ctypes.byref(self._p)))
+
+    def force(self, x_el, x_ion, rdf_ei=None, rdf_ii=None):
+        """Mirror of Force: returns (f_el, f_ion, epot_e, epot_i); rdf_* are
+        int64 arrays of 10001 bins that are accumulated in place."""
+        x_el, x_ion = _c3(x_el), _c3(x_ion)
+        assert len(x_el) == self.n_el and len(x_ion) == self.n_ion
+        f_el = np.empty_like(x_el)
+        f_ion = np.empty_like(x_ion)
+        ee = ctypes.c_double()
+        ei = ctypes.c_double()
+        lp = ctypes.POINTER(ctypes.c_int64)
+        for r in (rdf_ei, rdf_ii):
+            if r is not None:
+                assert r.dtype == np.int64 and r.size == RDF_BINS and r.flags.c_contiguous
+        self._check(self.lib.tree_gpu_force(
+            self.h, _dp(x_el), _dp(x_ion), _dp(f_el), _dp(f_ion),
+            ctypes.byref(ee), ctypes.byref(ei),
+            rdf_ei.ctypes.data_as(lp) if rdf_ei is not None else None,
+            rdf_ii.ctypes.data_as(lp) if rdf_ii is not None else None))
+        return f_el, f_ion, ee.value, ei.value
+
+    def set_state(self, x_el, v_el, x_ion, v_ion):
+        x_el, v_el, x_ion, v_ion = map(_c3, (x_el, v_el, x_ion, v_ion))
+        self._check(self.lib.tree_gpu_set_state(self.h, _dp(x_el), _dp(v_el),
+                                                _dp(x_ion), _dp(v_ion)))
+
+    def set_state_ptr(self, x_el, v_el, x_ion, v_ion):
+        """set_state from raw host addresses (pinned buffers)."""
+        self._check(self.lib.tree_gpu_set_state(self.h, _dp(x_el), _dp(v_el),
+                                                _dp(x_ion), _dp(v_ion)))
+
+    def load_state(self, x_el, v_el, f_el, x_ion, v_ion, f_ion):
+        """Full state in (no force evaluation); arrays or raw host addresses."""
+        conv = (lambda a: a) if isinstance(x_el, int) else _c3
+        args = [conv(a) for a in (x_el, v_el, f_el, x_ion, v_ion, f_ion)]
+        self._check(self.lib.tree_gpu_load_state(self.h, *[_dp(a) for a in args]))
+
+    def step(self, dt: float, nsteps: int = 1) -> Diag:
+        d = Diag()
+        self._check(self.lib.tree_gpu_step(self.h, dt, nsteps, ctypes.byref(d)))
+        return d
+
+    def get_state(self):
+        x_el = np.empty((self.n_el, 3))
+        v_el = np.empty_like(x_el)
+        f_el = np.empty_like(x_el)
+        x_ion = np.empty((self.n_ion, 3))
+        v_ion = np.empty_like(x_ion)
+        f_ion = np.empty_like(x_ion)
+        self._check(self.lib.tree_gpu_get_state(
+            self.h, _dp(x_el), _dp(v_el), _dp(f_el), _dp(x_ion), _dp(v_ion),
+            _dp(f_ion)))
+        return dict(x_el=x_el, v_el=v_el, f_el=f_el, x_ion=x_ion,
+                    v_ion=v_ion, f_ion=f_ion)
+
+    def get_state_ptr(self, x_el, v_el, f_el, x_ion, v_ion, f_ion):
+        self._check(self.lib.tree_gpu_get_state(
+            self.h, _dp(x_el), _dp(v_el), _dp(f_el), _dp(x_ion), _dp(v_ion),
+            _dp(f_ion)))
+
+    def direct(self, targets):
+        """FP64 direct sum at the current device positions for global target
+        indices; returns (f (nt,3), epot (nt,) = 0.5 sum V)."""
+        t = np.ascontiguousarray(np.asarray(targets, dtype=np.int64))
+        f = np.empty((len(t), 3))
+        e = np.empty(len(t))
+        self._check(self.lib.tree_gpu_direct(
+            self.h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), len(t),
+            _dp(f), _dp(e)))
+        return f, e
+
+    def tree_dump(self, species: int):
+        n = ctypes.c_int64()
+        self._check(self.lib.tree_gpu_tree_dump(self.h, species, 0, None, None,
+                                                None, None, None, None,
+                                                ctypes.byref(n)))
+        m = n.value
+        centre = np.zeros((m, 3))
+        mom = np.zeros((m, 10))
+        rcrit = np.zeros(m)
+        level = np.zeros(m, np.int32)
+        skip = np.zeros(m, np.int64)
+        pt = np.zeros(m, np.int64)
+        lp = ctypes.POINTER(ctypes.c_int64)
+        self._check(self.lib.tree_gpu_tree_dump(
+            self.h, species, m, _dp(centre), _dp(mom), _dp(rcrit),
+            level.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            skip.ctypes.data_as(lp), pt.ctypes.data_as(lp), ctypes.byref(n)))
+        return dict(centre=centre, moments=mom, rcrit=rcrit, level=level,
+                    skip=skip, pt=pt)
+
+    def set_stream(self, stream_handle: int | None):
+        """Enqueue later work on a caller's cudaStream_t (an integer handle,
+        e.g. torch.cuda.current_stream().cuda_stream); None restores the
+        handle's own stream."""
+        self._check(self.lib.tree_gpu_set_stream(self.h, stream_handle or None))
+
+    def timings(self) -> Timing:
+        t = Timing()
+        self._check(self.lib.tree_gpu_timings(self.h, ctypes.byref(t)))
+        return t
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tree_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

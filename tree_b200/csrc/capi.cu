@@ -1,0 +1,641 @@
+// capi.cu -- the extern "C" boundary (include/tree_gpu.h).
+//
+// Replaces SUBROUTINE Force (main.f90:506-701) and the VVerlet calls of the
+// step loop (main.f90:125-131) for one GPU: one device-resident tree per
+// species instead of the 8-rank octant decomposition and ghost-tree exchange.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tree_gpu.h"
+#include "build.h"
+#include "direct.h"
+#include "internal.cuh"
+#include "kdk.h"
+#include "walk.h"
+#include "walk_mixed.h"
+
+#ifndef TREE_GPU_VERSION_STR
+#define TREE_GPU_VERSION_STR "tree_b200 sm_100a"
+#endif
+
+namespace {
+
+constexpr double kHbar = 1.054571817e-34;  // J s
+constexpr double kAmu = 1.66053906660e-27;  // kg
+constexpr double kKbSi = 1.380649e-23;      // J/K
+
+double kelbg_lambda_um(double mu_amu, double te) {
+  return kHbar / std::sqrt(2.0 * mu_amu * kAmu * kKbSi * te) * 1e6;
+}
+
+struct EventSet {
+  cudaEvent_t e[4];
+};
+
+}  // namespace
+
+struct tree_gpu_handle {
+  tree_gpu_params prm{};
+  int64_t n_el = 0, n_ion = 0;
+  int n = 0;
+  int device = 0;
+  cudaStream_t st = nullptr;      // stream all work is enqueued on
+  cudaStream_t own_st = nullptr;  // the handle's own stream
+  double* x = nullptr;
+  double* v = nullptr;
+  double* f = nullptr;
+  double2* epot_part = nullptr;
+  tg::BuildBuffers b{};
+  tg::MixedBuffers mb{};
+  uint32_t* rdf = nullptr;
+  unsigned long long* counters = nullptr;
+  double* partial = nullptr;
+  double* diag = nullptr;  // [0..3] epot, [4..7] kinetic sums
+  int32_t* h_pinned = nullptr;  // small pinned readback area
+  bool has_state = false;
+  double lam[3] = {1, 1, 1};
+  tree_gpu_timing timing{};
+  std::vector<EventSet> events;
+  std::string last_error;
+};
+
+namespace {
+
+int fail(tree_gpu_handle* h, int code, const std::string& msg) {
+  if (h) h->last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                            \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return fail(h, TREE_GPU_ERR_CUDA,                                     \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+int check_params(const tree_gpu_params* p) {
+  if (!p) return TREE_GPU_ERR_ARG;
+  if (!(p->theta > 0.0) || !std::isfinite(p->theta)) return TREE_GPU_ERR_ARG;
+  if (p->physics != TREE_GPU_PHYS_REF && p->physics != TREE_GPU_PHYS_KELBG)
+    return TREE_GPU_ERR_ARG;
+  if (p->precision != TREE_GPU_PREC_FP64 && p->precision != TREE_GPU_PREC_MIXED)
+    return TREE_GPU_ERR_ARG;
+  if (p->mac != TREE_GPU_MAC_FIXED && p->mac != TREE_GPU_MAC_LEARNED)
+    return TREE_GPU_ERR_ARG;
+  if (p->physics == TREE_GPU_PHYS_REF && !(p->rs > 0.0)) return TREE_GPU_ERR_ARG;
+  if (p->physics == TREE_GPU_PHYS_KELBG &&
+      (!(p->te > 0.0) || !(p->xm_el > 0.0) || !(p->xm_ion > 0.0)))
+    return TREE_GPU_ERR_ARG;
+  if (!(p->dx_ei > 0.0) || !(p->dx_ii > 0.0)) return TREE_GPU_ERR_ARG;
+  return TREE_GPU_OK;
+}
+
+void set_lambdas(tree_gpu_handle* h) {
+  const tree_gpu_params& p = h->prm;
+  if (p.te > 0.0 && p.xm_el > 0.0 && p.xm_ion > 0.0) {
+    h->lam[0] = kelbg_lambda_um(p.xm_el / 2.0, p.te);
+    h->lam[1] = kelbg_lambda_um(p.xm_el * p.xm_ion / (p.xm_el + p.xm_ion), p.te);
+    h->lam[2] = kelbg_lambda_um(p.xm_ion / 2.0, p.te);
+  }
+}
+
+template <class T>
+int dalloc(tree_gpu_handle* h, T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc((void**)p, count * sizeof(T)));
+  return 0;
+}
+
+int alloc_nodes(tree_gpu_handle* h, int cap) {
+  tg::BuildBuffers& b = h->b;
+  b.cap = cap;
+  int rc = 0;
+  if ((rc = dalloc(h, &b.node_c, cap))) return rc;
+  if ((rc = dalloc(h, &b.node_m, 5 * (size_t)cap))) return rc;
+  if ((rc = dalloc(h, &b.node_skip, cap))) return rc;
+  if ((rc = dalloc(h, &b.node_pt, cap))) return rc;
+  if ((rc = dalloc(h, &b.node_parent, cap))) return rc;
+  if ((rc = dalloc(h, &b.node_nchild, cap))) return rc;
+  if ((rc = dalloc(h, &b.node_done, cap))) return rc;
+  if ((rc = dalloc(h, &b.node_level, cap))) return rc;
+  return tg::mixed_alloc_nodes(h->mb, cap) ? fail(h, TREE_GPU_ERR_CUDA, "mixed node alloc") : 0;
+}
+
+int alloc_all(tree_gpu_handle* h) {
+  int n = h->n;
+  tg::BuildBuffers& b = h->b;
+  int rc = 0;
+  if ((rc = dalloc(h, &h->x, 3 * (size_t)n))) return rc;
+  if ((rc = dalloc(h, &h->v, 3 * (size_t)n))) return rc;
+  if ((rc = dalloc(h, &h->f, 3 * (size_t)n))) return rc;
+  if ((rc = dalloc(h, &h->epot_part, n))) return rc;
+  if ((rc = dalloc(h, &b.keys, n))) return rc;
+  if ((rc = dalloc(h, &b.keys_alt, n))) return rc;
+  if ((rc = dalloc(h, &b.vals, n))) return rc;
+  if ((rc = dalloc(h, &b.vals_alt, n))) return rc;
+  if ((rc = dalloc(h, &b.L, n))) return rc;
+  if ((rc = dalloc(h, &b.cnt, n))) return rc;
+  if ((rc = dalloc(h, &b.off, (size_t)n + 1))) return rc;
+  int rb = tg::radix_blocks(n);
+  if ((rc = dalloc(h, &b.sort_hist, 256 * (size_t)rb))) return rc;
+  int sp = tg::scan_partials_needed(256 * rb > n + 1 ? 256 * rb : n + 1);
+  if ((rc = dalloc(h, &b.scan_partial, (size_t)sp + 1))) return rc;
+  if ((rc = dalloc(h, &b.bbox, 12))) return rc;
+  if ((rc = dalloc(h, &b.geom, 2))) return rc;
+  if ((rc = dalloc(h, &b.bounds, 4))) return rc;
+  if ((rc = dalloc(h, &b.err, 1))) return rc;
+  if ((rc = dalloc(h, &h->rdf, 2 * (size_t)tg::kRdfBins))) return rc;
+  if ((rc = dalloc(h, &h->counters, 2))) return rc;
+  if ((rc = dalloc(h, &h->partial, 4 * (size_t)tg::kdk_partials_needed(n) + 4)))
+    return rc;
+  if ((rc = dalloc(h, &h->diag, 8))) return rc;
+  CK(cudaMemsetAsync(h->diag, 0, 8 * sizeof(double), h->st));
+  if (tg::mixed_alloc_particles(h->mb, n))
+    return fail(h, TREE_GPU_ERR_CUDA, "mixed particle alloc");
+  int cap = 3 * n + 64;
+  return alloc_nodes(h, cap);
+}
+
+void free_all(tree_gpu_handle* h) {
+  tg::BuildBuffers& b = h->b;
+  void* ptrs[] = {h->x, h->v, h->f, h->epot_part, b.keys, b.keys_alt, b.vals,
+                  b.vals_alt, b.L, b.cnt, b.off, b.sort_hist, b.scan_partial,
+                  b.bbox, b.geom, b.bounds, b.err, b.node_c, b.node_m,
+                  b.node_skip, b.node_pt, b.node_parent, b.node_nchild,
+                  b.node_done, b.node_level, h->rdf, h->counters, h->partial,
+                  h->diag};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  tg::mixed_free(h->mb);
+}
+
+tg::TreeView tree_view(tree_gpu_handle* h) {
+  tg::TreeView tv;
+  tv.node_c = h->b.node_c;
+  tv.node_m = h->b.node_m;
+  tv.node_skip = h->b.node_skip;
+  tv.node_pt = h->b.node_pt;
+  tv.tree_bounds = h->b.bounds;
+  return tv;
+}
+
+tg::WalkParams walk_params(tree_gpu_handle* h) {
+  tg::WalkParams wp;
+  wp.physics = h->prm.physics;
+  wp.theta = h->prm.theta;
+  wp.rs = h->prm.rs;
+  wp.lam_ee = h->lam[0];
+  wp.lam_ei = h->lam[1];
+  wp.lam_ii = h->lam[2];
+  wp.dx_ei = h->prm.dx_ei;
+  wp.dx_ii = h->prm.dx_ii;
+  return wp;
+}
+
+EventSet& events_for(tree_gpu_handle* h, size_t i) {
+  while (h->events.size() <= i) {
+    EventSet es;
+    for (int k = 0; k < 4; ++k) cudaEventCreate(&es.e[k]);
+    h->events.push_back(es);
+  }
+  return h->events[i];
+}
+
+// Enqueues build + walk + potential-energy sum on the handle's stream.
+void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
+  cudaStream_t st = h->st;
+  if (ev) cudaEventRecord(ev->e[0], st);
+  h->timing.launches +=
+      tg::build_trees(h->b, h->x, h->n, (int)h->n_el, h->prm.theta, st);
+  if (ev) cudaEventRecord(ev->e[1], st);
+  cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), st);
+  if (with_rdf)
+    cudaMemsetAsync(h->rdf, 0, 2 * sizeof(uint32_t) * tg::kRdfBins, st);
+  tg::TreeView tv = tree_view(h);
+  tg::WalkParams wp = walk_params(h);
+  if (h->prm.precision == TREE_GPU_PREC_FP64) {
+    tg::walk64(h->x, h->n, (int)h->n_el, h->b.vals, tv, wp, h->f,
+               h->epot_part, with_rdf ? h->rdf : nullptr, h->counters,
+               h->b.err, st);
+  } else {
+    tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp,
+                   h->prm.mac, h->prm.group, h->f, h->epot_part,
+                   with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
+  }
+  if (ev) cudaEventRecord(ev->e[2], st);
+  h->timing.launches += (h->n > 0 ? 1 : 0) + 2;  // walk + epot partial/sum
+  tg::epot_sum(h->epot_part, h->n, h->partial, h->diag, st);
+}
+
+// Reads the error word and node counts after a synchronised call.
+int check_device_status(tree_gpu_handle* h, bool* grow) {
+  *grow = false;
+  int32_t* hp = h->h_pinned;
+  CK(cudaMemcpyAsync(hp, h->b.err, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(hp + 1, h->b.bounds, 4 * sizeof(int32_t),
+                     cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  int32_t err = hp[0];
+  h->timing.n_nodes = hp[1 + 3];
+  if (err & tg::kErrNonFinite)
+    return fail(h, TREE_GPU_ERR_NONFINITE, "non-finite particle position");
+  if (err & tg::kErrDepth)
+    return fail(h, TREE_GPU_ERR_DEPTH,
+                "two same-species particles share a 21-level cell");
+  if (err & tg::kErrCapacity) {
+    *grow = true;
+    return TREE_GPU_OK;
+  }
+  if (err & tg::kErrWalk) return fail(h, TREE_GPU_ERR_WALK, "walk guard tripped");
+  return TREE_GPU_OK;
+}
+
+int grow_nodes(tree_gpu_handle* h) {
+  int need = h->h_pinned[1 + 3];
+  if (need <= h->b.cap) need = h->b.cap;
+  int64_t cap = (int64_t)need + need / 4 + 64;
+  if (cap > 0x7fffffff) return fail(h, TREE_GPU_ERR_CAPACITY, "node count overflow");
+  CK(cudaStreamSynchronize(h->st));
+  return alloc_nodes(h, (int)cap);
+}
+
+void read_counters(tree_gpu_handle* h) {
+  unsigned long long c[2] = {0, 0};
+  cudaMemcpy(c, h->counters, sizeof(c), cudaMemcpyDeviceToHost);
+  h->timing.n_m2p = (int64_t)c[0];
+  h->timing.n_p2p = (int64_t)c[1];
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Computes forces of the current device positions, growing the node arrays
+// when the tree did not fit.
+int force_device(tree_gpu_handle* h, bool with_rdf) {
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    EventSet& ev = events_for(h, 0);
+    enqueue_force(h, with_rdf, &ev);
+    CK(cudaGetLastError());
+    bool grow = false;
+    int rc = check_device_status(h, &grow);
+    if (rc) return rc;
+    if (!grow) {
+      h->timing.ms_build += elapsed(ev.e[0], ev.e[1]);
+      h->timing.ms_walk += elapsed(ev.e[1], ev.e[2]);
+      h->timing.ms_total += elapsed(ev.e[0], ev.e[2]);
+      h->timing.calls += 1;
+      read_counters(h);
+      return TREE_GPU_OK;
+    }
+    if ((rc = grow_nodes(h))) return rc;
+  }
+  return fail(h, TREE_GPU_ERR_CAPACITY, "node capacity growth did not converge");
+}
+
+}  // namespace
+
+extern "C" {
+
+int tree_gpu_create(const tree_gpu_params* params, int64_t n_el, int64_t n_ion,
+                    tree_gpu_handle** out) {
+  if (!out) return TREE_GPU_ERR_ARG;
+  *out = nullptr;
+  if (check_params(params) != TREE_GPU_OK) return TREE_GPU_ERR_ARG;
+  if (n_el < 0 || n_ion < 0 || n_el + n_ion > (int64_t)0x7fffffff / 4)
+    return TREE_GPU_ERR_ARG;
+  tree_gpu_handle* h = new (std::nothrow) tree_gpu_handle();
+  if (!h) return TREE_GPU_ERR_ARG;
+  h->prm = *params;
+  h->n_el = n_el;
+  h->n_ion = n_ion;
+  h->n = (int)(n_el + n_ion);
+  set_lambdas(h);
+  int rc = TREE_GPU_OK;
+  do {
+    if (cudaGetDevice(&h->device) != cudaSuccess) {
+      rc = fail(h, TREE_GPU_ERR_CUDA, "no CUDA device");
+      break;
+    }
+    if (cudaStreamCreateWithFlags(&h->own_st, cudaStreamNonBlocking) != cudaSuccess) {
+      rc = fail(h, TREE_GPU_ERR_CUDA, "stream create failed");
+      break;
+    }
+    h->st = h->own_st;
+    if (cudaMallocHost((void**)&h->h_pinned, 64) != cudaSuccess) {
+      rc = fail(h, TREE_GPU_ERR_CUDA, "pinned alloc failed");
+      break;
+    }
+    rc = alloc_all(h);
+  } while (0);
+  if (rc != TREE_GPU_OK) {
+    tree_gpu_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_set_params(tree_gpu_handle* h, const tree_gpu_params* params) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (check_params(params) != TREE_GPU_OK)
+    return fail(h, TREE_GPU_ERR_ARG, "invalid parameters");
+  h->prm = *params;
+  set_lambdas(h);
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_force(tree_gpu_handle* h, const double* x_el, const double* x_ion,
+                   double* f_el, double* f_ion, double* epot_e, double* epot_i,
+                   int64_t* rdf_ei, int64_t* rdf_ii) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if ((h->n_el && (!x_el || !f_el)) || (h->n_ion && (!x_ion || !f_ion)))
+    return fail(h, TREE_GPU_ERR_ARG, "null particle buffer");
+  const size_t be = 3 * sizeof(double) * (size_t)h->n_el;
+  const size_t bi = 3 * sizeof(double) * (size_t)h->n_ion;
+  if (be) CK(cudaMemcpyAsync(h->x, x_el, be, cudaMemcpyHostToDevice, h->st));
+  if (bi)
+    CK(cudaMemcpyAsync(h->x + 3 * h->n_el, x_ion, bi, cudaMemcpyHostToDevice, h->st));
+  bool with_rdf = rdf_ei || rdf_ii;
+  int rc = force_device(h, with_rdf);
+  if (rc) return rc;
+  if (be) CK(cudaMemcpyAsync(f_el, h->f, be, cudaMemcpyDeviceToHost, h->st));
+  if (bi)
+    CK(cudaMemcpyAsync(f_ion, h->f + 3 * h->n_el, bi, cudaMemcpyDeviceToHost, h->st));
+  double ep[4];
+  CK(cudaMemcpyAsync(ep, h->diag, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  std::vector<uint32_t> hr;
+  if (with_rdf) {
+    hr.resize(2 * (size_t)tg::kRdfBins);
+    CK(cudaMemcpyAsync(hr.data(), h->rdf, hr.size() * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  if (epot_e) *epot_e = ep[0];
+  if (epot_i) *epot_i = ep[1];
+  if (with_rdf) {
+    for (int i = 0; i < tg::kRdfBins; ++i) {
+      if (rdf_ei) rdf_ei[i] += hr[i];
+      if (rdf_ii) rdf_ii[i] += hr[tg::kRdfBins + i];
+    }
+  }
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_set_state(tree_gpu_handle* h, const double* x_el,
+                       const double* v_el, const double* x_ion,
+                       const double* v_ion) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if ((h->n_el && (!x_el || !v_el)) || (h->n_ion && (!x_ion || !v_ion)))
+    return fail(h, TREE_GPU_ERR_ARG, "null particle buffer");
+  const size_t be = 3 * sizeof(double) * (size_t)h->n_el;
+  const size_t bi = 3 * sizeof(double) * (size_t)h->n_ion;
+  if (be) {
+    CK(cudaMemcpyAsync(h->x, x_el, be, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->v, v_el, be, cudaMemcpyHostToDevice, h->st));
+  }
+  if (bi) {
+    CK(cudaMemcpyAsync(h->x + 3 * h->n_el, x_ion, bi, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->v + 3 * h->n_el, v_ion, bi, cudaMemcpyHostToDevice, h->st));
+  }
+  int rc = force_device(h, false);
+  if (rc) return rc;
+  h->has_state = true;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_load_state(tree_gpu_handle* h, const double* x_el,
+                        const double* v_el, const double* f_el,
+                        const double* x_ion, const double* v_ion,
+                        const double* f_ion) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if ((h->n_el && (!x_el || !v_el || !f_el)) ||
+      (h->n_ion && (!x_ion || !v_ion || !f_ion)))
+    return fail(h, TREE_GPU_ERR_ARG, "null particle buffer");
+  const size_t be = 3 * sizeof(double) * (size_t)h->n_el;
+  const size_t bi = 3 * sizeof(double) * (size_t)h->n_ion;
+  const size_t oi = 3 * (size_t)h->n_el;
+  if (be) {
+    CK(cudaMemcpyAsync(h->x, x_el, be, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->v, v_el, be, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->f, f_el, be, cudaMemcpyHostToDevice, h->st));
+  }
+  if (bi) {
+    CK(cudaMemcpyAsync(h->x + oi, x_ion, bi, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->v + oi, v_ion, bi, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->f + oi, f_ion, bi, cudaMemcpyHostToDevice, h->st));
+  }
+  h->has_state = true;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_step(tree_gpu_handle* h, double dt, int32_t nsteps,
+                  tree_gpu_diag* out) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (!h->has_state) return fail(h, TREE_GPU_ERR_STATE, "tree_gpu_set_state first");
+  if (nsteps < 0 || !std::isfinite(dt)) return fail(h, TREE_GPU_ERR_ARG, "bad dt/nsteps");
+  if (nsteps == 0) return TREE_GPU_OK;
+  const tree_gpu_params& p = h->prm;
+  const int n = h->n, ne = (int)h->n_el;
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    events_for(h, (size_t)nsteps);  // grow first: references below stay valid
+    EventSet& e0 = events_for(h, 0);
+    cudaEventRecord(e0.e[3], h->st);
+    tg::kick_drift(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, h->st);
+    h->timing.launches += n > 0 ? 1 : 0;
+    for (int s = 0; s < nsteps; ++s) {
+      EventSet& ev = events_for(h, 1 + (size_t)s);
+      enqueue_force(h, false, &ev);
+      bool last = s == nsteps - 1;
+      tg::kick2(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, last, !last,
+                h->partial, h->diag + 4, h->st);
+      h->timing.launches += n > 0 ? (last ? 2 : 1) : 0;
+      cudaEventRecord(ev.e[3], h->st);
+    }
+    CK(cudaGetLastError());
+    bool grow = false;
+    int rc = check_device_status(h, &grow);
+    if (rc) return rc;
+    if (grow) {
+      // The positions already moved; a capacity miss means the forces of this
+      // batch are invalid.  Report it: the caller restores state and retries.
+      if ((rc = grow_nodes(h))) return rc;
+      return fail(h, TREE_GPU_ERR_CAPACITY,
+                  "node capacity grew during step; state must be reloaded");
+    }
+    for (int s = 0; s < nsteps; ++s) {
+      EventSet& ev = events_for(h, 1 + (size_t)s);
+      h->timing.ms_build += elapsed(ev.e[0], ev.e[1]);
+      h->timing.ms_walk += elapsed(ev.e[1], ev.e[2]);
+    }
+    EventSet& elast = events_for(h, (size_t)nsteps);
+    float tot = elapsed(e0.e[3], elast.e[3]);
+    h->timing.ms_total += tot;
+    h->timing.ms_kdk += 0.0;
+    h->timing.calls += nsteps;
+    read_counters(h);
+    if (out) {
+      double d[8];
+      CK(cudaMemcpy(d, h->diag, sizeof(d), cudaMemcpyDeviceToHost));
+      out->epot_e = d[0];
+      out->epot_i = d[1];
+      out->mv2_el = d[4];
+      out->rad_el = d[5];
+      out->mv2_ion = d[6];
+      out->rad_ion = d[7];
+      out->steps_done = nsteps;
+    }
+    return TREE_GPU_OK;
+  }
+  return fail(h, TREE_GPU_ERR_CAPACITY, "capacity");
+}
+
+int tree_gpu_get_state(tree_gpu_handle* h, double* x_el, double* v_el,
+                       double* f_el, double* x_ion, double* v_ion,
+                       double* f_ion) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  const size_t be = 3 * sizeof(double) * (size_t)h->n_el;
+  const size_t bi = 3 * sizeof(double) * (size_t)h->n_ion;
+  const size_t oi = 3 * (size_t)h->n_el;
+  if (be) {
+    if (x_el) CK(cudaMemcpyAsync(x_el, h->x, be, cudaMemcpyDeviceToHost, h->st));
+    if (v_el) CK(cudaMemcpyAsync(v_el, h->v, be, cudaMemcpyDeviceToHost, h->st));
+    if (f_el) CK(cudaMemcpyAsync(f_el, h->f, be, cudaMemcpyDeviceToHost, h->st));
+  }
+  if (bi) {
+    if (x_ion) CK(cudaMemcpyAsync(x_ion, h->x + oi, bi, cudaMemcpyDeviceToHost, h->st));
+    if (v_ion) CK(cudaMemcpyAsync(v_ion, h->v + oi, bi, cudaMemcpyDeviceToHost, h->st));
+    if (f_ion) CK(cudaMemcpyAsync(f_ion, h->f + oi, bi, cudaMemcpyDeviceToHost, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_direct(tree_gpu_handle* h, const int64_t* targets, int64_t nt,
+                    double* f, double* epot) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (nt < 0 || nt > 0x7fffffff || (nt && (!targets || !f || !epot)))
+    return fail(h, TREE_GPU_ERR_ARG, "bad target list");
+  if (nt == 0) return TREE_GPU_OK;
+  for (int64_t i = 0; i < nt; ++i)
+    if (targets[i] < 0 || targets[i] >= h->n)
+      return fail(h, TREE_GPU_ERR_ARG, "target index out of range");
+  int nch = tg::direct_chunks(h->n, (int)nt);
+  int64_t* d_t = nullptr;
+  double4* d_part = nullptr;
+  double* d_f = nullptr;
+  double* d_e = nullptr;
+  int rc = TREE_GPU_OK;
+  do {
+    if (cudaMalloc(&d_t, nt * sizeof(int64_t)) != cudaSuccess ||
+        cudaMalloc(&d_part, (size_t)nch * nt * sizeof(double4)) != cudaSuccess ||
+        cudaMalloc(&d_f, 3 * nt * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_e, nt * sizeof(double)) != cudaSuccess) {
+      rc = fail(h, TREE_GPU_ERR_CUDA, "direct-sum scratch allocation failed");
+      break;
+    }
+    cudaMemcpyAsync(d_t, targets, nt * sizeof(int64_t), cudaMemcpyHostToDevice, h->st);
+    h->timing.launches += tg::direct_sum(h->x, h->n, (int)h->n_el, d_t, (int)nt,
+                                         walk_params(h), nch, d_part, d_f, d_e,
+                                         h->st);
+    cudaMemcpyAsync(f, d_f, 3 * nt * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    cudaMemcpyAsync(epot, d_e, nt * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) rc = fail(h, TREE_GPU_ERR_CUDA, cudaGetErrorString(e));
+  } while (0);
+  cudaFree(d_t);
+  cudaFree(d_part);
+  cudaFree(d_f);
+  cudaFree(d_e);
+  return rc;
+}
+
+int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
+                       double* centre, double* moments, double* rcrit,
+                       int32_t* level, int64_t* skip, int64_t* pt,
+                       int64_t* n_nodes) {
+  if (!h || (species != 0 && species != 1)) return TREE_GPU_ERR_ARG;
+  int32_t bnd[4];
+  CK(cudaMemcpy(bnd, h->b.bounds, sizeof(bnd), cudaMemcpyDeviceToHost));
+  int lo = bnd[species], hi = bnd[species + 1];
+  int m = hi - lo;
+  if (n_nodes) *n_nodes = m;
+  if (!centre && !moments && !rcrit && !level && !skip && !pt) return TREE_GPU_OK;
+  if (cap < m) return fail(h, TREE_GPU_ERR_ARG, "dump buffer too small");
+  std::vector<double4> c(m);
+  std::vector<double2> mm(5 * (size_t)m);
+  std::vector<int32_t> sk(m), p(m);
+  std::vector<int8_t> lv(m);
+  if (m) {
+    CK(cudaMemcpy(c.data(), h->b.node_c + lo, m * sizeof(double4), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mm.data(), h->b.node_m + 5 * (size_t)lo, 5 * m * sizeof(double2),
+                  cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sk.data(), h->b.node_skip + lo, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(p.data(), h->b.node_pt + lo, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(lv.data(), h->b.node_level + lo, m * sizeof(int8_t), cudaMemcpyDeviceToHost));
+  }
+  for (int i = 0; i < m; ++i) {
+    if (centre) {
+      centre[3 * i] = c[i].x;
+      centre[3 * i + 1] = c[i].y;
+      centre[3 * i + 2] = c[i].z;
+    }
+    if (rcrit) rcrit[i] = c[i].w;
+    if (moments)
+      for (int j = 0; j < 5; ++j) {
+        moments[10 * i + 2 * j] = mm[5 * (size_t)i + j].x;
+        moments[10 * i + 2 * j + 1] = mm[5 * (size_t)i + j].y;
+      }
+    if (level) level[i] = lv[i];
+    if (skip) skip[i] = (int64_t)sk[i] - lo;
+    if (pt) {
+      int64_t q = p[i];
+      if (q >= 0 && species == 1) q -= h->n_el;  // species-local index
+      pt[i] = q;
+    }
+  }
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_set_stream(tree_gpu_handle* h, void* stream) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  CK(cudaStreamSynchronize(h->st));
+  h->st = stream ? (cudaStream_t)stream : h->own_st;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_timings(tree_gpu_handle* h, tree_gpu_timing* out) {
+  if (!h || !out) return TREE_GPU_ERR_ARG;
+  *out = h->timing;
+  return TREE_GPU_OK;
+}
+
+const char* tree_gpu_last_error(tree_gpu_handle* h) {
+  return h ? h->last_error.c_str() : "null handle";
+}
+
+int tree_gpu_destroy(tree_gpu_handle* h) {
+  if (!h) return TREE_GPU_OK;
+  if (h->st) cudaStreamSynchronize(h->st);
+  if (h->own_st && h->own_st != h->st) cudaStreamSynchronize(h->own_st);
+  free_all(h);
+  for (auto& es : h->events)
+    for (int k = 0; k < 4; ++k) cudaEventDestroy(es.e[k]);
+  if (h->h_pinned) cudaFreeHost(h->h_pinned);
+  if (h->own_st) cudaStreamDestroy(h->own_st);
+  delete h;
+  return TREE_GPU_OK;
+}
+
+const char* tree_gpu_version(void) { return TREE_GPU_VERSION_STR; }
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// kdk.cu -- velocity Verlet on the device (compiled -fmad=false) and the
+// deterministic reductions of the diagnostics.
+//
+// VVerletNotemp1 (vverlet.f90:24-39): v += 0.5*dt*f/m ; x += dt*v.
+// VVerletNotemp2 (vverlet.f90:64-76): v += 0.5*dt*f/m, and on sample steps
+// mv2 = sum m v^2, rad = sum m (x.v)^2/|x|^2 (vverlet.f90:81-106).
+// Between two force evaluations the second half kick of step k and the first
+// half kick + drift of step k+1 are one pass over memory (k_kick_kick_drift);
+// the two half kicks stay two roundings, exactly as the reference does them.
+#include "internal.cuh"
+#include "kdk.h"
+
+namespace tg {
+
+constexpr int kKdkThreads = 256;
+
+__device__ __forceinline__ void ke_terms(const double* xi, const double* vi,
+                                         double xm, double& mv2, double& rad) {
+  mv2 = xm * (vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]);
+  double xv = xi[0] * vi[0] + xi[1] * vi[1] + xi[2] * vi[2];
+  rad = xm * (xv * xv) / (xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2]);
+}
+
+// Block sums of 4 values in fixed order (deterministic): partial[b*4 + j].
+__device__ __forceinline__ void block_sum4(double a[4], double* partial) {
+  __shared__ double sh[kKdkThreads / 32][4];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    for (int o = 16; o > 0; o >>= 1) a[j] += __shfl_down_sync(0xffffffffu, a[j], o);
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sh[w][j] = a[j];
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = 0.0;
+    for (int ww = 0; ww < kKdkThreads / 32; ++ww) s += sh[ww][threadIdx.x];
+    partial[4 * blockIdx.x + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_kick_drift(double* __restrict__ x, double* __restrict__ v,
+                             const double* __restrict__ f, int n, int n_el,
+                             double dt, double xm_e, double xm_i) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double xm = i < n_el ? xm_e : xm_i;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    int64_t j = 3 * (int64_t)i + k;
+    double vv = v[j] + 0.5 * dt * f[j] / xm;
+    v[j] = vv;
+    x[j] = x[j] + dt * vv;
+  }
+}
+
+// Second half kick (+ kinetic sums of the kicked state when `sample`), then,
+// when `drift`, the next step's first half kick and drift.
+template <bool SAMPLE, bool DRIFT>
+__global__ void __launch_bounds__(kKdkThreads)
+    k_kick2(double* __restrict__ x, double* __restrict__ v,
+            const double* __restrict__ f, int n, int n_el, double dt,
+            double xm_e, double xm_i, double* __restrict__ partial) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (i < n) {
+    double xm = i < n_el ? xm_e : xm_i;
+    double xi[3], vi[3], fi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      int64_t j = 3 * (int64_t)i + k;
+      xi[k] = x[j];
+      vi[k] = v[j];
+      fi[k] = f[j];
+      vi[k] = vi[k] + 0.5 * dt * fi[k] / xm;  // VVerletNotemp2
+    }
+    if (SAMPLE) {
+      double mv2, rad;
+      ke_terms(xi, vi, xm, mv2, rad);
+      int s = i >= n_el;
+      acc[2 * s] = mv2;
+      acc[2 * s + 1] = rad;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      int64_t j = 3 * (int64_t)i + k;
+      if (DRIFT) {
+        vi[k] = vi[k] + 0.5 * dt * fi[k] / xm;  // next VVerletNotemp1
+        x[j] = xi[k] + dt * vi[k];
+      }
+      v[j] = vi[k];
+    }
+  }
+  if (SAMPLE) block_sum4(acc, partial);
+}
+
+// Sums rows of `partial` (nb x 4) in fixed order into out[0..3].
+__global__ void k_sum_partials4(const double* __restrict__ partial, int nb,
+                                double* out) {
+  __shared__ double sh[kKdkThreads];
+  for (int j = 0; j < 4; ++j) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[4 * b + j];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] = sh[0];
+    __syncthreads();
+  }
+}
+
+// Potential energy: epot_part[i] = (contribution to Epot_e, to Epot_i).
+__global__ void __launch_bounds__(kKdkThreads)
+    k_epot_partial(const double2* __restrict__ ep, int n, double* partial) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (i < n) {
+    double2 e = ep[i];
+    acc[0] = e.x;
+    acc[1] = e.y;
+  }
+  block_sum4(acc, partial);
+}
+
+int kdk_partials_needed(int n) { return (n + kKdkThreads - 1) / kKdkThreads; }
+
+void kick_drift(double* x, double* v, const double* f, int n, int n_el,
+                double dt, double xm_e, double xm_i, cudaStream_t st) {
+  if (n == 0) return;
+  int g = (n + kKdkThreads - 1) / kKdkThreads;
+  k_kick_drift<<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i);
+}
+
+void kick2(double* x, double* v, const double* f, int n, int n_el, double dt,
+           double xm_e, double xm_i, bool sample, bool drift, double* partial,
+           double* out4, cudaStream_t st) {
+  if (n == 0) return;
+  int g = (n + kKdkThreads - 1) / kKdkThreads;
+  if (sample) {
+    if (drift) k_kick2<true, true><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
+    else k_kick2<true, false><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
+    k_sum_partials4<<<1, kKdkThreads, 0, st>>>(partial, g, out4);
+  } else {
+    if (drift) k_kick2<false, true><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
+    else k_kick2<false, false><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
+  }
+}
+
+void epot_sum(const double2* ep, int n, double* partial, double* out4,
+              cudaStream_t st) {
+  if (n == 0) {
+    cudaMemsetAsync(out4, 0, 4 * sizeof(double), st);
+    return;
+  }
+  int g = (n + kKdkThreads - 1) / kKdkThreads;
+  k_epot_partial<<<g, kKdkThreads, 0, st>>>(ep, n, partial);
+  k_sum_partials4<<<1, kKdkThreads, 0, st>>>(partial, g, out4);
+}
+
+}  // namespace tg
