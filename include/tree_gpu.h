@@ -149,6 +149,31 @@ int tree_gpu_get_state(tree_gpu_handle* h, double* x_el, double* v_el,
 int tree_gpu_direct(tree_gpu_handle* h, const int64_t* targets, int64_t nt,
                     double* f, double* epot);
 
+/* Allocation-free direct sum.  No counterpart in the reference.  For callers
+ * that cannot call cudaMalloc: a host program whose memory manager owns all
+ * device memory and hands out only its own buffers, or code running where an
+ * allocation would synchronise the device or is not permitted.  It computes
+ * what tree_gpu_direct computes, but takes DEVICE pointers and no handle:
+ *   d_x       positions, 3*(n_el+n_ion) doubles, electrons first (AoS xyz)
+ *   d_targets nt global particle indices (int64)
+ *   d_f, d_epot  outputs: 3*nt forces and nt values of 0.5*sum V
+ *   stream    cudaStream_t to run on (NULL: the default stream)
+ * Its scratch is a file-scope static device array of 8 MiB that every GPU
+ * loading this library keeps until the process exits.  nt may be at most
+ * TREE_GPU_DIRECT_STATIC_MAX_TARGETS (larger lists return
+ * TREE_GPU_ERR_CAPACITY and do no work); an index outside [0, n) returns
+ * TREE_GPU_ERR_ARG (it is replaced by 0 on the device, so nothing is read out
+ * of bounds).  The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array and its contents persist between calls:
+ * calls that overlap on the GPU (other streams or threads) race on it.  The
+ * call returns after `stream` has finished the work. */
+#define TREE_GPU_DIRECT_STATIC_MAX_TARGETS 65536
+int tree_gpu_direct_static(const double* d_x, int64_t n_el, int64_t n_ion,
+                           const tree_gpu_params* params,
+                           const int64_t* d_targets, int64_t nt, double* d_f,
+                           double* d_epot, void* stream);
+
 /* Debug/parity: copies one species tree (0 electrons, 1 ions) of the last
  * build in pre-order (children 1..8, the reference's visiting order).
  * Per node: centre[3] (charge centre, or the particle for leaves), moments[10]

@@ -30,7 +30,7 @@ RDF_BINS = 10001
 # Every symbol include/tree_gpu.h declares.
 EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
            "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step", "tree_gpu_get_state",
-           "tree_gpu_direct", "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_timings",
+           "tree_gpu_direct", "tree_gpu_direct_static", "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_timings",
            "tree_gpu_last_error",
            "tree_gpu_destroy", "tree_gpu_version")
 
@@ -90,6 +90,9 @@ def load_library(path: str = LIB_PATH):
                                      dp, dp, ctypes.POINTER(ctypes.c_int32),
                                      lp, lp, lp]
     L.tree_gpu_direct.argtypes = [vp, lp, ctypes.c_int64, dp, dp]
+    L.tree_gpu_direct_static.argtypes = [vp, ctypes.c_int64, ctypes.c_int64,
+                                         ctypes.POINTER(Params), vp,
+                                         ctypes.c_int64, vp, vp, vp]
     L.tree_gpu_set_stream.argtypes = [vp, vp]
     L.tree_gpu_timings.argtypes = [vp, ctypes.POINTER(Timing)]
     L.tree_gpu_last_error.argtypes = [vp]

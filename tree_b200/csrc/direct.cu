@@ -102,3 +102,121 @@ int direct_sum(const double* x, int n, int n_el, const int64_t* targets,
 }
 
 }  // namespace tg
+
+// ------------------------------------------------ allocation-free variant ----
+// tree_gpu_direct_static: the same direct sum for callers that cannot
+// allocate device memory.  Its scratch -- a validated copy of the target
+// list, the per-chunk partial sums and an error word -- lives in one
+// file-scope array that every GPU loading this library holds until exit.
+#include <mutex>
+#include "../../include/tree_gpu.h"
+
+namespace {
+
+constexpr size_t kStaticBytes = 8u << 20;         // 8 MiB per device
+constexpr size_t kStaticFlagBytes = 256;          // error word (+ padding)
+constexpr size_t kStaticTargetBytes = (size_t)TREE_GPU_DIRECT_STATIC_MAX_TARGETS * sizeof(int64_t);
+constexpr size_t kStaticPartials =
+    (kStaticBytes - kStaticFlagBytes - kStaticTargetBytes) / sizeof(double4);
+
+__device__ __align__(256) unsigned char g_direct_scratch[kStaticBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+unsigned char* g_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Copies the targets into the scratch, replacing any index outside [0, n) by
+// 0 and raising the error word, so the sum never reads out of bounds.
+__global__ void k_sanitize_targets(const int64_t* __restrict__ in, int nt,
+                                   int64_t n, int64_t* __restrict__ out,
+                                   int32_t* flag) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  int64_t v = in[t];
+  if (v < 0 || v >= n) {
+    atomicOr(flag, 1);
+    v = 0;
+  }
+  out[t] = v;
+}
+
+// Address of the scratch on the current device, looked up once per device.
+unsigned char* scratch_for_current_device(int* status) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    *status = TREE_GPU_ERR_CUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_direct_scratch) != cudaSuccess || !p) {
+      *status = TREE_GPU_ERR_CUDA;
+      return nullptr;
+    }
+    g_scratch_ptr[dev] = (unsigned char*)p;
+  }
+  *status = TREE_GPU_OK;
+  return g_scratch_ptr[dev];
+}
+
+double kelbg_lambda_um_static(double mu_amu, double te) {
+  return 1.054571817e-34 / sqrt(2.0 * mu_amu * 1.66053906660e-27 * 1.380649e-23 * te) * 1e6;
+}
+
+}  // namespace
+
+extern "C" int tree_gpu_direct_static(const double* d_x, int64_t n_el,
+                                      int64_t n_ion,
+                                      const tree_gpu_params* params,
+                                      const int64_t* d_targets, int64_t nt,
+                                      double* d_f, double* d_epot,
+                                      void* stream) {
+  if (!params || n_el < 0 || n_ion < 0 || n_el + n_ion > 0x7fffffff || nt < 0)
+    return TREE_GPU_ERR_ARG;
+  if (nt > TREE_GPU_DIRECT_STATIC_MAX_TARGETS) return TREE_GPU_ERR_CAPACITY;
+  if (params->physics != TREE_GPU_PHYS_REF && params->physics != TREE_GPU_PHYS_KELBG)
+    return TREE_GPU_ERR_ARG;
+  if (params->physics == TREE_GPU_PHYS_REF && !(params->rs > 0.0)) return TREE_GPU_ERR_ARG;
+  if (params->physics == TREE_GPU_PHYS_KELBG &&
+      !(params->te > 0.0 && params->xm_el > 0.0 && params->xm_ion > 0.0))
+    return TREE_GPU_ERR_ARG;
+  if (nt == 0) return TREE_GPU_OK;
+  const int64_t n = n_el + n_ion;
+  if (n == 0 || !d_x || !d_targets || !d_f || !d_epot) return TREE_GPU_ERR_ARG;
+  int status = TREE_GPU_OK;
+  unsigned char* base = scratch_for_current_device(&status);
+  if (!base) return status;
+  int32_t* flag = (int32_t*)base;
+  int64_t* targets = (int64_t*)(base + kStaticFlagBytes);
+  double4* partial = (double4*)(base + kStaticFlagBytes + kStaticTargetBytes);
+
+  tg::WalkParams wp{};
+  wp.physics = params->physics;
+  wp.theta = params->theta;
+  wp.rs = params->rs;
+  if (params->physics == TREE_GPU_PHYS_KELBG) {
+    const double me = params->xm_el, mi = params->xm_ion;
+    wp.lam_ee = kelbg_lambda_um_static(me / 2.0, params->te);
+    wp.lam_ei = kelbg_lambda_um_static(me * mi / (me + mi), params->te);
+    wp.lam_ii = kelbg_lambda_um_static(mi / 2.0, params->te);
+  }
+  wp.dx_ei = params->dx_ei;
+  wp.dx_ii = params->dx_ii;
+
+  int nch = tg::direct_chunks((int)n, (int)nt);
+  const int64_t fit = (int64_t)kStaticPartials / nt;
+  if (nch > fit) nch = (int)fit;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the error word keeps the previous call's value: clear it first
+  if (cudaMemsetAsync(flag, 0, sizeof(int32_t), st) != cudaSuccess) return TREE_GPU_ERR_CUDA;
+  k_sanitize_targets<<<(int)((nt + 255) / 256), 256, 0, st>>>(d_targets, (int)nt, n, targets, flag);
+  tg::direct_sum(d_x, (int)n, (int)n_el, targets, (int)nt, wp, nch, partial,
+                 d_f, d_epot, st);
+  if (cudaGetLastError() != cudaSuccess) return TREE_GPU_ERR_CUDA;
+  int32_t hflag = 0;
+  if (cudaMemcpyAsync(&hflag, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return TREE_GPU_ERR_CUDA;
+  return hflag ? TREE_GPU_ERR_ARG : TREE_GPU_OK;
+}
