@@ -191,6 +191,13 @@ int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
  * device work and time it with events on the same stream. */
 int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
 
+/* Tunables of the mixed-precision walk: twigs holding at most `bucket`
+ * particles (1..8) are summed particle by particle instead of being opened;
+ * `blocks_per_sm` (1..4) sets the persistent grid.  No counterpart in the
+ * reference; set by the autotuner (tree_b200/tune.py). */
+int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
+                        int32_t blocks_per_sm);
+
 int tree_gpu_timings(tree_gpu_handle* h, tree_gpu_timing* out);
 const char* tree_gpu_last_error(tree_gpu_handle* h);
 int tree_gpu_destroy(tree_gpu_handle* h);

@@ -30,7 +30,7 @@ RDF_BINS = 10001
 # Every symbol include/tree_gpu.h declares.
 EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
            "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step", "tree_gpu_get_state",
-           "tree_gpu_direct", "tree_gpu_direct_static", "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_timings",
+           "tree_gpu_direct", "tree_gpu_direct_static", "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning", "tree_gpu_timings",
            "tree_gpu_last_error",
            "tree_gpu_destroy", "tree_gpu_version")
 
@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.POINTER(Params), vp,
                                          ctypes.c_int64, vp, vp, vp]
     L.tree_gpu_set_stream.argtypes = [vp, vp]
+    L.tree_gpu_set_tuning.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
     L.tree_gpu_timings.argtypes = [vp, ctypes.POINTER(Timing)]
     L.tree_gpu_last_error.argtypes = [vp]
     L.tree_gpu_last_error.restype = ctypes.c_char_p
@@ -261,6 +262,9 @@ class TreeForce:
         e.g. torch.cuda.current_stream().cuda_stream); None restores the
         handle's own stream."""
         self._check(self.lib.tree_gpu_set_stream(self.h, stream_handle or None))
+
+    def set_tuning(self, bucket: int = 4, blocks_per_sm: int = 4):
+        self._check(self.lib.tree_gpu_set_tuning(self.h, bucket, blocks_per_sm))
 
     def timings(self) -> Timing:
         t = Timing()

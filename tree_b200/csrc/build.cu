@@ -116,9 +116,13 @@ __global__ void k_geom(const uint64_t* bb, int n, int n_el, Geom* g) {
 // ---------------------------------------------------------------- keys ----
 // Replays Insert_Tree's descent (tree.f90:132-173 comparisons, 123-126 child
 // centres) for 21 levels.
+// Key layouts.  Per-species trees (lsb = 0): bit 63 = species, bits 62..0 =
+// 21 levels of 3 bits.  Combined tree (lsb = 1): bits 63..1 = 21 levels,
+// bit 0 = species, a 22nd one-bit level that separates an electron sitting
+// exactly on an ion (the t = 0 state of the clouds).
 __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
-                       const Geom* __restrict__ geom, uint64_t* keys,
-                       uint32_t* vals) {
+                       int lsb, int n_el_charge, const Geom* __restrict__ geom,
+                       uint64_t* keys, uint32_t* vals) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int s = i >= n_el;
@@ -142,7 +146,9 @@ __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
     }
     key = (key << 3) | b;
   }
-  keys[i] = key | (s ? kSpeciesBit : 0ull);
+  if (lsb) key = (key << 1) | (i >= n_el_charge ? 1ull : 0ull);
+  else key |= s ? kSpeciesBit : 0ull;
+  keys[i] = key;
   vals[i] = (uint32_t)i;
 }
 
@@ -368,20 +374,23 @@ int radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
 // L[p] = number of leading levels that sorted keys p and p+1 share (same
 // species), else -1.  Identical keys mean the 21-level cap was hit.
 __global__ void k_common_levels(const uint64_t* __restrict__ keys, int n,
-                                int8_t* L, int32_t* err) {
+                                int lsb, int8_t* L, int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int8_t r = -1;
   if (p + 1 < n) {
     uint64_t a = keys[p], b = keys[p + 1];
     uint64_t x = a ^ b;
-    if ((x >> 63) == 0) {
+    if (lsb || (x >> 63) == 0) {
       if (x == 0) {
         set_error(err, kErrDepth);
         r = kMaxLevel;
       } else {
-        int lz = __clzll((long long)x);  // >= 1 (species bit equal)
-        r = (int8_t)((lz - 1) / 3);
+        int lz = __clzll((long long)x);
+        // lsb = 0: lz >= 1 (species bit equal); lsb = 1: lz = 63 means only
+        // the species bit differs, i.e. all 21 spatial levels are shared
+        int lev = lsb ? lz / 3 : (lz - 1) / 3;
+        r = (int8_t)(lev < kMaxLevel ? lev : kMaxLevel);
       }
     }
   }
@@ -426,14 +435,19 @@ __device__ __forceinline__ int lower_prefix(const uint64_t* __restrict__ keys,
   return lo_i;
 }
 
-__device__ __forceinline__ int shift_for_level(int d) { return 63 - 3 * d; }
+// Shift that leaves the first d levels of a key (1 <= d <= 21); level 22 of
+// the combined layout is the whole key.
+__device__ __forceinline__ int shift_for_level(int d, int lsb) {
+  int s = 63 - 3 * d + lsb;
+  return s > 0 ? s : 0;
+}
 
 // Index of the twig at level d that contains sorted particle p, given that it
 // was opened at an earlier particle (first particle of the level-d prefix).
 __device__ __forceinline__ int twig_index_before(
     const uint64_t* __restrict__ keys, const int8_t* __restrict__ L,
-    const int32_t* __restrict__ off, int sb, int p, int d) {
-  int sh = shift_for_level(d);
+    const int32_t* __restrict__ off, int sb, int p, int d, int lsb) {
+  int sh = shift_for_level(d, lsb);
   uint64_t pre = keys[p] >> sh;
   int q = lower_prefix(keys, sb, p + 1, sh, pre);
   int lo_q = q == 0 ? -1 : (int)L[q - 1];
@@ -446,11 +460,11 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
                            const uint32_t* __restrict__ vals,
                            const int8_t* __restrict__ L,
                            const int32_t* __restrict__ off, int n, int n_el,
-                           const Geom* __restrict__ geom, int cap,
+                           int lsb, const Geom* __restrict__ geom, int cap,
                            double4* node_c, int32_t* node_skip,
                            int32_t* node_pt, int32_t* node_parent,
                            int32_t* node_nchild, int32_t* node_done,
-                           int8_t* node_level, int32_t* err) {
+                           int8_t* node_level, MixedNodes mx, int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int lo, hi;
@@ -480,24 +494,33 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
       node_done[idx] = 0;
       node_nchild[idx] = 0;  // children add themselves below (other threads
                              // add after this store: see k_link_children)
-      int sk;
+      int sk, q_end;
       if (d == 0) {
         sk = tree_end;
+        q_end = se;
       } else {
-        int sh = shift_for_level(d);
+        int sh = shift_for_level(d, lsb);
         int q = upper_prefix(keys, p + 1, se, sh, key >> sh);
         sk = q < se ? off[q] : tree_end;
+        q_end = q;
       }
       node_skip[idx] = sk;
+      // particle range and child table used by the mixed-precision walk
+      mx.first[idx] = p;
+      mx.count[idx] = q_end - p;
+      mx.digit[idx] = d == 0 ? (int8_t)0 : (int8_t)((key >> (63 - 3 * d + lsb)) & 7);
+      int4* kk = reinterpret_cast<int4*>(mx.kids + 8 * (int64_t)idx);
+      kk[0] = make_int4(-1, -1, -1, -1);
+      kk[1] = make_int4(-1, -1, -1, -1);
       int par;
       if (d == 0) par = -1;
       else if (d > lo + 1) par = idx - 1;
-      else par = twig_index_before(keys, L, off, sb, p, d - 1);
+      else par = twig_index_before(keys, L, off, sb, p, d - 1, lsb);
       node_parent[idx] = par;
     }
     // descend one level along this particle's digits
     if (d < kMaxLevel) {
-      int dig = (int)((key >> (60 - 3 * d)) & 7);
+      int dig = (int)((key >> (60 - 3 * d + lsb)) & 7);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         bool bit = (dig >> k) & 1;
@@ -518,20 +541,27 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
   node_pt[leaf] = (int32_t)vals[p];
   node_done[leaf] = 0;
   node_nchild[leaf] = 0;
+  mx.first[leaf] = p;
+  mx.count[leaf] = 1;
+  mx.digit[leaf] = depth <= kMaxLevel ? (int8_t)((key >> (63 - 3 * depth + lsb)) & 7)
+                                      : (int8_t)(lsb ? (key & 1) : 0);
   node_parent[leaf] = ntw > 0 ? leaf - 1
-                              : twig_index_before(keys, L, off, sb, p, depth - 1);
+                              : twig_index_before(keys, L, off, sb, p, depth - 1, lsb);
 }
 
 // Counts children per twig (separate launch so the zeroing in k_topology is
 // complete).
 __global__ void k_link_children(const int32_t* __restrict__ node_parent,
                                 const int32_t* __restrict__ bounds, int cap,
-                                int32_t* node_nchild) {
+                                int32_t* node_nchild, MixedNodes mx) {
   int m = bounds[2] < cap ? bounds[2] : cap;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int par = node_parent[i];
-  if (par >= 0) atomicAdd(&node_nchild[par], 1);
+  if (par >= 0) {
+    atomicAdd(&node_nchild[par], 1);
+    mx.kids[8 * (int64_t)par + mx.digit[i]] = i;  // siblings have distinct digits
+  }
 }
 
 __global__ void k_bounds(const int32_t* __restrict__ off, int n, int n_el,
@@ -652,9 +682,196 @@ __global__ void k_upward(const double* __restrict__ x,
   }
 }
 
+// ------------------------------------------------ net-charge upward pass ----
+// Combined tree (both species in one tree) for the mixed-precision walk.  Per
+// node: particle count n, centroid X (the expansion centre), net charge Q,
+// dipole D = sum q (x - X), second moment S = 1/2 sum q (x - X)(x - X)^T and
+// the ion count.  Children are combined exactly (parallel axis):
+//   d_c = X_c - X,  D = sum D_c + Q_c d_c,
+//   S = sum S_c + (D_c d_c^T + d_c D_c^T)/2 + Q_c d_c d_c^T / 2.
+// In a quasi-neutral plasma Q ~ 0 for large cells and the far field is the
+// small net (dipole/quadrupole) field, so its truncation error is relative to
+// that net field rather than to each species' monopole.
+// m64 per node (6 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
+// (Szz, Sxy) | (Syz, Szx).  mom per node (3 x float4): (Q, Dx, Dy, Dz),
+// (Sxx, Syy, Szz, Sxy), (Syz, Szx, trace S, q_ion).
+__global__ void k_upward_net(const double* __restrict__ x,
+                             const uint32_t* __restrict__ vals,
+                             const int8_t* __restrict__ L,
+                             const int32_t* __restrict__ off, int n,
+                             int n_el_charge, const Geom* __restrict__ geom,
+                             double theta, int cap, double4* node_c,
+                             const int32_t* __restrict__ node_skip,
+                             const int32_t* __restrict__ node_parent,
+                             const int32_t* __restrict__ node_nchild,
+                             int32_t* node_done,
+                             const int8_t* __restrict__ node_level,
+                             MixedNodes mx, int32_t* err) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  if (*((volatile int32_t*)err) & kErrCapacity) return;
+  int lo, hi;
+  lo_hi(L, p, lo, hi);
+  int ntw = hi > lo ? hi - lo : 0;
+  int leaf = off[p] + ntw;
+  if (leaf >= cap) return;
+  uint32_t o = vals[p];
+  const bool ion = (int)o >= n_el_charge;
+  const double q = ion ? 1.0 : -1.0;
+  const double px = x[3 * (int64_t)o], py = x[3 * (int64_t)o + 1],
+               pz = x[3 * (int64_t)o + 2];
+  node_c[leaf] = make_double4(px, py, pz, -1.0);
+  {
+    double2* m = mx.m64 + 6 * (int64_t)leaf;
+    m[0] = make_double2(1.0, q);
+    m[1] = make_double2(0.0, 0.0);
+    m[2] = make_double2(0.0, ion ? 1.0 : 0.0);
+    m[3] = make_double2(0.0, 0.0);
+    m[4] = make_double2(0.0, 0.0);
+    m[5] = make_double2(0.0, 0.0);
+    float4* f = mx.mom + 3 * (int64_t)leaf;
+    f[0] = make_float4((float)q, 0.f, 0.f, 0.f);
+    f[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f[2] = make_float4(0.f, 0.f, 0.f, ion ? 1.f : 0.f);
+    mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
+  }
+  __threadfence();
+  const double smax0 = geom[0].smax0;
+  int cur = node_parent[leaf];
+  int guard = 0;
+  while (cur >= 0) {
+    if (++guard > kMaxLevel + 2) {
+      set_error(err, kErrWalk);
+      return;
+    }
+    int old = atomicAdd(&node_done[cur], 1);
+    if (old != node_nchild[cur] - 1) return;
+    __threadfence();
+    const double4 gc = ldcg_d4(&node_c[cur]);  // geometric centre (topology)
+    int end = node_skip[cur];
+    if (end > cap) end = cap;
+    // pass 1: count and centroid
+    double nsum = 0.0, X0 = 0.0, X1 = 0.0, X2 = 0.0;
+    int c = cur + 1;
+    while (c < end) {
+      const double4 cc = ldcg_d4(&node_c[c]);
+      const double nc = __ldcg(mx.m64 + 6 * (int64_t)c).x;
+      nsum += nc;
+      X0 += nc * cc.x;
+      X1 += nc * cc.y;
+      X2 += nc * cc.z;
+      int nx = node_skip[c];
+      if (nx <= c) {
+        set_error(err, kErrWalk);
+        return;
+      }
+      c = nx;
+    }
+    X0 /= nsum;
+    X1 /= nsum;
+    X2 /= nsum;
+    // pass 2: moments about the centroid
+    double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
+    double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
+    c = cur + 1;
+    while (c < end) {
+      const double4 cc = ldcg_d4(&node_c[c]);
+      const double2* cm = mx.m64 + 6 * (int64_t)c;
+      const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
+                    a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
+      const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
+      const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
+      Q += qc;
+      qi += a2.y;
+      Dx += dcx + qc * ex;
+      Dy += dcy + qc * ey;
+      Dz += dcz + qc * ez;
+      Sxx += a3.x + dcx * ex + 0.5 * qc * ex * ex;
+      Syy += a3.y + dcy * ey + 0.5 * qc * ey * ey;
+      Szz += a4.x + dcz * ez + 0.5 * qc * ez * ez;
+      Sxy += a4.y + 0.5 * (dcx * ey + ex * dcy) + 0.5 * qc * ex * ey;
+      Syz += a5.x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez;
+      Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
+      c = node_skip[c];
+    }
+    const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
+    const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+    const int lev = node_level[cur];
+    double smax = smax0;
+    for (int l = 0; l < lev; ++l) smax = smax * 0.5;
+    node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
+    double2* m = mx.m64 + 6 * (int64_t)cur;
+    m[0] = make_double2(nsum, Q);
+    m[1] = make_double2(Dx, Dy);
+    m[2] = make_double2(Dz, qi);
+    m[3] = make_double2(Sxx, Syy);
+    m[4] = make_double2(Szz, Sxy);
+    m[5] = make_double2(Syz, Szx);
+    float4* f = mx.mom + 3 * (int64_t)cur;
+    f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
+    f[1] = make_float4((float)Sxx, (float)Syy, (float)Szz, (float)Sxy);
+    f[2] = make_float4((float)Syz, (float)Szx, (float)(Sxx + Syy + Szz), (float)qi);
+    __threadfence();
+    cur = node_parent[cur];
+  }
+}
+
+// ------------------------------------------------------------ groups ----
+// Target groups of the mixed walk: maximal cells holding at most kGroupMax
+// particles, with consecutive small siblings packed together up to kGroupMax.
+// Every group is a contiguous sorted range inside one parent cell, so its
+// bounding box stays compact.  Group order is not deterministic (atomic
+// append); the content of every group is.
+__global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
+                         MixedNodes mx, int2* groups, int32_t* n_groups) {
+  int m = bounds[2] < cap ? bounds[2] : cap;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m) return;
+  const int cnt = mx.count[t];
+  if (t == 0 && cnt <= kGroupMax) {  // whole tree fits one group
+    int g = atomicAdd(n_groups, 1);
+    groups[g] = make_int2(mx.first[0], cnt);
+    return;
+  }
+  if (cnt <= kGroupMax || cnt == 1) return;
+  const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)t);
+  const int4 k0 = kk[0], k1 = kk[1];
+  const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+  int run_first = -1, run_cnt = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int c = kv[j];
+    if (c < 0) continue;
+    const int cc = mx.count[c];
+    if (cc > kGroupMax) {  // recursed into by its own thread: closes the run
+      if (run_cnt > 0) {
+        int g = atomicAdd(n_groups, 1);
+        groups[g] = make_int2(run_first, run_cnt);
+      }
+      run_first = -1;
+      run_cnt = 0;
+      continue;
+    }
+    if (run_cnt > 0 && run_cnt + cc > kGroupMax) {
+      int g = atomicAdd(n_groups, 1);
+      groups[g] = make_int2(run_first, run_cnt);
+      run_first = -1;
+      run_cnt = 0;
+    }
+    if (run_cnt == 0) run_first = mx.first[c];
+    run_cnt += cc;
+  }
+  if (run_cnt > 0) {
+    int g = atomicAdd(n_groups, 1);
+    groups[g] = make_int2(run_first, run_cnt);
+  }
+}
+
 // ------------------------------------------------------------- driver ----
 int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
-                double theta, cudaStream_t st) {
+                double theta, int mode, cudaStream_t st) {
+  // mode 0: one tree per species (parity path); mode 1: one combined tree
+  const int split = mode == 0 ? n_el : n;
   const int T = 256;
   k_bbox_init<<<1, 32, 0, st>>>(b.bbox, b.err);
   if (n == 0) {
@@ -664,27 +881,39 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   int launches = 1;
   int gb = (n + T - 1) / T;
   int gbb = gb < 4 * 148 ? gb : 4 * 148;
-  k_bbox<<<gbb, T, 0, st>>>(x, n, n_el, b.bbox, b.err);
-  k_geom<<<1, 32, 0, st>>>(b.bbox, n, n_el, b.geom);
-  k_keys<<<gb, T, 0, st>>>(x, n, n_el, b.geom, b.keys, b.vals);
+  k_bbox<<<gbb, T, 0, st>>>(x, n, split, b.bbox, b.err);
+  k_geom<<<1, 32, 0, st>>>(b.bbox, n, split, b.geom);
+  const int lsb = mode == 0 ? 0 : 1;
+  k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, b.keys, b.vals);
   launches += 3;
   launches += radix_sort(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
                          b.sort_hist, b.scan_partial, st);
-  k_common_levels<<<gb, T, 0, st>>>(b.keys, n, b.L, b.err);
+  k_common_levels<<<gb, T, 0, st>>>(b.keys, n, lsb, b.L, b.err);
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);
-  k_bounds<<<1, 32, 0, st>>>(b.off, n, n_el, b.cap, b.bounds, b.err);
-  k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, n_el, b.geom,
+  k_bounds<<<1, 32, 0, st>>>(b.off, n, split, b.cap, b.bounds, b.err);
+  k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, split, lsb, b.geom,
                                b.cap, b.node_c, b.node_skip, b.node_pt,
                                b.node_parent, b.node_nchild, b.node_done,
-                               b.node_level, b.err);
+                               b.node_level, b.mx, b.err);
   int gcap = (b.cap + T - 1) / T;
   k_link_children<<<gcap, T, 0, st>>>(b.node_parent, b.bounds, b.cap,
-                                      b.node_nchild);
-  k_upward<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.geom, theta, b.cap, b.bounds, b.node_c, b.node_m,
-                             b.node_skip, b.node_parent, b.node_nchild,
-                             b.node_done, b.node_level, b.err);
-  return launches + 4;
+                                      b.node_nchild, b.mx);
+  launches += 3;
+  if (mode == 0) {
+    k_upward<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, split, b.geom, theta,
+                               b.cap, b.bounds, b.node_c, b.node_m,
+                               b.node_skip, b.node_parent, b.node_nchild,
+                               b.node_done, b.node_level, b.err);
+    return launches + 1;
+  }
+  k_upward_net<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.geom, theta,
+                                 b.cap, b.node_c, b.node_skip, b.node_parent,
+                                 b.node_nchild, b.node_done, b.node_level, b.mx,
+                                 b.err);
+  cudaMemsetAsync(b.mx.n_groups, 0, sizeof(int32_t), st);
+  k_groups<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.mx, b.mx.groups, b.mx.n_groups);
+  return launches + 2;
 }
 
 }  // namespace tg

@@ -6,6 +6,20 @@
 
 namespace tg {
 
+// Node data of the combined tree that the mixed-precision walk reads.
+constexpr int kGroupMax = 32;  // targets per warp group
+struct MixedNodes {
+  int32_t* kids;     // 8 per node: child index per octant digit, -1 if none
+  int32_t* first;    // first sorted particle of the node's range
+  int32_t* count;    // particles in the node
+  int8_t* digit;     // octant of the node inside its parent
+  double2* m64;      // 6 per node: (n, Q) (Dx, Dy) (Dz, q_ion) (Sxx, Syy) (Szz, Sxy) (Syz, Szx)
+  float4* mom;       // 3 per node: (Q, Dx, Dy, Dz) (Sxx, Syy, Szz, Sxy) (Syz, Szx, trS, q_ion)
+  double4* xs;       // per sorted particle: position, w = 1 for ions
+  int2* groups;      // target groups (first sorted particle, count)
+  int32_t* n_groups; // device count of groups
+};
+
 struct BuildBuffers {
   // particle-indexed (n)
   uint64_t* keys;
@@ -32,6 +46,7 @@ struct BuildBuffers {
   Geom* geom;           // 2
   int32_t* bounds;      // 4: 0, M_e, M (clamped to cap), M (untruncated)
   int32_t* err;
+  MixedNodes mx;
 };
 
 int radix_blocks(int n);
@@ -41,8 +56,10 @@ int exclusive_scan(const int32_t* in, int32_t* out, int n, int32_t* partial,
 int radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
                 uint32_t* vals_alt, int n, int32_t* hist, int32_t* partial,
                 cudaStream_t st);
-// Builds both species trees for positions x (AoS, electrons first).
+// Builds the trees for positions x (AoS, electrons first).  mode 0: one tree
+// per species with the reference's one-level moments (parity path); mode 1:
+// one combined tree with net-charge moments and target groups (mixed path).
 int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
-                 double theta, cudaStream_t st);
+                double theta, int mode, cudaStream_t st);
 
 }  // namespace tg

@@ -51,6 +51,7 @@ struct tree_gpu_handle {
   double2* epot_part = nullptr;
   tg::BuildBuffers b{};
   tg::MixedBuffers mb{};
+  tg::MixedTuning tune{};
   uint32_t* rdf = nullptr;
   unsigned long long* counters = nullptr;
   double* partial = nullptr;
@@ -125,7 +126,10 @@ int alloc_nodes(tree_gpu_handle* h, int cap) {
   if ((rc = dalloc(h, &b.node_nchild, cap))) return rc;
   if ((rc = dalloc(h, &b.node_done, cap))) return rc;
   if ((rc = dalloc(h, &b.node_level, cap))) return rc;
-  return tg::mixed_alloc_nodes(h->mb, cap) ? fail(h, TREE_GPU_ERR_CUDA, "mixed node alloc") : 0;
+  if (tg::mixed_alloc_nodes(h->mb, cap))
+    return fail(h, TREE_GPU_ERR_CUDA, "mixed node alloc");
+  h->b.mx = tg::mixed_nodes(h->mb);
+  return 0;
 }
 
 int alloc_all(tree_gpu_handle* h) {
@@ -159,6 +163,7 @@ int alloc_all(tree_gpu_handle* h) {
   CK(cudaMemsetAsync(h->diag, 0, 8 * sizeof(double), h->st));
   if (tg::mixed_alloc_particles(h->mb, n))
     return fail(h, TREE_GPU_ERR_CUDA, "mixed particle alloc");
+  h->b.mx = tg::mixed_nodes(h->mb);
   int cap = 3 * n + 64;
   return alloc_nodes(h, cap);
 }
@@ -212,8 +217,9 @@ EventSet& events_for(tree_gpu_handle* h, size_t i) {
 void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
   cudaStream_t st = h->st;
   if (ev) cudaEventRecord(ev->e[0], st);
+  const int mode = h->prm.precision == TREE_GPU_PREC_FP64 ? 0 : 1;
   h->timing.launches +=
-      tg::build_trees(h->b, h->x, h->n, (int)h->n_el, h->prm.theta, st);
+      tg::build_trees(h->b, h->x, h->n, (int)h->n_el, h->prm.theta, mode, st);
   if (ev) cudaEventRecord(ev->e[1], st);
   cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), st);
   if (with_rdf)
@@ -225,12 +231,13 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
                h->epot_part, with_rdf ? h->rdf : nullptr, h->counters,
                h->b.err, st);
   } else {
-    tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp,
-                   h->prm.mac, h->prm.group, h->f, h->epot_part,
-                   with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
+    tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp, h->tune,
+                   h->f, h->epot_part, with_rdf ? h->rdf : nullptr,
+                   h->counters, h->b.err, st);
   }
   if (ev) cudaEventRecord(ev->e[2], st);
   h->timing.launches += (h->n > 0 ? 1 : 0) + 2;  // walk + epot partial/sum
+  // (the mixed walk is one kernel as well)
   tg::epot_sum(h->epot_part, h->n, h->partial, h->diag, st);
 }
 
@@ -610,6 +617,16 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream) {
   if (!h) return TREE_GPU_ERR_ARG;
   CK(cudaStreamSynchronize(h->st));
   h->st = stream ? (cudaStream_t)stream : h->own_st;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
+                        int32_t blocks_per_sm) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (bucket < 1 || bucket > 8 || blocks_per_sm < 1 || blocks_per_sm > 4)
+    return fail(h, TREE_GPU_ERR_ARG, "bucket must be 1..8, blocks_per_sm 1..4");
+  h->tune.bucket = bucket;
+  h->tune.blocks_per_sm = blocks_per_sm;
   return TREE_GPU_OK;
 }
 

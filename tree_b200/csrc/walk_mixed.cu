@@ -1,0 +1,545 @@
+// walk_mixed.cu -- warp-group Barnes-Hut walk in mixed precision.
+//
+// The mixed path walks ONE combined tree of both species (net-charge moments
+// about each cell's particle centroid, built by k_upward_net).  One warp owns a
+// target group -- a compact cell of at most 32 particles of either species,
+// built by k_groups -- and builds ONE interaction list for it:
+//   * group MAC: a cell is accepted when rcrit = s/theta + dx (the reference
+//     criterion, tree.f90:736-743) is below the distance from the cell's charge
+//     centre to the group's bounding box, so every target of the group would
+//     also accept it on its own;
+//   * accepted cells go to a shared-memory ring of far-field (M2P) entries,
+//     leaves and twigs with at most `bucket` particles go to a ring of
+//     particle (P2P) entries, other twigs push their children on a per-warp
+//     stack;
+//   * every 32 entries the warp stages them in shared memory and each lane
+//     evaluates them for its own target in FP32.
+// Precision: positions, the group centre and the MAC stay FP64.  Cells are
+// evaluated in FP32 relative to the group centre; particle pairs use a
+// two-float (hi + lo) split of the FP64 offsets, so a pair separation keeps
+// ~1e-7 relative accuracy even for the closest e-i pairs.  Chunk sums of 32
+// terms are added into Kahan-compensated per-lane accumulators.
+// Far field: net monopole + dipole + exact quadrupole about the centroid
+// (Coulomb, the expansion of tree.f90:744-779 carried one order further for
+// cells whose net charge nearly cancels).  Near field: erf-Kelbg (or the
+// reference laws) for every particle pair.
+#include <cstdio>
+#include "walk_mixed.h"
+
+namespace tg {
+
+constexpr int kMxWarps = 8;
+constexpr int kMxThreads = 32 * kMxWarps;
+constexpr int kStackCap = 4096;   // node indices per warp
+constexpr int kM2pRing = 64;      // power of two, > 31 + 32
+constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
+constexpr int kMaxBucket = 8;
+constexpr int kMaxBlocksPerSm = 4;
+
+struct WarpSmem {
+  int m2p[kM2pRing];
+  int p2p[kP2pRing];
+  float4 cell[32 * 4];   // (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion), (Sxx, Syy, Szz, Sxy), (Syz, Szx, tr, -)
+  float4 part[32 * 2];   // (hi xyz, sorted index bits), (lo xyz, ion?)
+};
+
+struct MixedArgs {
+  const double4* __restrict__ node_c;
+  const float4* __restrict__ mom;
+  const int32_t* __restrict__ kids;
+  const int32_t* __restrict__ first;
+  const int32_t* __restrict__ count;
+  const double4* __restrict__ xs;
+  const uint32_t* __restrict__ order;
+  const int32_t* __restrict__ bounds;
+  const int2* __restrict__ groups;
+  const int32_t* __restrict__ n_groups;
+  int n, n_el;
+  int32_t* control;
+  int32_t* stack;
+  int bucket;
+  int physics;
+  float inv_lam2_ee, inv_lam2_ei, inv_lam2_ii;
+  float inv_lam_ee, inv_lam_ei, inv_lam_ii;
+  float rs_inv;
+  double dx_ei_inv, dx_ii_inv;
+  double* f;
+  double2* epot_part;
+  uint32_t* rdf;
+  unsigned long long* counters;
+  int32_t* err;
+};
+
+struct Acc {
+  float sx, sy, sz, cx, cy, cz;  // Kahan sums of the unscaled force
+  double phi_all, phi_ion;       // unscaled potential: all sources, ion part
+};
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  float y = v - c;
+  float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
+  int inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  *total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - v;
+}
+
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// ---------------------------------------------------------------- M2P ----
+// 74 flop per entry (FMA = 2): net monopole Q, dipole D and traceful second
+// moment S about the cell centroid.  With d = target - centroid:
+//   phi = Q/r + D.d/r^3 + (3 d.S.d - r^2 tr S)/r^5
+//   -grad phi = g d - D/r^3 - 6 S d/r^5,  g = Q/r^3 + (3 D.d + 15 d.S.d/r^2 - 3 tr S)/r^5
+// The ion part of phi for the Epot_e/Epot_i split is taken at monopole order
+// (q_ion / r).
+__device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
+                                         const MixedArgs& a, double Gx,
+                                         double Gy, double Gz, float tx,
+                                         float ty, float tz, int lane,
+                                         Acc& acc) {
+  if (lane < cnt) {
+    int node = sm.m2p[(head + lane) & (kM2pRing - 1)];
+    double4 c = ldg_d4(&a.node_c[node]);
+    const float4* mp = a.mom + 3 * (int64_t)node;
+    float4 m0 = __ldg(mp), m1 = __ldg(mp + 1), m2 = __ldg(mp + 2);
+    sm.cell[4 * lane] = make_float4((float)(c.x - Gx), (float)(c.y - Gy),
+                                    (float)(c.z - Gz), m0.x);
+    sm.cell[4 * lane + 1] = make_float4(m0.y, m0.z, m0.w, m2.w);
+    sm.cell[4 * lane + 2] = m1;
+    sm.cell[4 * lane + 3] = make_float4(m2.x, m2.y, m2.z, 0.f);
+  }
+  __syncwarp();
+  float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
+#pragma unroll 2
+  for (int k = 0; k < cnt; ++k) {
+    const float4 A = sm.cell[4 * k], B = sm.cell[4 * k + 1];
+    const float4 C = sm.cell[4 * k + 2], E = sm.cell[4 * k + 3];
+    const float dx = tx - A.x, dy = ty - A.y, dz = tz - A.z;
+    // accepted cells are farther than rcrit >= 0; the floor only guards a
+    // zero-size cell against an FP32 distance of 0
+    const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    const float rinv3 = rinv * rinv2;
+    const float rinv5 = rinv3 * rinv2;
+    // S d with S = [[Sxx,Sxy,Szx],[Sxy,Syy,Syz],[Szx,Syz,Szz]]
+    const float Sx = fmaf(C.x, dx, fmaf(C.w, dy, E.y * dz));
+    const float Sy = fmaf(C.w, dx, fmaf(C.y, dy, E.x * dz));
+    const float Sz = fmaf(E.y, dx, fmaf(E.x, dy, C.z * dz));
+    const float u = fmaf(dx, Sx, fmaf(dy, Sy, dz * Sz));
+    const float Dd = fmaf(B.x, dx, fmaf(B.y, dy, B.z * dz));
+    const float ur2 = u * rinv2;
+    const float g = fmaf(A.w, rinv3,
+                         rinv5 * fmaf(3.f, Dd, fmaf(15.f, ur2, -3.f * E.z)));
+    const float h6 = 6.f * rinv5;
+    fx = fmaf(g, dx, fmaf(-h6, Sx, fmaf(-rinv3, B.x, fx)));
+    fy = fmaf(g, dy, fmaf(-h6, Sy, fmaf(-rinv3, B.y, fy)));
+    fz = fmaf(g, dz, fmaf(-h6, Sz, fmaf(-rinv3, B.z, fz)));
+    const float ph = fmaf(A.w, rinv, rinv3 * (Dd + fmaf(3.f, ur2, -E.z)));
+    pa += ph;
+    pi = fmaf(B.w, rinv, pi);
+  }
+  __syncwarp();
+  kahan_add(acc.sx, acc.cx, fx);
+  kahan_add(acc.sy, acc.cy, fy);
+  kahan_add(acc.sz, acc.cz, fz);
+  acc.phi_all += (double)pa;
+  acc.phi_ion += (double)pi;
+}
+
+// ---------------------------------------------------------------- P2P ----
+template <int PHYS, bool RDF>
+__device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
+                                         const MixedArgs& a, double Gx,
+                                         double Gy, double Gz, float thx,
+                                         float thy, float thz, float tlx,
+                                         float tly, float tlz, int p_self,
+                                         int tsp, bool act, int lane,
+                                         Acc& acc) {
+  if (lane < cnt) {
+    int s = sm.p2p[(head + lane) & (kP2pRing - 1)];
+    double4 xs = a.xs[s];
+    double rx = xs.x - Gx, ry = xs.y - Gy, rz = xs.z - Gz;
+    float hx = (float)rx, hy = (float)ry, hz = (float)rz;
+    sm.part[2 * lane] = make_float4(hx, hy, hz, __int_as_float(s));
+    sm.part[2 * lane + 1] =
+        make_float4((float)(rx - (double)hx), (float)(ry - (double)hy),
+                    (float)(rz - (double)hz), (float)xs.w);
+  }
+  __syncwarp();
+  const float tspf = (float)tsp;
+  float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
+  for (int k = 0; k < cnt; ++k) {
+    const float4 P = sm.part[2 * k], Q = sm.part[2 * k + 1];
+    const int s = __float_as_int(P.w);
+    const float dx = (thx - P.x) + (tlx - Q.x);
+    const float dy = (thy - P.y) + (tly - Q.y);
+    const float dz = (thz - P.z) + (tlz - Q.z);
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const bool same = Q.w == tspf;
+    const float ssign = Q.w * 2.f - 1.f;  // source charge: -1 e, +1 ion
+    const bool self = s == p_self;
+    bool rare;
+    float wc;  // weight of the plain Coulomb term
+    if (PHYS == 1) {
+      const float il2 = same ? (tsp ? a.inv_lam2_ii : a.inv_lam2_ee) : a.inv_lam2_ei;
+      rare = !self && r2 * il2 < 40.f;  // exp(-x^2) still visible in FP32
+      wc = (self || rare) ? 0.f : ssign;
+    } else {
+      if (same) {
+        rare = false;
+        wc = r2 > 0.01f ? ssign : 0.f;  // reference cutoff, also drops self
+      } else {
+        rare = r2 * (a.rs_inv * a.rs_inv) < 400.f;  // exp(-r/rs) visible
+        wc = rare ? 0.f : ssign;
+      }
+    }
+    const float rinv = rsqrtf(r2 > 0.f ? r2 : 1.f);
+    const float fs = wc * rinv * rinv * rinv;
+    fx = fmaf(fs, dx, fx);
+    fy = fmaf(fs, dy, fy);
+    fz = fmaf(fs, dz, fz);
+    float ph = wc * rinv;
+    if (rare) {
+      float rfs = 0.f, ve;
+      if (PHYS == 1) {
+        const float il = same ? (tsp ? a.inv_lam_ii : a.inv_lam_ee) : a.inv_lam_ei;
+        const float sqrtpi = 1.77245385f;
+        if (r2 > 0.f) {
+          const float r = sqrtf(r2);
+          const float ri = 1.f / r;
+          const float x2 = r2 * il * il;
+          const float g = -expm1f(-x2);
+          rfs = ssign * g * ri * ri * ri;
+          ve = g * ri + sqrtpi * erfcf(r * il) * il;
+        } else {
+          ve = sqrtpi * il;  // distinct particles on one point: V(0)
+        }
+      } else {
+        if (r2 > 0.f) {
+          const float r = sqrtf(r2);
+          const float ri = 1.f / r;
+          const float e = expf(-r * a.rs_inv);
+          const float g = ri - e * (ri + a.rs_inv);
+          rfs = ssign * g * ri * ri;
+          ve = (1.f - e) * ri;
+        } else {
+          ve = a.rs_inv;  // r -> 0 limit of (1 - exp(-r/rs))/r
+        }
+      }
+      fx = fmaf(rfs, dx, fx);
+      fy = fmaf(rfs, dy, fy);
+      fz = fmaf(rfs, dz, fz);
+      ph += ssign * ve;
+    }
+    pa += ph;
+    pi = fmaf(Q.w, ph, pi);
+    if (RDF && act) {
+      bool counted = PHYS == 1 ? !self : (same ? r2 > 0.01f : true);
+      if (counted && (!same || tsp == 1)) {
+        // bin in FP64 from the hi/lo offsets so bin edges match the FP64 path
+        const double ex = ((double)thx - (double)P.x) + ((double)tlx - (double)Q.x);
+        const double ey = ((double)thy - (double)P.y) + ((double)tly - (double)Q.y);
+        const double ez = ((double)thz - (double)P.z) + ((double)tlz - (double)Q.z);
+        const double t = sqrt(ex * ex + ey * ey + ez * ez) * (same ? a.dx_ii_inv : a.dx_ei_inv);
+        if (t < (double)kRdfBins) {
+          int id = (int)t;
+          if (id >= 0 && id < kRdfBins) atomicAdd(&a.rdf[(same ? kRdfBins : 0) + id], 1u);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  kahan_add(acc.sx, acc.cx, fx);
+  kahan_add(acc.sy, acc.cy, fy);
+  kahan_add(acc.sz, acc.cz, fz);
+  acc.phi_all += (double)pa;
+  acc.phi_ion += (double)pi;
+}
+
+// --------------------------------------------------------------- walk ----
+template <int PHYS, bool RDF>
+__global__ void __launch_bounds__(kMxThreads, 2)
+    k_walk_mixed(MixedArgs a) {
+  __shared__ WarpSmem smem[kMxWarps];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  WarpSmem& sm = smem[wib];
+  const int gwarp = blockIdx.x * kMxWarps + wib;
+  int32_t* stack = a.stack + (int64_t)gwarp * kStackCap;
+  const unsigned lt = (1u << lane) - 1u;
+  if (*((volatile int32_t*)a.err) & (kErrCapacity | kErrDepth | kErrNonFinite)) return;
+  const int root_end = a.bounds[2];  // combined tree: nodes [0, root_end)
+  const int ngroups = *a.n_groups;
+  int max_stack = 0;
+  while (root_end > 0) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(&a.control[0], 1);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= ngroups) break;
+    const int2 grp = a.groups[g];
+    const int p0 = grp.x, n_act = grp.y;
+    const bool act = lane < n_act;
+    const int pt = p0 + (act ? lane : n_act - 1);
+    const double4 xt = a.xs[pt];
+    const int tsp = xt.w > 0.5 ? 1 : 0;  // this lane's target species
+    const double mnx = warp_min_d(xt.x), mny = warp_min_d(xt.y), mnz = warp_min_d(xt.z);
+    const double mxx = warp_max_d(xt.x), mxy = warp_max_d(xt.y), mxz = warp_max_d(xt.z);
+    const double Gx = 0.5 * (mnx + mxx), Gy = 0.5 * (mny + mxy), Gz = 0.5 * (mnz + mxz);
+    const double hx = 0.5 * (mxx - mnx), hy = 0.5 * (mxy - mny), hz = 0.5 * (mxz - mnz);
+    const double rtx = xt.x - Gx, rty = xt.y - Gy, rtz = xt.z - Gz;
+    const float thx = (float)rtx, thy = (float)rty, thz = (float)rtz;
+    const float tlx = (float)(rtx - (double)thx), tly = (float)(rty - (double)thy),
+                tlz = (float)(rtz - (double)thz);
+    Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
+    int ssize = 1;
+    if (lane == 0) stack[0] = 0;  // root
+    __syncwarp();
+    int m2h = 0, m2t = 0, p2h = 0, p2t = 0;  // ring heads/tails (warp-uniform)
+    long long n_m2p = 0, n_p2p = 0;
+    bool overflow = false;
+    while (ssize > 0) {
+      const int nb = min(32, ssize);
+      const int node = lane < nb ? stack[ssize - 1 - lane] : -1;
+      ssize -= nb;
+      __syncwarp();
+      int action = 0, pfirst = 0, pcnt = 0;  // 1 far field, 2 particles, 3 open
+      if (node >= 0) {
+        const double4 c = ldg_d4(&a.node_c[node]);
+        if (c.w < 0.0) {
+          action = 2;
+          pfirst = __ldg(&a.first[node]);
+          pcnt = 1;
+        } else {
+          // group MAC: rcrit below the distance from the centroid to the box
+          const double ex = fmax(fabs(c.x - Gx) - hx, 0.0);
+          const double ey = fmax(fabs(c.y - Gy) - hy, 0.0);
+          const double ez = fmax(fabs(c.z - Gz) - hz, 0.0);
+          const double d2 = ex * ex + ey * ey + ez * ez;
+          if (c.w * c.w < d2) {
+            action = 1;
+          } else {
+            const int cnt = __ldg(&a.count[node]);
+            if (cnt <= a.bucket) {
+              action = 2;
+              pfirst = __ldg(&a.first[node]);
+              pcnt = cnt;
+            } else {
+              action = 3;
+            }
+          }
+        }
+      }
+      // far-field entries
+      const unsigned bm = __ballot_sync(0xffffffffu, action == 1);
+      if (action == 1) sm.m2p[(m2t + __popc(bm & lt)) & (kM2pRing - 1)] = node;
+      m2t += __popc(bm);
+      // particle entries
+      int ptot;
+      const int pex = warp_excl_scan(action == 2 ? pcnt : 0, lane, &ptot);
+      if (action == 2)
+        for (int k = 0; k < pcnt; ++k)
+          sm.p2p[(p2t + pex + k) & (kP2pRing - 1)] = pfirst + k;
+      p2t += ptot;
+      // opened twigs push their children (octant order)
+      int4 k0 = make_int4(-1, -1, -1, -1), k1 = k0;
+      if (action == 3) {
+        const int4* kk = reinterpret_cast<const int4*>(a.kids + 8 * (int64_t)node);
+        k0 = __ldg(kk);
+        k1 = __ldg(kk + 1);
+      }
+      const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+      int kc = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) kc += kv[j] >= 0 ? 1 : 0;
+      int ktot;
+      const int kex = warp_excl_scan(kc, lane, &ktot);
+      if (ssize + ktot > kStackCap) {
+        overflow = true;
+        break;
+      }
+      {
+        int pos = ssize + kex;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (kv[j] >= 0) stack[pos++] = kv[j];
+      }
+      ssize += ktot;
+      max_stack = max(max_stack, ssize);
+      __syncwarp();
+      while (p2t - p2h >= 32) {
+        eval_p2p<PHYS, RDF>(sm, p2h, 32, a, Gx, Gy, Gz, thx, thy, thz, tlx, tly,
+                            tlz, pt, tsp, act, lane, acc);
+        p2h += 32;
+        n_p2p += 32;
+      }
+      while (m2t - m2h >= 32) {
+        eval_m2p(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+        m2h += 32;
+        n_m2p += 32;
+      }
+    }
+    if (overflow) {
+      if (lane == 0) set_error(a.err, kErrWalk);
+      continue;
+    }
+    if (p2t > p2h) {
+      eval_p2p<PHYS, RDF>(sm, p2h, p2t - p2h, a, Gx, Gy, Gz, thx, thy, thz, tlx,
+                          tly, tlz, pt, tsp, act, lane, acc);
+      n_p2p += p2t - p2h;
+    }
+    if (m2t > m2h) {
+      eval_m2p(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+      n_m2p += m2t - m2h;
+    }
+    if (act) {
+      const double sc = tsp ? kEps : -kEps;  // eps * target charge
+      const int64_t o = a.order[pt];
+      a.f[3 * o] = sc * ((double)acc.sx - (double)acc.cx);
+      a.f[3 * o + 1] = sc * ((double)acc.sy - (double)acc.cy);
+      a.f[3 * o + 2] = sc * ((double)acc.sz - (double)acc.cz);
+      const double all = 0.5 * sc * acc.phi_all;
+      const double from_i = 0.5 * sc * acc.phi_ion;
+      // Epot_e = ee + ie + ei, Epot_i = ii (tree.f90:674-715)
+      a.epot_part[o] = tsp ? make_double2(all - from_i, from_i)
+                           : make_double2(all, 0.0);
+    }
+    if (lane == 0) {
+      atomicAdd(&a.counters[0], (unsigned long long)(n_m2p * n_act));
+      atomicAdd(&a.counters[1], (unsigned long long)(n_p2p * n_act));
+    }
+  }
+  if (lane == 0) atomicMax(&a.control[1], max_stack);
+}
+
+// ------------------------------------------------------------- memory ----
+template <class T>
+static int realloc_dev(T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, count * sizeof(T)) == cudaSuccess ? 0 : 1;
+}
+
+int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
+  mb.cap = cap;
+  int rc = 0;
+  rc |= realloc_dev(&mb.kids, 8 * (size_t)cap);
+  rc |= realloc_dev(&mb.first, (size_t)cap);
+  rc |= realloc_dev(&mb.count, (size_t)cap);
+  rc |= realloc_dev(&mb.digit, (size_t)cap);
+  rc |= realloc_dev(&mb.m64, 6 * (size_t)cap);
+  rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
+  return rc;
+}
+
+int mixed_alloc_particles(MixedBuffers& mb, int n) {
+  mb.n = n;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  mb.grid_warps = sms * kMaxBlocksPerSm * kMxWarps;
+  int rc = 0;
+  rc |= realloc_dev(&mb.xs, (size_t)n);
+  rc |= realloc_dev(&mb.groups, (size_t)n);
+  rc |= realloc_dev(&mb.stack, (size_t)mb.grid_warps * kStackCap);
+  rc |= realloc_dev(&mb.control, 4);
+  return rc;
+}
+
+void mixed_free(MixedBuffers& mb) {
+  void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
+                  mb.xs, mb.groups, mb.stack, mb.control};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  mb = MixedBuffers();
+}
+
+MixedNodes mixed_nodes(const MixedBuffers& mb) {
+  MixedNodes m;
+  m.kids = mb.kids;
+  m.first = mb.first;
+  m.count = mb.count;
+  m.digit = mb.digit;
+  m.m64 = mb.m64;
+  m.mom = mb.mom;
+  m.xs = mb.xs;
+  m.groups = mb.groups;
+  m.n_groups = mb.control + 2;
+  return m;
+}
+
+int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
+               int n, int n_el, const TreeView& tv, const WalkParams& wp,
+               const MixedTuning& tune, double* f, double2* epot_part,
+               uint32_t* rdf, unsigned long long* counters, int32_t* err,
+               cudaStream_t st) {
+  (void)x;
+  if (n == 0) return 0;
+  MixedArgs a;
+  a.node_c = tv.node_c;
+  a.mom = mb.mom;
+  a.kids = mb.kids;
+  a.first = mb.first;
+  a.count = mb.count;
+  a.xs = mb.xs;
+  a.order = b.vals;
+  a.bounds = tv.tree_bounds;
+  a.groups = mb.groups;
+  a.n_groups = mb.control + 2;
+  a.n = n;
+  a.n_el = n_el;
+  a.control = mb.control;
+  a.stack = mb.stack;
+  a.bucket = tune.bucket < 1 ? 1 : (tune.bucket > kMaxBucket ? kMaxBucket : tune.bucket);
+  a.physics = wp.physics;
+  a.inv_lam2_ee = (float)(1.0 / (wp.lam_ee * wp.lam_ee));
+  a.inv_lam2_ei = (float)(1.0 / (wp.lam_ei * wp.lam_ei));
+  a.inv_lam2_ii = (float)(1.0 / (wp.lam_ii * wp.lam_ii));
+  a.inv_lam_ee = (float)(1.0 / wp.lam_ee);
+  a.inv_lam_ei = (float)(1.0 / wp.lam_ei);
+  a.inv_lam_ii = (float)(1.0 / wp.lam_ii);
+  a.rs_inv = (float)(1.0 / wp.rs);
+  a.dx_ei_inv = 1.0 / wp.dx_ei;
+  a.dx_ii_inv = 1.0 / wp.dx_ii;
+  a.f = f;
+  a.epot_part = epot_part;
+  a.rdf = rdf;
+  a.counters = counters;
+  a.err = err;
+  // control[0] group cursor, [1] deepest stack; [2] (group count) is written
+  // by the build
+  cudaMemsetAsync(mb.control, 0, 2 * sizeof(int32_t), st);
+  int bps = tune.blocks_per_sm < 1 ? 1 : (tune.blocks_per_sm > kMaxBlocksPerSm ? kMaxBlocksPerSm : tune.blocks_per_sm);
+  int grid = (mb.grid_warps / (kMaxBlocksPerSm * kMxWarps)) * bps;
+  bool r = rdf != nullptr;
+  if (wp.physics == 1) {
+    if (r) k_walk_mixed<1, true><<<grid, kMxThreads, 0, st>>>(a);
+    else k_walk_mixed<1, false><<<grid, kMxThreads, 0, st>>>(a);
+  } else {
+    if (r) k_walk_mixed<0, true><<<grid, kMxThreads, 0, st>>>(a);
+    else k_walk_mixed<0, false><<<grid, kMxThreads, 0, st>>>(a);
+  }
+  return 1;
+}
+
+}  // namespace tg

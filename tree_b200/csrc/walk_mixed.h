@@ -9,29 +9,37 @@
 namespace tg {
 
 struct MixedBuffers {
-  int cap = 0;
-  int n = 0;
+  int cap = 0;       // node capacity of the arrays below
+  int n = 0;         // particles
+  int32_t* kids = nullptr;
+  int32_t* first = nullptr;
+  int32_t* count = nullptr;
+  int8_t* digit = nullptr;
+  double2* m64 = nullptr;
+  float4* mom = nullptr;
+  double4* xs = nullptr;
+  int2* groups = nullptr;
+  int32_t* stack = nullptr;    // per resident warp: kStackCap node indices
+  int32_t* control = nullptr;  // [0] group cursor, [1] max stack depth, [2] groups
+  int grid_warps = 0;
 };
 
-inline int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
-  mb.cap = cap;
-  return 0;
-}
-inline int mixed_alloc_particles(MixedBuffers& mb, int n) {
-  mb.n = n;
-  return 0;
-}
-inline void mixed_free(MixedBuffers&) {}
+// Tunables of the walk (picked by tree_b200/tune.py; defaults below).
+struct MixedTuning {
+  int bucket = 4;          // twigs with <= bucket particles are summed directly
+  int blocks_per_sm = 4;   // persistent grid: SMs x blocks_per_sm blocks
+};
 
-// Not built yet: flags a walk error so the caller fails loudly.
-inline void walk_mixed(MixedBuffers&, const BuildBuffers& b, const double*,
-                       int, int, const TreeView&, const WalkParams&, int, int,
-                       double*, double2*, uint32_t*, unsigned long long*,
-                       int32_t* err, cudaStream_t st) {
-  (void)b;
-  int32_t bit = kErrWalk;
-  cudaMemcpyAsync(err, &bit, sizeof(bit), cudaMemcpyHostToDevice, st);
-  cudaStreamSynchronize(st);
-}
+int mixed_alloc_nodes(MixedBuffers& mb, int cap);
+int mixed_alloc_particles(MixedBuffers& mb, int n);
+void mixed_free(MixedBuffers& mb);
+MixedNodes mixed_nodes(const MixedBuffers& mb);
+
+// Forces on every particle from both trees.  Returns kernels launched.
+int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
+               int n, int n_el, const TreeView& tv, const WalkParams& wp,
+               const MixedTuning& tune, double* f, double2* epot_part,
+               uint32_t* rdf, unsigned long long* counters, int32_t* err,
+               cudaStream_t st);
 
 }  // namespace tg
