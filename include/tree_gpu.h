@@ -90,6 +90,8 @@ typedef struct tree_gpu_timing {
   int64_t n_nodes;   /* nodes of both trees, last build */
   int64_t calls;
   int64_t launches;  /* kernels this library launched (cumulative) */
+  int64_t n_mac_net;       /* cells the learned MAC evaluated, last call */
+  int64_t n_mac_fallback;  /* of those, outside the training range (fixed theta) */
 } tree_gpu_timing;
 
 typedef struct tree_gpu_handle tree_gpu_handle;
@@ -197,6 +199,51 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
  * reference; set by the autotuner (tree_b200/tune.py). */
 int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
                         int32_t blocks_per_sm);
+
+/* ---- learned multipole acceptance criterion (no counterpart in the
+ * reference, whose criterion is the fixed s/theta + dx < r of tree.f90:743).
+ * A 16 -> 64 -> 64 -> 1 network predicts log10 of the error of accepting a
+ * cell for a target group, relative to the cell's gross monopole field; in the
+ * band rho_lo <= s/(d - dx) <= rho_hi the mixed walk accepts a cell when the
+ * predicted error is at most eta * (smallest |F| of the group at the previous
+ * step), and uses the fixed-theta test elsewhere or when the features fall
+ * outside the training range.  Active when precision = MIXED and mac =
+ * LEARNED and a model is loaded. */
+#define TREE_GPU_MLP_PARAMS 5313 /* W1[16][64] b1[64] W2[64][64] b2[64] w3[64] b3 */
+#define TREE_GPU_MLP_STATS 64    /* feature mean[16], 1/std[16], min[16], max[16] */
+
+/* Walks the combined tree of the current device positions with a fixed
+ * theta drawn per target group from [theta_lo, theta_hi] and appends one
+ * training sample (16 features, label, and (theta, rho)) per tested cell in
+ * the band [rho_lo, rho_hi] holding at most max_count particles; the label
+ * is the exact FP64 error of accepting it.  The sample buffer holds `cap`
+ * samples (reallocated, and emptied, when cap changes); *n_total receives
+ * the number held. */
+int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
+                         double rho_lo, double rho_hi, int32_t max_count,
+                         uint64_t seed, int64_t cap, int64_t* n_total);
+/* Copies the collected samples out (NULL buffers: count only). */
+int tree_gpu_mac_samples(tree_gpu_handle* h, float* feats, float* labels,
+                         float* extra, int64_t cap, int64_t* n);
+int tree_gpu_mac_clear(tree_gpu_handle* h);
+/* Trains the network from scratch on the collected samples with the
+ * BF16 tensor-core kernels (pinball loss at quantile tau, Adam, cosine decay)
+ * and loads it; loss_per_epoch (epochs floats) may be NULL. */
+int tree_gpu_mac_train(tree_gpu_handle* h, int32_t epochs, int32_t batch,
+                       float lr, float tau, uint64_t seed,
+                       float* loss_per_epoch);
+int tree_gpu_mac_set_model(tree_gpu_handle* h, const float* params,
+                           const float* stats);
+int tree_gpu_mac_get_model(tree_gpu_handle* h, float* params, float* stats);
+int tree_gpu_mac_config(tree_gpu_handle* h, float eta, float rho_lo,
+                        float rho_hi);
+/* Stand-alone network kernels (host buffers, device scratch per call), used to
+ * check gradients and inference against a CPU implementation. */
+int tree_gpu_mlp_grad(const float* X, const float* y, int64_t n,
+                      const float* params, float tau, float* grad,
+                      float* loss);
+int tree_gpu_mlp_infer(const float* X, int64_t n, const float* params,
+                       const float* stats, float* y);
 
 int tree_gpu_timings(tree_gpu_handle* h, tree_gpu_timing* out);
 const char* tree_gpu_last_error(tree_gpu_handle* h);

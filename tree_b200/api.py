@@ -29,9 +29,13 @@ RDF_BINS = 10001
 
 # Every symbol include/tree_gpu.h declares.
 EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
-           "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step", "tree_gpu_get_state",
-           "tree_gpu_direct", "tree_gpu_direct_static", "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning", "tree_gpu_timings",
-           "tree_gpu_last_error",
+           "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step",
+           "tree_gpu_get_state", "tree_gpu_direct", "tree_gpu_direct_static",
+           "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning",
+           "tree_gpu_mac_collect", "tree_gpu_mac_samples", "tree_gpu_mac_clear",
+           "tree_gpu_mac_train", "tree_gpu_mac_set_model",
+           "tree_gpu_mac_get_model", "tree_gpu_mac_config", "tree_gpu_mlp_grad",
+           "tree_gpu_mlp_infer", "tree_gpu_timings", "tree_gpu_last_error",
            "tree_gpu_destroy", "tree_gpu_version")
 
 
@@ -56,7 +60,8 @@ class Timing(ctypes.Structure):
                 ("ms_kdk", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("n_m2p", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
                 ("n_nodes", ctypes.c_int64), ("calls", ctypes.c_int64),
-                ("launches", ctypes.c_int64)]
+                ("launches", ctypes.c_int64), ("n_mac_net", ctypes.c_int64),
+                ("n_mac_fallback", ctypes.c_int64)]
 
 
 class TreeGpuError(RuntimeError):
@@ -95,6 +100,21 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.c_int64, vp, vp, vp]
     L.tree_gpu_set_stream.argtypes = [vp, vp]
     L.tree_gpu_set_tuning.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.tree_gpu_mac_collect.argtypes = [vp, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int32, ctypes.c_uint64,
+                                       ctypes.c_int64, lp]
+    L.tree_gpu_mac_samples.argtypes = [vp, fp, fp, fp, ctypes.c_int64, lp]
+    L.tree_gpu_mac_clear.argtypes = [vp]
+    L.tree_gpu_mac_train.argtypes = [vp, ctypes.c_int32, ctypes.c_int32,
+                                     ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_uint64, fp]
+    L.tree_gpu_mac_set_model.argtypes = [vp, fp, fp]
+    L.tree_gpu_mac_get_model.argtypes = [vp, fp, fp]
+    L.tree_gpu_mac_config.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+    L.tree_gpu_mlp_grad.argtypes = [fp, fp, ctypes.c_int64, fp, ctypes.c_float, fp, fp]
+    L.tree_gpu_mlp_infer.argtypes = [fp, ctypes.c_int64, fp, fp, fp]
     L.tree_gpu_timings.argtypes = [vp, ctypes.POINTER(Timing)]
     L.tree_gpu_last_error.argtypes = [vp]
     L.tree_gpu_last_error.restype = ctypes.c_char_p
@@ -104,6 +124,40 @@ def load_library(path: str = LIB_PATH):
         getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int
     _lib = L
     return L
+
+
+MLP_PARAMS = 5313
+MLP_STATS = 64
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mlp_grad(X, y, params, tau=0.9):
+    """Device gradient of the mean pinball loss (tree_gpu_mlp_grad)."""
+    L = load_library()
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    p = np.ascontiguousarray(params, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    rc = L.tree_gpu_mlp_grad(_fp(X), _fp(y), len(X), _fp(p), tau, _fp(g), _fp(loss))
+    if rc != OK:
+        raise TreeGpuError(rc, "tree_gpu_mlp_grad")
+    return float(loss[0]), g
+
+
+def mlp_infer(X, params, stats):
+    """Device inference of the packed network on raw features."""
+    L = load_library()
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.zeros(len(X), np.float32)
+    rc = L.tree_gpu_mlp_infer(_fp(X), len(X), _fp(np.ascontiguousarray(params, np.float32)),
+                              _fp(np.ascontiguousarray(stats, np.float32)), _fp(y))
+    if rc != OK:
+        raise TreeGpuError(rc, "tree_gpu_mlp_infer")
+    return y
 
 
 def _dp(a):
@@ -265,6 +319,51 @@ class TreeForce:
 
     def set_tuning(self, bucket: int = 4, blocks_per_sm: int = 4):
         self._check(self.lib.tree_gpu_set_tuning(self.h, bucket, blocks_per_sm))
+
+    # ---- learned MAC ----
+    def mac_collect(self, theta_lo=0.2, theta_hi=0.9, rho_lo=0.2, rho_hi=0.9,
+                    max_count=16384, seed=1, cap=1 << 22):
+        n = ctypes.c_int64()
+        self._check(self.lib.tree_gpu_mac_collect(self.h, theta_lo, theta_hi,
+                                                  rho_lo, rho_hi, max_count,
+                                                  seed, cap, ctypes.byref(n)))
+        return n.value
+
+    def mac_samples(self):
+        n = ctypes.c_int64()
+        self._check(self.lib.tree_gpu_mac_samples(self.h, None, None, None, 0, ctypes.byref(n)))
+        m = n.value
+        f = np.zeros((m, 16), np.float32)
+        y = np.zeros(m, np.float32)
+        e = np.zeros((m, 2), np.float32)
+        if m:
+            self._check(self.lib.tree_gpu_mac_samples(self.h, _fp(f), _fp(y), _fp(e), m,
+                                                      ctypes.byref(n)))
+        return f, y, e
+
+    def mac_clear(self):
+        self._check(self.lib.tree_gpu_mac_clear(self.h))
+
+    def mac_train(self, epochs=8, batch=8192, lr=2e-3, tau=0.9, seed=1):
+        losses = np.zeros(epochs, np.float32)
+        self._check(self.lib.tree_gpu_mac_train(self.h, epochs, batch, lr, tau, seed,
+                                                _fp(losses)))
+        return losses
+
+    def mac_set_model(self, params, stats):
+        p = np.ascontiguousarray(params, np.float32)
+        s = np.ascontiguousarray(stats, np.float32)
+        assert p.size == MLP_PARAMS and s.size == MLP_STATS
+        self._check(self.lib.tree_gpu_mac_set_model(self.h, _fp(p), _fp(s)))
+
+    def mac_get_model(self):
+        p = np.zeros(MLP_PARAMS, np.float32)
+        s = np.zeros(MLP_STATS, np.float32)
+        self._check(self.lib.tree_gpu_mac_get_model(self.h, _fp(p), _fp(s)))
+        return p, s
+
+    def mac_config(self, eta=1e-5, rho_lo=0.2, rho_hi=0.9):
+        self._check(self.lib.tree_gpu_mac_config(self.h, eta, rho_lo, rho_hi))
 
     def timings(self) -> Timing:
         t = Timing()

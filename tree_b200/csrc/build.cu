@@ -733,6 +733,7 @@ __global__ void k_upward_net(const double* __restrict__ x,
     f[0] = make_float4((float)q, 0.f, 0.f, 0.f);
     f[1] = make_float4(0.f, 0.f, 0.f, 0.f);
     f[2] = make_float4(0.f, 0.f, 0.f, ion ? 1.f : 0.f);
+    mx.geom[leaf] = make_float4(0.f, 0.f, 1.f, 0.f);
     mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
   }
   __threadfence();
@@ -811,6 +812,7 @@ __global__ void k_upward_net(const double* __restrict__ x,
     f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
     f[1] = make_float4((float)Sxx, (float)Syy, (float)Szz, (float)Sxy);
     f[2] = make_float4((float)Syz, (float)Szx, (float)(Sxx + Syy + Szz), (float)qi);
+    mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, 0.f);
     __threadfence();
     cur = node_parent[cur];
   }

@@ -15,6 +15,7 @@ struct MixedNodes {
   int8_t* digit;     // octant of the node inside its parent
   double2* m64;      // 6 per node: (n, Q) (Dx, Dy) (Dz, q_ion) (Sxx, Syy) (Szz, Sxy) (Syz, Szx)
   float4* mom;       // 3 per node: (Q, Dx, Dy, Dz) (Sxx, Syy, Szz, Sxy) (Syz, Szx, trS, q_ion)
+  float4* geom;      // per node: (box side s, |centroid - box centre|, n, 0)
   double4* xs;       // per sorted particle: position, w = 1 for ions
   int2* groups;      // target groups (first sorted particle, count)
   int32_t* n_groups; // device count of groups

@@ -15,6 +15,7 @@
 #include "direct.h"
 #include "internal.cuh"
 #include "kdk.h"
+#include "mlp.h"
 #include "walk.h"
 #include "walk_mixed.h"
 
@@ -52,6 +53,18 @@ struct tree_gpu_handle {
   tg::BuildBuffers b{};
   tg::MixedBuffers mb{};
   tg::MixedTuning tune{};
+  // learned MAC
+  float* mlp_params = nullptr;   // kMlpParams FP32 master parameters
+  float* mlp_stats = nullptr;    // mean[16] inv_std[16] fmin[16] fmax[16]
+  tg::MlpPacked* mlp_packed = nullptr;
+  bool has_model = false;
+  bool has_fprev = false;        // h->f holds forces of the current positions' predecessor
+  float mac_eta = 1e-5f, mac_rho_lo = 0.2f, mac_rho_hi = 0.9f;
+  float* smp_feats = nullptr;    // collected training samples
+  float* smp_labels = nullptr;
+  float* smp_extra = nullptr;
+  int32_t* smp_count = nullptr;
+  int64_t smp_cap = 0;
   uint32_t* rdf = nullptr;
   unsigned long long* counters = nullptr;
   double* partial = nullptr;
@@ -156,7 +169,7 @@ int alloc_all(tree_gpu_handle* h) {
   if ((rc = dalloc(h, &b.bounds, 4))) return rc;
   if ((rc = dalloc(h, &b.err, 1))) return rc;
   if ((rc = dalloc(h, &h->rdf, 2 * (size_t)tg::kRdfBins))) return rc;
-  if ((rc = dalloc(h, &h->counters, 2))) return rc;
+  if ((rc = dalloc(h, &h->counters, 4))) return rc;
   if ((rc = dalloc(h, &h->partial, 4 * (size_t)tg::kdk_partials_needed(n) + 4)))
     return rc;
   if ((rc = dalloc(h, &h->diag, 8))) return rc;
@@ -175,7 +188,8 @@ void free_all(tree_gpu_handle* h) {
                   b.bbox, b.geom, b.bounds, b.err, b.node_c, b.node_m,
                   b.node_skip, b.node_pt, b.node_parent, b.node_nchild,
                   b.node_done, b.node_level, h->rdf, h->counters, h->partial,
-                  h->diag};
+                  h->diag, h->mlp_params, h->mlp_stats, h->mlp_packed,
+                  h->smp_feats, h->smp_labels, h->smp_extra, h->smp_count};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   tg::mixed_free(h->mb);
@@ -221,7 +235,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
   h->timing.launches +=
       tg::build_trees(h->b, h->x, h->n, (int)h->n_el, h->prm.theta, mode, st);
   if (ev) cudaEventRecord(ev->e[1], st);
-  cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), st);
+  cudaMemsetAsync(h->counters, 0, 4 * sizeof(unsigned long long), st);
   if (with_rdf)
     cudaMemsetAsync(h->rdf, 0, 2 * sizeof(uint32_t) * tg::kRdfBins, st);
   tg::TreeView tv = tree_view(h);
@@ -231,9 +245,21 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
                h->epot_part, with_rdf ? h->rdf : nullptr, h->counters,
                h->b.err, st);
   } else {
+    tg::LearnedMac lm;
+    const bool use_learned = h->prm.mac == TREE_GPU_MAC_LEARNED && h->has_model &&
+                             h->has_fprev;
+    if (use_learned) {
+      lm.packed = h->mlp_packed;
+      lm.fmin = h->mlp_stats + 32;
+      lm.fmax = h->mlp_stats + 48;
+      lm.f_prev = h->f;  // each target's previous force, read before it is overwritten
+      lm.eta = h->mac_eta;
+      lm.rho_lo = h->mac_rho_lo;
+      lm.rho_hi = h->mac_rho_hi;
+    }
     tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp, h->tune,
-                   h->f, h->epot_part, with_rdf ? h->rdf : nullptr,
-                   h->counters, h->b.err, st);
+                   use_learned ? &lm : nullptr, h->f, h->epot_part,
+                   with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
   }
   if (ev) cudaEventRecord(ev->e[2], st);
   h->timing.launches += (h->n > 0 ? 1 : 0) + 2;  // walk + epot partial/sum
@@ -274,10 +300,12 @@ int grow_nodes(tree_gpu_handle* h) {
 }
 
 void read_counters(tree_gpu_handle* h) {
-  unsigned long long c[2] = {0, 0};
+  unsigned long long c[4] = {0, 0, 0, 0};
   cudaMemcpy(c, h->counters, sizeof(c), cudaMemcpyDeviceToHost);
   h->timing.n_m2p = (int64_t)c[0];
   h->timing.n_p2p = (int64_t)c[1];
+  h->timing.n_mac_net = (int64_t)c[2];
+  h->timing.n_mac_fallback = (int64_t)c[3];
 }
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
@@ -373,7 +401,17 @@ int tree_gpu_force(tree_gpu_handle* h, const double* x_el, const double* x_ion,
   if (bi)
     CK(cudaMemcpyAsync(h->x + 3 * h->n_el, x_ion, bi, cudaMemcpyHostToDevice, h->st));
   bool with_rdf = rdf_ei || rdf_ii;
-  int rc = force_device(h, with_rdf);
+  int rc;
+  if (h->prm.mac == TREE_GPU_MAC_LEARNED && h->prm.precision == TREE_GPU_PREC_MIXED) {
+    // new positions: a fixed-theta pass gives the force magnitudes the learned
+    // criterion budgets against, then the learned pass
+    h->has_fprev = false;
+    if ((rc = force_device(h, false))) return rc;
+    h->has_fprev = true;
+  }
+  rc = force_device(h, with_rdf);
+  h->has_fprev = false;
+  h->has_state = false;  // the device positions are now this call's, not a state
   if (rc) return rc;
   if (be) CK(cudaMemcpyAsync(f_el, h->f, be, cudaMemcpyDeviceToHost, h->st));
   if (bi)
@@ -414,9 +452,11 @@ int tree_gpu_set_state(tree_gpu_handle* h, const double* x_el,
     CK(cudaMemcpyAsync(h->x + 3 * h->n_el, x_ion, bi, cudaMemcpyHostToDevice, h->st));
     CK(cudaMemcpyAsync(h->v + 3 * h->n_el, v_ion, bi, cudaMemcpyHostToDevice, h->st));
   }
+  h->has_fprev = false;  // initial forces with the fixed-theta test
   int rc = force_device(h, false);
   if (rc) return rc;
   h->has_state = true;
+  h->has_fprev = true;
   return TREE_GPU_OK;
 }
 
@@ -442,6 +482,7 @@ int tree_gpu_load_state(tree_gpu_handle* h, const double* x_el,
     CK(cudaMemcpyAsync(h->f + oi, f_ion, bi, cudaMemcpyHostToDevice, h->st));
   }
   h->has_state = true;
+  h->has_fprev = true;
   return TREE_GPU_OK;
 }
 
@@ -654,5 +695,227 @@ int tree_gpu_destroy(tree_gpu_handle* h) {
 }
 
 const char* tree_gpu_version(void) { return TREE_GPU_VERSION_STR; }
+
+}  // extern "C"
+
+// ------------------------------------------------------- learned MAC ----
+namespace {
+
+int ensure_model_buffers(tree_gpu_handle* h) {
+  if (h->mlp_params) return TREE_GPU_OK;
+  CK(cudaMalloc(&h->mlp_params, sizeof(float) * tg::kMlpParams));
+  CK(cudaMalloc(&h->mlp_stats, sizeof(float) * 64));
+  CK(cudaMalloc(&h->mlp_packed, sizeof(tg::MlpPacked)));
+  return TREE_GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
+                         double rho_lo, double rho_hi, int32_t max_count,
+                         uint64_t seed, int64_t cap, int64_t* n_total) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (!(theta_lo > 0 && theta_hi >= theta_lo && rho_lo > 0 && rho_hi >= rho_lo) ||
+      cap <= 0 || cap > (int64_t)0x7fffffff || max_count < 2)
+    return fail(h, TREE_GPU_ERR_ARG, "bad sampling arguments");
+  if (h->n == 0) return fail(h, TREE_GPU_ERR_STATE, "no particles");
+  if (h->smp_cap != cap) {
+    if (h->smp_feats) cudaFree(h->smp_feats);
+    if (h->smp_labels) cudaFree(h->smp_labels);
+    if (h->smp_extra) cudaFree(h->smp_extra);
+    if (h->smp_count) cudaFree(h->smp_count);
+    h->smp_feats = h->smp_labels = h->smp_extra = nullptr;
+    h->smp_count = nullptr;
+    CK(cudaMalloc(&h->smp_feats, sizeof(float) * 16 * (size_t)cap));
+    CK(cudaMalloc(&h->smp_labels, sizeof(float) * (size_t)cap));
+    CK(cudaMalloc(&h->smp_extra, sizeof(float) * 2 * (size_t)cap));
+    CK(cudaMalloc(&h->smp_count, sizeof(int32_t) * 2));
+    CK(cudaMemsetAsync(h->smp_count, 0, sizeof(int32_t) * 2, h->st));
+    h->smp_cap = cap;
+  }
+  // combined tree of the current device positions
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    h->timing.launches += tg::build_trees(h->b, h->x, h->n, (int)h->n_el,
+                                          h->prm.theta, 1, h->st);
+    bool grow = false;
+    int rc = check_device_status(h, &grow);
+    if (rc) return rc;
+    if (!grow) break;
+    if ((rc = grow_nodes(h))) return rc;
+    if (attempt == 2) return fail(h, TREE_GPU_ERR_CAPACITY, "capacity");
+  }
+  tg::SampleArgs a;
+  a.node_c = h->b.node_c;
+  a.mom = h->mb.mom;
+  a.geom = h->mb.geom;
+  a.m64 = h->mb.m64;
+  a.kids = h->mb.kids;
+  a.first = h->mb.first;
+  a.count = h->mb.count;
+  a.xs = h->mb.xs;
+  a.groups = h->mb.groups;
+  a.n_groups = h->mb.control + 2;
+  a.cursor = h->smp_count + 1;
+  a.stack = h->mb.stack;
+  a.theta_lo = (float)theta_lo;
+  a.theta_hi = (float)theta_hi;
+  a.rho_lo = (float)rho_lo;
+  a.rho_hi = (float)rho_hi;
+  a.seed = (uint32_t)(seed ^ (seed >> 32));
+  a.max_count = max_count;
+  a.lam_ei = (float)h->lam[1];
+  a.feats = h->smp_feats;
+  a.labels = h->smp_labels;
+  a.extra = h->smp_extra;
+  a.n_out = h->smp_count;
+  a.cap = (int)cap;
+  a.err = h->b.err;
+  h->timing.launches += tg::mac_sample(a, h->mb.grid_warps, h->st);
+  CK(cudaGetLastError());
+  int32_t cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, h->smp_count, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+  bool grow = false;
+  int rc = check_device_status(h, &grow);
+  if (rc) return rc;
+  if (n_total) *n_total = cnt < cap ? cnt : cap;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mac_samples(tree_gpu_handle* h, float* feats, float* labels,
+                         float* extra, int64_t cap, int64_t* n) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  int32_t cnt = 0;
+  if (h->smp_count)
+    CK(cudaMemcpy(&cnt, h->smp_count, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  int64_t m = cnt < h->smp_cap ? cnt : h->smp_cap;
+  if (n) *n = m;
+  if (!feats && !labels && !extra) return TREE_GPU_OK;
+  if (cap < m) return fail(h, TREE_GPU_ERR_ARG, "buffer too small");
+  if (m == 0) return TREE_GPU_OK;
+  if (feats) CK(cudaMemcpy(feats, h->smp_feats, sizeof(float) * 16 * m, cudaMemcpyDeviceToHost));
+  if (labels) CK(cudaMemcpy(labels, h->smp_labels, sizeof(float) * m, cudaMemcpyDeviceToHost));
+  if (extra) CK(cudaMemcpy(extra, h->smp_extra, sizeof(float) * 2 * m, cudaMemcpyDeviceToHost));
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mac_clear(tree_gpu_handle* h) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (h->smp_count) CK(cudaMemset(h->smp_count, 0, sizeof(int32_t) * 2));
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mac_train(tree_gpu_handle* h, int32_t epochs, int32_t batch,
+                       float lr, float tau, uint64_t seed,
+                       float* loss_per_epoch) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  int64_t m = 0;
+  int rc = tree_gpu_mac_samples(h, nullptr, nullptr, nullptr, 0, &m);
+  if (rc) return rc;
+  if (m < 64) return fail(h, TREE_GPU_ERR_STATE, "collect samples first");
+  if (epochs <= 0 || batch <= 0 || !(lr > 0) || !(tau > 0 && tau < 1))
+    return fail(h, TREE_GPU_ERR_ARG, "bad training arguments");
+  if ((rc = ensure_model_buffers(h))) return rc;
+  int e = tg::mlp_train(h->smp_feats, h->smp_labels, (int)m, epochs, batch, lr,
+                        tau, seed, h->mlp_params, h->mlp_stats, loss_per_epoch,
+                        h->st);
+  if (e) return fail(h, TREE_GPU_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+  h->timing.launches += tg::mlp_pack(h->mlp_params, h->mlp_stats, h->mlp_stats + 16,
+                                     h->mlp_packed, h->st);
+  CK(cudaStreamSynchronize(h->st));
+  h->has_model = true;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mac_set_model(tree_gpu_handle* h, const float* params,
+                           const float* stats) {
+  if (!h || !params || !stats) return TREE_GPU_ERR_ARG;
+  int rc = ensure_model_buffers(h);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->mlp_params, params, sizeof(float) * tg::kMlpParams,
+                     cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->mlp_stats, stats, sizeof(float) * 64, cudaMemcpyHostToDevice, h->st));
+  h->timing.launches += tg::mlp_pack(h->mlp_params, h->mlp_stats, h->mlp_stats + 16,
+                                     h->mlp_packed, h->st);
+  CK(cudaStreamSynchronize(h->st));
+  h->has_model = true;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mac_get_model(tree_gpu_handle* h, float* params, float* stats) {
+  if (!h || !params || !stats) return TREE_GPU_ERR_ARG;
+  if (!h->has_model) return fail(h, TREE_GPU_ERR_STATE, "no model");
+  CK(cudaMemcpy(params, h->mlp_params, sizeof(float) * tg::kMlpParams, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(stats, h->mlp_stats, sizeof(float) * 64, cudaMemcpyDeviceToHost));
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mac_config(tree_gpu_handle* h, float eta, float rho_lo, float rho_hi) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (!(eta > 0) || !(rho_lo > 0) || !(rho_hi >= rho_lo))
+    return fail(h, TREE_GPU_ERR_ARG, "bad learned-MAC configuration");
+  h->mac_eta = eta;
+  h->mac_rho_lo = rho_lo;
+  h->mac_rho_hi = rho_hi;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_mlp_grad(const float* X, const float* Y, int64_t n,
+                      const float* params, float tau, float* grad, float* loss) {
+  if (!X || !Y || !params || !grad || !loss || n <= 0 || n > 0x7fffffff)
+    return TREE_GPU_ERR_ARG;
+  float *dX = nullptr, *dY = nullptr, *dP = nullptr, *dG = nullptr, *dL = nullptr;
+  cudaError_t e = cudaSuccess;
+  auto al = [&](float** q, size_t cnt) { if (e == cudaSuccess) e = cudaMalloc(q, cnt * sizeof(float)); };
+  al(&dX, 16 * (size_t)n);
+  al(&dY, (size_t)n);
+  al(&dP, tg::kMlpParams);
+  al(&dG, tg::kMlpParams);
+  al(&dL, 1);
+  if (e == cudaSuccess) {
+    cudaMemcpy(dX, X, sizeof(float) * 16 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dY, Y, sizeof(float) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dP, params, sizeof(float) * tg::kMlpParams, cudaMemcpyHostToDevice);
+    cudaMemset(dG, 0, sizeof(float) * tg::kMlpParams);
+    cudaMemset(dL, 0, sizeof(float));
+    tg::mlp_grad(dX, dY, (int)n, dP, tau, dG, dL, 64, 0);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) {
+      cudaMemcpy(grad, dG, sizeof(float) * tg::kMlpParams, cudaMemcpyDeviceToHost);
+      cudaMemcpy(loss, dL, sizeof(float), cudaMemcpyDeviceToHost);
+    }
+  }
+  float* all[] = {dX, dY, dP, dG, dL};
+  for (float* q : all) if (q) cudaFree(q);
+  return e == cudaSuccess ? TREE_GPU_OK : TREE_GPU_ERR_CUDA;
+}
+
+int tree_gpu_mlp_infer(const float* X, int64_t n, const float* params,
+                       const float* stats, float* y) {
+  if (!X || !params || !stats || !y || n <= 0 || n > 0x7fffffff) return TREE_GPU_ERR_ARG;
+  float *dX = nullptr, *dP = nullptr, *dS = nullptr, *dY = nullptr;
+  tg::MlpPacked* dK = nullptr;
+  cudaError_t e = cudaSuccess;
+  auto al = [&](float** q, size_t cnt) { if (e == cudaSuccess) e = cudaMalloc(q, cnt * sizeof(float)); };
+  al(&dX, 16 * (size_t)n);
+  al(&dP, tg::kMlpParams);
+  al(&dS, 64);
+  al(&dY, (size_t)n);
+  if (e == cudaSuccess) e = cudaMalloc(&dK, sizeof(tg::MlpPacked));
+  if (e == cudaSuccess) {
+    cudaMemcpy(dX, X, sizeof(float) * 16 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dP, params, sizeof(float) * tg::kMlpParams, cudaMemcpyHostToDevice);
+    cudaMemcpy(dS, stats, sizeof(float) * 64, cudaMemcpyHostToDevice);
+    tg::mlp_pack(dP, dS, dS + 16, dK, 0);
+    tg::mlp_infer(dX, (int)n, dK, dY, 0);
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) cudaMemcpy(y, dY, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  }
+  float* all[] = {dX, dP, dS, dY};
+  for (float* q : all) if (q) cudaFree(q);
+  if (dK) cudaFree(dK);
+  return e == cudaSuccess ? TREE_GPU_OK : TREE_GPU_ERR_CUDA;
+}
 
 }  // extern "C"

@@ -1,0 +1,82 @@
+// mac.cuh -- features of a (target group, cell) pair for the learned
+// multipole acceptance criterion, shared by the sampling walk (training data)
+// and the mixed walk (inference) so both see identical inputs.
+//
+// All 16 features are dimensionless.  With X the cell centroid, d the
+// distance from X to the group's bounding box, u the unit vector from X to
+// the group centre, s the cell's box side, dx = |X - geometric centre|, n the
+// particle count, Q/D/S the net monopole/dipole/second moment and q_ion the
+// ion count:
+//   0 s/d            1 dx/d              2 |h|/d (group half-diagonal)
+//   3 log2(n)/16     4 Q/n               5 |D|/(n s)
+//   6 |S|_F/(n s^2)  7 tr S/(n s^2)      8 q_ion/n (species mix)
+//   9 D.u/(n s)      10 u.S.u/(n s^2)    11 log10(lambda_ei/d)/8
+//   12 group fill    13 |G-X|/d - 1      14 log10(s/d)
+//   15 |D|/(|Q| s + |D|)
+// The label is log10(max over the group of |F_multipole - F_exact| /
+// (n / d^2)), i.e. the acceptance error relative to the cell's gross
+// monopole field (charges in units of e, Coulomb constant dropped).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "mlp.cuh"
+
+namespace tg {
+
+constexpr int kMacFeatures = kMlpIn;  // 16
+
+struct CellGeom {   // mx.geom: (s, dx, n, -)
+  float s, dx, n, pad;
+};
+
+__device__ __forceinline__ void mac_features(
+    double cx, double cy, double cz, const float4 g4, const float4 m0,
+    const float4 m1, const float4 m2, double Gx, double Gy, double Gz,
+    float hlen, float d, float n_act, float lam_ei, float f[kMacFeatures]) {
+  const float s = g4.x, dxo = g4.y, n = g4.z;
+  const float Q = m0.x, Dx = m0.y, Dy = m0.z, Dz = m0.w;
+  const float Sxx = m1.x, Syy = m1.y, Szz = m1.z, Sxy = m1.w;
+  const float Syz = m2.x, Szx = m2.y, trS = m2.z, qi = m2.w;
+  const float ux0 = (float)(Gx - cx), uy0 = (float)(Gy - cy), uz0 = (float)(Gz - cz);
+  const float ul = sqrtf(ux0 * ux0 + uy0 * uy0 + uz0 * uz0);
+  const float iu = ul > 0.f ? 1.f / ul : 0.f;
+  const float ux = ux0 * iu, uy = uy0 * iu, uz = uz0 * iu;
+  const float id = 1.f / d;
+  const float ns = n * s, ns2 = n * s * s;
+  const float Dn = sqrtf(Dx * Dx + Dy * Dy + Dz * Dz);
+  const float SF = sqrtf(Sxx * Sxx + Syy * Syy + Szz * Szz +
+                         2.f * (Sxy * Sxy + Syz * Syz + Szx * Szx));
+  const float Du = Dx * ux + Dy * uy + Dz * uz;
+  const float Sux = Sxx * ux + Sxy * uy + Szx * uz;
+  const float Suy = Sxy * ux + Syy * uy + Syz * uz;
+  const float Suz = Szx * ux + Syz * uy + Szz * uz;
+  const float uSu = ux * Sux + uy * Suy + uz * Suz;
+  f[0] = s * id;
+  f[1] = dxo * id;
+  f[2] = hlen * id;
+  f[3] = log2f(n) * (1.f / 16.f);
+  f[4] = Q / n;
+  f[5] = Dn / ns;
+  f[6] = SF / ns2;
+  f[7] = trS / ns2;
+  f[8] = qi / n;
+  f[9] = Du / ns;
+  f[10] = uSu / ns2;
+  f[11] = fmaxf(log10f(lam_ei * id), -8.f) * 0.125f;
+  f[12] = n_act * (1.f / 32.f);
+  f[13] = ul * id - 1.f;
+  f[14] = log10f(s * id);
+  f[15] = Dn / (fabsf(Q) * s + Dn + 1e-30f);
+}
+
+// Distance from a point to an axis-aligned box (centre G, half extents h).
+__device__ __forceinline__ double dist_to_box(double cx, double cy, double cz,
+                                              double Gx, double Gy, double Gz,
+                                              double hx, double hy, double hz) {
+  const double ex = fmax(fabs(cx - Gx) - hx, 0.0);
+  const double ey = fmax(fabs(cy - Gy) - hy, 0.0);
+  const double ez = fmax(fabs(cz - Gz) - hz, 0.0);
+  return sqrt(ex * ex + ey * ey + ez * ez);
+}
+
+}  // namespace tg

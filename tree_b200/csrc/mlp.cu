@@ -1,0 +1,466 @@
+// mlp.cu -- training of the learned-MAC network with BF16 tensor-core mma.
+//
+// k_mlp_grad: forward and backward of the pinball (quantile) loss for a
+// mini-batch.  Each warp takes 32 samples at a time:
+//   Z1 = X W1 + b1          (mma: 2 x 8 tiles, K = 16)
+//   Z2 = relu(Z1) W2 + b2   (mma: 2 x 8 tiles, K = 64)
+//   y  = relu(Z2) . w3 + b3 (FP32)
+//   dW2 = relu(Z1)^T dZ2    (mma: 4 x 8 tiles, K = 32)
+//   dH1 = dZ2 W2^T          (mma: 2 x 8 tiles, K = 64)
+//   dW1 = X^T dZ1           (mma: 1 x 8 tiles, K = 32)
+// Gradients are accumulated in shared memory per block and added to the
+// global gradient once per block; k_mlp_adam applies Adam to the FP32 master
+// parameters.  The operands the mma instructions read are rounded to BF16;
+// everything else is FP32 (oracle/mlp.py emulates the same roundings).
+#include <cstdio>
+#include "internal.cuh"
+#include "mlp.cuh"
+#include "mlp.h"
+
+namespace tg {
+
+constexpr int kMlpWarps = 4;
+constexpr int kMlpThreads = 32 * kMlpWarps;
+
+struct MlpWarpSmem {
+  float x[32 * kMlpIn];
+  float z1[32 * kMlpH];
+  float z2[32 * kMlpH];
+};
+
+__global__ void __launch_bounds__(kMlpThreads)
+    k_mlp_grad(const float* __restrict__ X, const float* __restrict__ Y,
+               int n, const float* __restrict__ params, float tau,
+               float inv_n, float* __restrict__ grad, float* __restrict__ loss) {
+  extern __shared__ float4 smem_raw[];
+  float* P = reinterpret_cast<float*>(smem_raw);  // kMlpParams
+  float* G = P + kMlpParams + 3;                   // kMlpParams (grads)
+  MlpWarpSmem* ws = reinterpret_cast<MlpWarpSmem*>(G + kMlpParams + 3);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  MlpWarpSmem& S = ws[w];
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+    P[i] = params[i];
+    G[i] = 0.f;
+  }
+  __syncthreads();
+  const float* W1 = P + kOffW1;
+  const float* b1 = P + kOffB1;
+  const float* W2 = P + kOffW2;
+  const float* b2 = P + kOffB2;
+  const float* w3 = P + kOffW3;
+  const float b3 = P[kOffB3];
+  const int g = lane >> 2, t = lane & 3;
+  float lsum = 0.f;
+  const int ntiles = (n + 31) / 32;
+  for (int tile = blockIdx.x * kMlpWarps + w; tile < ntiles;
+       tile += gridDim.x * kMlpWarps) {
+    const int s = tile * 32 + lane;
+    const bool valid = s < n;
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) S.x[lane * kMlpIn + k] = valid ? X[(int64_t)s * kMlpIn + k] : 0.f;
+    __syncwarp();
+    // ---- forward ----
+    for (int mt = 0; mt < 2; ++mt) {
+      uint32_t a[4];
+      load_a_f32<false>(a, S.x, kMlpIn, 1, 16 * mt, 0, lane);
+      for (int nt = 0; nt < 8; ++nt) {
+        uint32_t b[2];
+        load_b_f32(b, W1, kMlpH, 1, 0, 8 * nt, lane);
+        const float z[4] = {0.f, 0.f, 0.f, 0.f};
+        float c[4];
+        mma_bf16_16816(c, a, b, z);
+        const int col = 8 * nt + 2 * t, r0 = 16 * mt + g, r1 = r0 + 8;
+        S.z1[r0 * kMlpH + col] = c[0] + b1[col];
+        S.z1[r0 * kMlpH + col + 1] = c[1] + b1[col + 1];
+        S.z1[r1 * kMlpH + col] = c[2] + b1[col];
+        S.z1[r1 * kMlpH + col + 1] = c[3] + b1[col + 1];
+      }
+    }
+    __syncwarp();
+    for (int mt = 0; mt < 2; ++mt)
+      for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 4; ++kt) {
+          uint32_t a[4], b[2];
+          load_a_f32<true>(a, S.z1, kMlpH, 1, 16 * mt, 16 * kt, lane);
+          load_b_f32(b, W2, kMlpH, 1, 16 * kt, 8 * nt, lane);
+          mma_bf16_16816(c, a, b, c);
+        }
+        const int col = 8 * nt + 2 * t, r0 = 16 * mt + g, r1 = r0 + 8;
+        S.z2[r0 * kMlpH + col] = c[0] + b2[col];
+        S.z2[r0 * kMlpH + col + 1] = c[1] + b2[col + 1];
+        S.z2[r1 * kMlpH + col] = c[2] + b2[col];
+        S.z2[r1 * kMlpH + col + 1] = c[3] + b2[col + 1];
+      }
+    __syncwarp();
+    float yhat = b3;
+    for (int j = 0; j < kMlpH; ++j) yhat += fmaxf(S.z2[lane * kMlpH + j], 0.f) * w3[j];
+    // ---- pinball loss ----
+    const float e = valid ? Y[s] - yhat : 0.f;
+    if (valid) lsum += fmaxf(tau * e, (tau - 1.f) * e);
+    const float gy = valid ? (e > 0.f ? -tau : 1.f - tau) * inv_n : 0.f;
+    // ---- backward ----
+    // dW3, db3
+    {
+      float d0 = 0.f, d1 = 0.f;
+      for (int i = 0; i < 32; ++i) {
+        const float gi = __shfl_sync(0xffffffffu, gy, i);
+        d0 += gi * fmaxf(S.z2[i * kMlpH + lane], 0.f);
+        d1 += gi * fmaxf(S.z2[i * kMlpH + lane + 32], 0.f);
+      }
+      atomicAdd(&G[kOffW3 + lane], d0);
+      atomicAdd(&G[kOffW3 + lane + 32], d1);
+      float gs = gy;
+      for (int o = 16; o > 0; o >>= 1) gs += __shfl_xor_sync(0xffffffffu, gs, o);
+      if (lane == 0) atomicAdd(&G[kOffB3], gs);
+    }
+    __syncwarp();
+    // dZ2 = gy w3 * (Z2 > 0), in place of Z2
+    for (int j = 0; j < kMlpH; ++j) {
+      const float z = S.z2[lane * kMlpH + j];
+      S.z2[lane * kMlpH + j] = z > 0.f ? gy * w3[j] : 0.f;
+    }
+    __syncwarp();
+    {  // db2
+      float d0 = 0.f, d1 = 0.f;
+      for (int i = 0; i < 32; ++i) {
+        d0 += S.z2[i * kMlpH + lane];
+        d1 += S.z2[i * kMlpH + lane + 32];
+      }
+      atomicAdd(&G[kOffB2 + lane], d0);
+      atomicAdd(&G[kOffB2 + lane + 32], d1);
+    }
+    // dW2 = relu(Z1)^T dZ2: A(m, k) = relu(Z1[k][m]), B(k, n) = dZ2[k][n]
+    for (int mt = 0; mt < 4; ++mt)
+      for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 2; ++kt) {
+          uint32_t a[4], b[2];
+          load_a_f32<true>(a, S.z1, 1, kMlpH, 16 * mt, 16 * kt, lane);
+          load_b_f32(b, S.z2, kMlpH, 1, 16 * kt, 8 * nt, lane);
+          mma_bf16_16816(c, a, b, c);
+        }
+        const int col = 8 * nt + 2 * t, r0 = 16 * mt + g, r1 = r0 + 8;
+        atomicAdd(&G[kOffW2 + r0 * kMlpH + col], c[0]);
+        atomicAdd(&G[kOffW2 + r0 * kMlpH + col + 1], c[1]);
+        atomicAdd(&G[kOffW2 + r1 * kMlpH + col], c[2]);
+        atomicAdd(&G[kOffW2 + r1 * kMlpH + col + 1], c[3]);
+      }
+    __syncwarp();
+    // dH1 = dZ2 W2^T, then dZ1 = dH1 * (Z1 > 0) in place of Z1
+    float dz1[2][8][4];
+    for (int mt = 0; mt < 2; ++mt)
+      for (int nt = 0; nt < 8; ++nt) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 4; ++kt) {
+          uint32_t a[4], b[2];
+          load_a_f32<false>(a, S.z2, kMlpH, 1, 16 * mt, 16 * kt, lane);
+          load_b_f32(b, W2, 1, kMlpH, 16 * kt, 8 * nt, lane);  // B(k,n) = W2[n][k]
+          mma_bf16_16816(c, a, b, c);
+        }
+        for (int i = 0; i < 4; ++i) dz1[mt][nt][i] = c[i];
+      }
+    __syncwarp();
+    for (int mt = 0; mt < 2; ++mt)
+      for (int nt = 0; nt < 8; ++nt) {
+        const int col = 8 * nt + 2 * t, r0 = 16 * mt + g, r1 = r0 + 8;
+        float* z = S.z1;
+        z[r0 * kMlpH + col] = z[r0 * kMlpH + col] > 0.f ? dz1[mt][nt][0] : 0.f;
+        z[r0 * kMlpH + col + 1] = z[r0 * kMlpH + col + 1] > 0.f ? dz1[mt][nt][1] : 0.f;
+        z[r1 * kMlpH + col] = z[r1 * kMlpH + col] > 0.f ? dz1[mt][nt][2] : 0.f;
+        z[r1 * kMlpH + col + 1] = z[r1 * kMlpH + col + 1] > 0.f ? dz1[mt][nt][3] : 0.f;
+      }
+    __syncwarp();
+    {  // db1
+      float d0 = 0.f, d1 = 0.f;
+      for (int i = 0; i < 32; ++i) {
+        d0 += S.z1[i * kMlpH + lane];
+        d1 += S.z1[i * kMlpH + lane + 32];
+      }
+      atomicAdd(&G[kOffB1 + lane], d0);
+      atomicAdd(&G[kOffB1 + lane + 32], d1);
+    }
+    // dW1 = X^T dZ1: A(m, k) = X[k][m] (16 x 32), B(k, n) = dZ1[k][n]
+    for (int nt = 0; nt < 8; ++nt) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+      for (int kt = 0; kt < 2; ++kt) {
+        uint32_t a[4], b[2];
+        load_a_f32<false>(a, S.x, 1, kMlpIn, 0, 16 * kt, lane);
+        load_b_f32(b, S.z1, kMlpH, 1, 16 * kt, 8 * nt, lane);
+        mma_bf16_16816(c, a, b, c);
+      }
+      const int col = 8 * nt + 2 * t;
+      atomicAdd(&G[kOffW1 + g * kMlpH + col], c[0]);
+      atomicAdd(&G[kOffW1 + g * kMlpH + col + 1], c[1]);
+      atomicAdd(&G[kOffW1 + (g + 8) * kMlpH + col], c[2]);
+      atomicAdd(&G[kOffW1 + (g + 8) * kMlpH + col + 1], c[3]);
+    }
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) atomicAdd(&grad[i], G[i]);
+  if (lane == 0) atomicAdd(loss, lsum * inv_n);
+}
+
+__global__ void k_mlp_adam(float* __restrict__ params, float* __restrict__ grad,
+                           float* __restrict__ m, float* __restrict__ v,
+                           float lr, float beta1, float beta2, float eps,
+                           float bc1, float bc2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kMlpParams) return;
+  const float gi = grad[i];
+  const float mi = beta1 * m[i] + (1.f - beta1) * gi;
+  const float vi = beta2 * v[i] + (1.f - beta2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  params[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  grad[i] = 0.f;
+}
+
+// Packs FP32 parameters (+ feature normalisation) into MlpPacked.
+__global__ void k_mlp_pack(const float* __restrict__ params,
+                           const float* __restrict__ mean,
+                           const float* __restrict__ inv_std, MlpPacked* out) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const float* W1 = params + kOffW1;
+  const float* W2 = params + kOffW2;
+  if (tid < 8 * 32) {  // W1 fragments
+    const int nt = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+    const int nn = 8 * nt + g, k = 2 * t;
+    out->w1f[tid] = make_uint2(pack_bf16x2(W1[k * kMlpH + nn], W1[(k + 1) * kMlpH + nn]),
+                               pack_bf16x2(W1[(k + 8) * kMlpH + nn], W1[(k + 9) * kMlpH + nn]));
+  }
+  if (tid < 4 * 8 * 32) {  // W2 fragments
+    const int kt = tid >> 8, nt = (tid >> 5) & 7, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3, nn = 8 * nt + g, k = 16 * kt + 2 * t;
+    out->w2f[tid] = make_uint2(pack_bf16x2(W2[k * kMlpH + nn], W2[(k + 1) * kMlpH + nn]),
+                               pack_bf16x2(W2[(k + 8) * kMlpH + nn], W2[(k + 9) * kMlpH + nn]));
+  }
+  if (tid < kMlpH) {
+    out->vec[tid] = params[kOffB1 + tid];
+    out->vec[kMlpH + tid] = params[kOffB2 + tid];
+    out->vec[2 * kMlpH + tid] = params[kOffW3 + tid];
+  }
+  if (tid == 0) out->vec[3 * kMlpH] = params[kOffB3];
+  if (tid < kMlpIn) {
+    out->vec[3 * kMlpH + 1 + tid] = mean[tid];
+    out->vec[3 * kMlpH + 1 + kMlpIn + tid] = inv_std[tid];
+  }
+}
+
+// Inference over n samples (for tests): y[i] for X[i][16] raw features.
+__global__ void k_mlp_infer(const float* __restrict__ X, int n,
+                            const MlpPacked* __restrict__ packed, float* y) {
+  __shared__ MlpPacked P;
+  __shared__ float xs[kMlpWarps][32 * kMlpIn];
+  __shared__ __nv_bfloat16 h1[kMlpWarps][32 * kMlpH];
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(packed);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&P);
+    for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 4); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ntiles = (n + 31) / 32;
+  for (int tile = blockIdx.x * kMlpWarps + w; tile < ntiles; tile += gridDim.x * kMlpWarps) {
+    const int s = tile * 32 + lane;
+    float x[kMlpIn];
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) x[k] = s < n ? X[(int64_t)s * kMlpIn + k] : 0.f;
+    const float yy = mlp_forward_warp(x, xs[w], h1[w], P, lane);
+    if (s < n) y[s] = yy;
+  }
+}
+
+size_t mlp_grad_smem() {
+  return sizeof(float) * (2 * (kMlpParams + 3)) + sizeof(MlpWarpSmem) * kMlpWarps;
+}
+
+int mlp_grad(const float* X, const float* Y, int n, const float* params,
+             float tau, float* grad, float* loss, int blocks, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)mlp_grad_smem());
+    attr = true;
+  }
+  if (n <= 0) return 0;
+  int tiles = (n + 31) / 32;
+  int maxb = (tiles + kMlpWarps - 1) / kMlpWarps;
+  if (blocks > maxb) blocks = maxb;
+  k_mlp_grad<<<blocks, kMlpThreads, mlp_grad_smem(), st>>>(X, Y, n, params, tau,
+                                                           1.f / (float)n, grad, loss);
+  return 1;
+}
+
+int mlp_adam(float* params, float* grad, float* m, float* v, float lr, int t,
+             cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  float bc1 = 1.f - powf(b1, (float)t), bc2 = 1.f - powf(b2, (float)t);
+  k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(params, grad, m, v, lr, b1,
+                                                       b2, 1e-8f, bc1, bc2);
+  return 1;
+}
+
+int mlp_pack(const float* params, const float* mean, const float* inv_std,
+             MlpPacked* out, cudaStream_t st) {
+  k_mlp_pack<<<4, 256, 0, st>>>(params, mean, inv_std, out);
+  return 1;
+}
+
+int mlp_infer(const float* X, int n, const MlpPacked* packed, float* y,
+              cudaStream_t st) {
+  if (n <= 0) return 0;
+  int tiles = (n + 31) / 32;
+  int blocks = (tiles + kMlpWarps - 1) / kMlpWarps;
+  if (blocks > 1184) blocks = 1184;
+  k_mlp_infer<<<blocks, kMlpThreads, 0, st>>>(X, n, packed, y);
+  return 1;
+}
+
+}  // namespace tg
+
+// ------------------------------------------------------------ training ----
+namespace tg {
+
+// Per-feature mean, 1/std, min and max (one block per feature, FP64 sums).
+__global__ void k_feat_stats(const float* __restrict__ X, int n, float* stats) {
+  const int k = blockIdx.x;
+  double s = 0.0, s2 = 0.0;
+  float mn = 3.0e38f, mx = -3.0e38f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = X[(int64_t)i * kMlpIn + k];
+    s += v;
+    s2 += (double)v * v;
+    mn = fminf(mn, v);
+    mx = fmaxf(mx, v);
+  }
+  __shared__ double ss[256], ss2[256];
+  __shared__ float smn[256], smx[256];
+  ss[threadIdx.x] = s;
+  ss2[threadIdx.x] = s2;
+  smn[threadIdx.x] = mn;
+  smx[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+      ss2[threadIdx.x] += ss2[threadIdx.x + o];
+      smn[threadIdx.x] = fminf(smn[threadIdx.x], smn[threadIdx.x + o]);
+      smx[threadIdx.x] = fmaxf(smx[threadIdx.x], smx[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double mean = ss[0] / n;
+    const double var = fmax(ss2[0] / n - mean * mean, 0.0);
+    stats[k] = (float)mean;
+    stats[kMlpIn + k] = (float)(1.0 / fmax(sqrt(var), 1e-6));
+    stats[2 * kMlpIn + k] = smn[0];
+    stats[3 * kMlpIn + k] = smx[0];
+  }
+}
+
+__global__ void k_shuffle_keys(uint64_t* keys, uint32_t* vals, int n, uint64_t seed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = (uint64_t)i + seed * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  keys[i] = z ^ (z >> 31);
+  vals[i] = (uint32_t)i;
+}
+
+__global__ void k_normalize_gather(const float* __restrict__ X,
+                                   const float* __restrict__ Y,
+                                   const uint32_t* __restrict__ perm, int n,
+                                   const float* __restrict__ stats,
+                                   float* __restrict__ Xn, float* __restrict__ Yn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t j = perm[i];
+#pragma unroll
+  for (int k = 0; k < kMlpIn; ++k)
+    Xn[(int64_t)i * kMlpIn + k] = (X[j * kMlpIn + k] - stats[k]) * stats[kMlpIn + k];
+  Yn[i] = Y[j];
+}
+
+}  // namespace tg
+
+#include <cmath>
+#include <random>
+#include <vector>
+#include "build.h"
+
+namespace tg {
+
+int mlp_train(const float* X, const float* Y, int n, int epochs, int batch,
+              float lr, float tau, uint64_t seed, float* params, float* stats,
+              float* loss_per_epoch, cudaStream_t st) {
+  if (n <= 0 || epochs <= 0 || batch <= 0) return (int)cudaErrorInvalidValue;
+  // He initialisation on the host from the seed
+  std::vector<float> p(kMlpParams, 0.f);
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  for (int i = 0; i < kMlpIn * kMlpH; ++i) p[kOffW1 + i] = nd(rng) * std::sqrt(2.f / kMlpIn);
+  for (int i = 0; i < kMlpH * kMlpH; ++i) p[kOffW2 + i] = nd(rng) * std::sqrt(2.f / kMlpH);
+  for (int i = 0; i < kMlpH; ++i) p[kOffW3 + i] = nd(rng) * std::sqrt(1.f / kMlpH);
+  float *Xn = nullptr, *Yn = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *loss = nullptr;
+  uint64_t *k0 = nullptr, *k1 = nullptr;
+  uint32_t *v0 = nullptr, *v1 = nullptr;
+  int32_t *hist = nullptr, *part = nullptr;
+  const int rb = radix_blocks(n);
+  const int sp = scan_partials_needed(256 * rb > n + 1 ? 256 * rb : n + 1);
+  cudaError_t e = cudaSuccess;
+  auto al = [&](void** q, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(q, bytes);
+  };
+  al((void**)&Xn, sizeof(float) * (size_t)n * kMlpIn);
+  al((void**)&Yn, sizeof(float) * (size_t)n);
+  al((void**)&grad, sizeof(float) * kMlpParams);
+  al((void**)&m, sizeof(float) * kMlpParams);
+  al((void**)&v, sizeof(float) * kMlpParams);
+  al((void**)&loss, sizeof(float));
+  al((void**)&k0, sizeof(uint64_t) * n);
+  al((void**)&k1, sizeof(uint64_t) * n);
+  al((void**)&v0, sizeof(uint32_t) * n);
+  al((void**)&v1, sizeof(uint32_t) * n);
+  al((void**)&hist, sizeof(int32_t) * 256 * (size_t)rb);
+  al((void**)&part, sizeof(int32_t) * ((size_t)sp + 1));
+  if (e == cudaSuccess) {
+    cudaMemcpyAsync(params, p.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(grad, 0, sizeof(float) * kMlpParams, st);
+    cudaMemsetAsync(m, 0, sizeof(float) * kMlpParams, st);
+    cudaMemsetAsync(v, 0, sizeof(float) * kMlpParams, st);
+    k_feat_stats<<<kMlpIn, 256, 0, st>>>(X, n, stats);
+    k_shuffle_keys<<<(n + 255) / 256, 256, 0, st>>>(k0, v0, n, seed);
+    radix_sort(k0, v0, k1, v1, n, hist, part, st);
+    k_normalize_gather<<<(n + 255) / 256, 256, 0, st>>>(X, Y, v0, n, stats, Xn, Yn);
+    const int nb = (n + batch - 1) / batch;
+    int t = 0;
+    for (int ep = 0; ep < epochs; ++ep) {
+      cudaMemsetAsync(loss, 0, sizeof(float), st);
+      const float lr_e = 0.5f * lr * (1.f + std::cos(3.14159265f * ep / epochs));
+      for (int bi = 0; bi < nb; ++bi) {
+        const int s0 = bi * batch;
+        const int len = s0 + batch <= n ? batch : n - s0;
+        mlp_grad(Xn + (int64_t)s0 * kMlpIn, Yn + s0, len, params, tau, grad, loss, 64, st);
+        mlp_adam(params, grad, m, v, lr_e, ++t, st);
+      }
+      float hl = 0.f;
+      cudaMemcpyAsync(&hl, loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+      e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) break;
+      if (loss_per_epoch) loss_per_epoch[ep] = hl / nb;
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+  }
+  cudaStreamSynchronize(st);
+  void* all[] = {Xn, Yn, grad, m, v, loss, k0, k1, v0, v1, hist, part};
+  for (void* q : all)
+    if (q) cudaFree(q);
+  return (int)e;
+}
+
+}  // namespace tg

@@ -24,6 +24,7 @@
 // cells whose net charge nearly cancels).  Near field: erf-Kelbg (or the
 // reference laws) for every particle pair.
 #include <cstdio>
+#include "mac.cuh"
 #include "walk_mixed.h"
 
 namespace tg {
@@ -68,6 +69,15 @@ struct MixedArgs {
   uint32_t* rdf;
   unsigned long long* counters;
   int32_t* err;
+  // learned acceptance
+  const MlpPacked* packed;
+  const float* fmin;
+  const float* fmax;
+  const float4* geom;
+  const double* f_prev;
+  float eta_over_eps;
+  float rho_lo, rho_hi;
+  float lam_ei;
 };
 
 struct Acc {
@@ -277,13 +287,39 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
 }
 
 // --------------------------------------------------------------- walk ----
-template <int PHYS, bool RDF>
+// Dynamic shared memory: WarpSmem[kMxWarps], then (learned MAC only) the
+// packed network and one 32x64 BF16 hidden tile per warp.
+template <bool LEARNED>
+constexpr size_t walk_smem_bytes() {
+  return sizeof(WarpSmem) * kMxWarps +
+         (LEARNED ? sizeof(MlpPacked) + sizeof(__nv_bfloat16) * 32 * kMlpH * kMxWarps : 0);
+}
+
+template <int PHYS, bool RDF, bool LEARNED>
 __global__ void __launch_bounds__(kMxThreads, 2)
     k_walk_mixed(MixedArgs a) {
-  __shared__ WarpSmem smem[kMxWarps];
+  extern __shared__ float4 dyn_smem[];
+  WarpSmem* smem = reinterpret_cast<WarpSmem*>(dyn_smem);
+  MlpPacked* mlp = reinterpret_cast<MlpPacked*>(smem + kMxWarps);
+  __nv_bfloat16* h1_all = reinterpret_cast<__nv_bfloat16*>(mlp + 1);
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   WarpSmem& sm = smem[wib];
+  if (LEARNED) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(a.packed);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(mlp);
+    for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 4); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+  }
+  __nv_bfloat16* h1_tile = h1_all + (size_t)wib * 32 * kMlpH;
+  float fmin_r[kMacFeatures], fmax_r[kMacFeatures];
+  if (LEARNED) {
+#pragma unroll
+    for (int k = 0; k < kMacFeatures; ++k) {
+      fmin_r[k] = __ldg(&a.fmin[k]);
+      fmax_r[k] = __ldg(&a.fmax[k]);
+    }
+  }
   const int gwarp = blockIdx.x * kMxWarps + wib;
   int32_t* stack = a.stack + (int64_t)gwarp * kStackCap;
   const unsigned lt = (1u << lane) - 1u;
@@ -311,11 +347,22 @@ __global__ void __launch_bounds__(kMxThreads, 2)
     const float tlx = (float)(rtx - (double)thx), tly = (float)(rty - (double)thy),
                 tlz = (float)(rtz - (double)thz);
     Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
+    // error budget of the learned MAC: eta * min |F_prev| / eps over the group
+    float budget = 0.f, hlen = 0.f;
+    if (LEARNED) {
+      const int64_t o = a.order[pt];
+      const double fx = a.f_prev[3 * o], fy = a.f_prev[3 * o + 1], fz = a.f_prev[3 * o + 2];
+      float fm = act ? (float)sqrt(fx * fx + fy * fy + fz * fz) : 3.0e38f;
+      for (int o2 = 16; o2 > 0; o2 >>= 1) fm = fminf(fm, __shfl_xor_sync(0xffffffffu, fm, o2));
+      budget = a.eta_over_eps * fm;
+      hlen = (float)sqrt(hx * hx + hy * hy + hz * hz);
+    }
     int ssize = 1;
     if (lane == 0) stack[0] = 0;  // root
     __syncwarp();
     int m2h = 0, m2t = 0, p2h = 0, p2t = 0;  // ring heads/tails (warp-uniform)
     long long n_m2p = 0, n_p2p = 0;
+    unsigned n_mlp = 0, n_fallback = 0;  // per lane: cells this lane sent to the MLP
     bool overflow = false;
     while (ssize > 0) {
       const int nb = min(32, ssize);
@@ -323,8 +370,11 @@ __global__ void __launch_bounds__(kMxThreads, 2)
       ssize -= nb;
       __syncwarp();
       int action = 0, pfirst = 0, pcnt = 0;  // 1 far field, 2 particles, 3 open
+      bool cand = false;                       // 4: left to the learned MAC
+      float cand_d = 0.f;
+      double4 c;
       if (node >= 0) {
-        const double4 c = ldg_d4(&a.node_c[node]);
+        c = ldg_d4(&a.node_c[node]);
         if (c.w < 0.0) {
           action = 2;
           pfirst = __ldg(&a.first[node]);
@@ -335,7 +385,63 @@ __global__ void __launch_bounds__(kMxThreads, 2)
           const double ey = fmax(fabs(c.y - Gy) - hy, 0.0);
           const double ez = fmax(fabs(c.z - Gz) - hz, 0.0);
           const double d2 = ex * ex + ey * ey + ez * ez;
-          if (c.w * c.w < d2) {
+          bool accept = c.w * c.w < d2;
+          if (LEARNED && budget > 0.f) {
+            // band of the learned criterion: rho = s / (d - dx)
+            const float4 g4 = __ldg(&a.geom[node]);
+            const double dd = sqrt(d2);
+            const double margin = dd - (double)g4.y;
+            const float rho = margin > 0.0 ? (float)((double)g4.x / margin) : 3.0e38f;
+            if (rho < a.rho_lo) accept = true;
+            else if (rho > a.rho_hi) accept = false;
+            else {
+              cand = true;
+              cand_d = (float)dd;
+            }
+          }
+          if (accept && !cand) {
+            action = 1;
+          } else if (cand) {
+            action = 4;  // decided by the network below
+          } else {
+            const int cnt = __ldg(&a.count[node]);
+            if (cnt <= a.bucket) {
+              action = 2;
+              pfirst = __ldg(&a.first[node]);
+              pcnt = cnt;
+            } else {
+              action = 3;
+            }
+          }
+        }
+      }
+      if (LEARNED && __any_sync(0xffffffffu, cand)) {
+        float feat[kMacFeatures];
+        if (cand) {
+          const float4* mp = a.mom + 3 * (int64_t)node;
+          mac_features(c.x, c.y, c.z, __ldg(&a.geom[node]), __ldg(mp), __ldg(mp + 1),
+                       __ldg(mp + 2), Gx, Gy, Gz, hlen, cand_d, (float)n_act,
+                       a.lam_ei, feat);
+        } else {
+#pragma unroll
+          for (int k = 0; k < kMacFeatures; ++k) feat[k] = 0.f;
+        }
+        const float y = mlp_forward_warp(feat, reinterpret_cast<float*>(sm.cell),
+                                         h1_tile, *mlp, lane);
+        if (cand) {
+          bool in_range = true;
+#pragma unroll
+          for (int k = 0; k < kMacFeatures; ++k)
+            in_range = in_range && feat[k] >= fmin_r[k] && feat[k] <= fmax_r[k];
+          bool accept;
+          if (in_range) {
+            // predicted |dF| = 10^y * n / d^2 against the group's budget
+            const float n = __ldg(&a.geom[node]).z;
+            accept = y <= log10f(budget * cand_d * cand_d / n);
+          } else {
+            accept = c.w < (double)cand_d;  // fixed-theta fallback
+          }
+          if (accept) {
             action = 1;
           } else {
             const int cnt = __ldg(&a.count[node]);
@@ -347,6 +453,8 @@ __global__ void __launch_bounds__(kMxThreads, 2)
               action = 3;
             }
           }
+          n_mlp += 1;
+          n_fallback += in_range ? 0 : 1;
         }
       }
       // far-field entries
@@ -427,6 +535,17 @@ __global__ void __launch_bounds__(kMxThreads, 2)
       atomicAdd(&a.counters[0], (unsigned long long)(n_m2p * n_act));
       atomicAdd(&a.counters[1], (unsigned long long)(n_p2p * n_act));
     }
+    if (LEARNED) {
+      unsigned long long m = n_mlp, fb = n_fallback;
+      for (int o2 = 16; o2 > 0; o2 >>= 1) {
+        m += __shfl_xor_sync(0xffffffffu, m, o2);
+        fb += __shfl_xor_sync(0xffffffffu, fb, o2);
+      }
+      if (lane == 0) {
+        atomicAdd(&a.counters[2], m);
+        atomicAdd(&a.counters[3], fb);
+      }
+    }
   }
   if (lane == 0) atomicMax(&a.control[1], max_stack);
 }
@@ -449,6 +568,7 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.digit, (size_t)cap);
   rc |= realloc_dev(&mb.m64, 6 * (size_t)cap);
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
+  rc |= realloc_dev(&mb.geom, (size_t)cap);
   return rc;
 }
 
@@ -468,7 +588,7 @@ int mixed_alloc_particles(MixedBuffers& mb, int n) {
 
 void mixed_free(MixedBuffers& mb) {
   void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
-                  mb.xs, mb.groups, mb.stack, mb.control};
+                  mb.geom, mb.xs, mb.groups, mb.stack, mb.control};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   mb = MixedBuffers();
@@ -482,6 +602,7 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
   m.digit = mb.digit;
   m.m64 = mb.m64;
   m.mom = mb.mom;
+  m.geom = mb.geom;
   m.xs = mb.xs;
   m.groups = mb.groups;
   m.n_groups = mb.control + 2;
@@ -490,7 +611,8 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
 
 int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
                int n, int n_el, const TreeView& tv, const WalkParams& wp,
-               const MixedTuning& tune, double* f, double2* epot_part,
+               const MixedTuning& tune, const LearnedMac* learned,
+               double* f, double2* epot_part,
                uint32_t* rdf, unsigned long long* counters, int32_t* err,
                cudaStream_t st) {
   (void)x;
@@ -529,16 +651,37 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   // control[0] group cursor, [1] deepest stack; [2] (group count) is written
   // by the build
   cudaMemsetAsync(mb.control, 0, 2 * sizeof(int32_t), st);
+  const bool L = learned != nullptr && learned->packed != nullptr &&
+                 learned->f_prev != nullptr;
+  a.packed = L ? learned->packed : nullptr;
+  a.fmin = L ? learned->fmin : nullptr;
+  a.fmax = L ? learned->fmax : nullptr;
+  a.geom = mb.geom;
+  a.f_prev = L ? learned->f_prev : nullptr;
+  a.eta_over_eps = L ? (float)(learned->eta / kEps) : 0.f;
+  a.rho_lo = L ? learned->rho_lo : 0.f;
+  a.rho_hi = L ? learned->rho_hi : 0.f;
+  a.lam_ei = (float)wp.lam_ei;
   int bps = tune.blocks_per_sm < 1 ? 1 : (tune.blocks_per_sm > kMaxBlocksPerSm ? kMaxBlocksPerSm : tune.blocks_per_sm);
   int grid = (mb.grid_warps / (kMaxBlocksPerSm * kMxWarps)) * bps;
-  bool r = rdf != nullptr;
+  const bool r = rdf != nullptr;
+  const size_t s0 = walk_smem_bytes<false>(), s1 = walk_smem_bytes<true>();
+#define TG_LAUNCH(P, R, LL)                                                   \
+  do {                                                                        \
+    auto kfn = k_walk_mixed<P, R, LL>;                                        \
+    const size_t sb = LL ? s1 : s0;                                           \
+    cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                         (int)sb);                                            \
+    kfn<<<grid, kMxThreads, sb, st>>>(a);                                     \
+  } while (0)
   if (wp.physics == 1) {
-    if (r) k_walk_mixed<1, true><<<grid, kMxThreads, 0, st>>>(a);
-    else k_walk_mixed<1, false><<<grid, kMxThreads, 0, st>>>(a);
+    if (L) { if (r) TG_LAUNCH(1, true, true); else TG_LAUNCH(1, false, true); }
+    else { if (r) TG_LAUNCH(1, true, false); else TG_LAUNCH(1, false, false); }
   } else {
-    if (r) k_walk_mixed<0, true><<<grid, kMxThreads, 0, st>>>(a);
-    else k_walk_mixed<0, false><<<grid, kMxThreads, 0, st>>>(a);
+    if (L) { if (r) TG_LAUNCH(0, true, true); else TG_LAUNCH(0, false, true); }
+    else { if (r) TG_LAUNCH(0, true, false); else TG_LAUNCH(0, false, false); }
   }
+#undef TG_LAUNCH
   return 1;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include "build.h"
 #include "internal.cuh"
+#include "mlp.cuh"
 #include "walk.h"
 
 namespace tg {
@@ -17,6 +18,7 @@ struct MixedBuffers {
   int8_t* digit = nullptr;
   double2* m64 = nullptr;
   float4* mom = nullptr;
+  float4* geom = nullptr;
   double4* xs = nullptr;
   int2* groups = nullptr;
   int32_t* stack = nullptr;    // per resident warp: kStackCap node indices
@@ -30,6 +32,19 @@ struct MixedTuning {
   int blocks_per_sm = 4;   // persistent grid: SMs x blocks_per_sm blocks
 };
 
+// Learned acceptance: inside the band rho_lo <= s/(d - dx) <= rho_hi a cell
+// is accepted when the predicted error 10^y * n/d^2 (units of e, Coulomb
+// constant dropped) is at most eta * min over the group of |F_prev| / eps.
+struct LearnedMac {
+  const MlpPacked* packed = nullptr;  // device
+  const float* fmin = nullptr;        // device, 16: training range
+  const float* fmax = nullptr;        // device, 16
+  const double* f_prev = nullptr;     // device forces of the previous step
+  float eta = 1e-5f;
+  float rho_lo = 0.2f, rho_hi = 0.9f;
+  float lam_ei = 0.f;
+};
+
 int mixed_alloc_nodes(MixedBuffers& mb, int cap);
 int mixed_alloc_particles(MixedBuffers& mb, int n);
 void mixed_free(MixedBuffers& mb);
@@ -38,7 +53,8 @@ MixedNodes mixed_nodes(const MixedBuffers& mb);
 // Forces on every particle from both trees.  Returns kernels launched.
 int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
                int n, int n_el, const TreeView& tv, const WalkParams& wp,
-               const MixedTuning& tune, double* f, double2* epot_part,
+               const MixedTuning& tune, const LearnedMac* learned,
+               double* f, double2* epot_part,
                uint32_t* rdf, unsigned long long* counters, int32_t* err,
                cudaStream_t st);
 

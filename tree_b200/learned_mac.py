@@ -1,0 +1,101 @@
+"""Trains the learned multipole acceptance criterion on the GPU.
+
+    python -m tree_b200.learned_mac [--n 65536] [--out tree_b200/data/mac_model.npz]
+
+Training data is generated by the method itself: seeded clouds of N = 65,536
+particles at electron temperatures across [10, 200] K are evolved a few steps
+with the fixed-theta mixed walk, and at each state `tree_gpu_mac_collect`
+walks the combined tree with opening angles drawn from [0.2, 0.9], recording
+for every tested cell in the acceptance band its features and the exact FP64
+error of accepting it.  The network (16 -> 64 -> 64 -> 1) is then trained by
+the library's own BF16 tensor-core kernels (`tree_gpu_mac_train`) with a
+0.9-quantile pinball loss, so its predictions lean to over-estimating the
+error.  The model file holds the FP32 parameters, the feature statistics and
+a short training report.
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import api, cloud, units
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_MODEL = os.path.join(HERE, "data", "mac_model.npz")
+
+
+def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
+                      steps_list=(2, 6, 20), theta=(0.2, 0.9), rho=(0.2, 0.9),
+                      max_count=16384, cap=12_000_000, epochs=10, batch=8192,
+                      lr=2e-3, tau=0.9, seed=11, verbose=True):
+    dt = units.dt_code(1e-11)
+    half = n // 2
+    report = {"n": n, "te_list": list(te_list), "steps_list": list(steps_list),
+              "theta": list(theta), "rho": list(rho), "max_count": max_count,
+              "tau": tau, "epochs": epochs, "batch": batch, "lr": lr, "collects": []}
+    t0 = time.time()
+    cfg = api.Config(theta=0.5, te=te_list[0], physics=api.PHYS_KELBG,
+                     precision=api.PREC_MIXED, mac=api.MAC_FIXED)
+    with api.TreeForce(half, half, cfg) as tf:
+        k = 0
+        for te in te_list:
+            tf.set_config(api.Config(theta=0.5, te=te, physics=api.PHYS_KELBG,
+                                     precision=api.PREC_MIXED, mac=api.MAC_FIXED))
+            c = cloud.make_cloud(n, seed=seed + int(te), te_k=te)
+            tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
+            done = 0
+            for s in steps_list:
+                tf.step(dt, s - done)
+                done = s
+                k += 1
+                tot = tf.mac_collect(theta[0], theta[1], rho[0], rho[1], max_count,
+                                     seed * 1000 + k, cap)
+                report["collects"].append({"te": te, "step": s, "total": tot})
+                if verbose:
+                    print(f"collect te={te:g} step={s}: {tot} samples", flush=True)
+        t1 = time.time()
+        losses = tf.mac_train(epochs, batch, lr, tau, seed)
+        t2 = time.time()
+        params, stats = tf.mac_get_model()
+        feats, labels, extra = tf.mac_samples()
+    report.update({"samples": int(len(labels)), "collect_s": t1 - t0,
+                   "train_s": t2 - t1, "loss_per_epoch": [float(x) for x in losses],
+                   "label_quantiles": {str(q): float(np.quantile(labels, q))
+                                       for q in (0.01, 0.1, 0.5, 0.9, 0.99)}})
+    if verbose:
+        print(json.dumps({k: v for k, v in report.items() if k != "collects"}), flush=True)
+    return params, stats, report, (feats, labels, extra)
+
+
+def save_model(path, params, stats, report):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez(path, params=np.asarray(params, np.float32),
+             stats=np.asarray(stats, np.float32),
+             report=np.frombuffer(json.dumps(report).encode(), np.uint8))
+
+
+def load_model(path=DEFAULT_MODEL):
+    d = np.load(path)
+    report = json.loads(bytes(d["report"]).decode()) if "report" in d else {}
+    return d["params"], d["stats"], report
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=65536)
+    ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--out", default=DEFAULT_MODEL)
+    ap.add_argument("--dump-samples", default="")
+    args = ap.parse_args()
+    params, stats, report, (f, y, e) = collect_and_train(n=args.n, epochs=args.epochs)
+    save_model(args.out, params, stats, report)
+    if args.dump_samples:
+        idx = np.random.default_rng(0).choice(len(y), min(len(y), 2_000_000), replace=False)
+        np.savez_compressed(args.dump_samples, feats=f[idx], labels=y[idx], extra=e[idx])
+    print("saved", args.out)
+
+
+if __name__ == "__main__":
+    main()
