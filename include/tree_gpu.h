@@ -195,22 +195,25 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
 
 /* Tunables of the mixed-precision walk: twigs holding at most `bucket`
  * particles (1..8) are summed particle by particle instead of being opened;
- * `blocks_per_sm` (1..4) sets the persistent grid.  No counterpart in the
- * reference; set by the autotuner (tree_b200/tune.py). */
+ * `blocks_per_sm` (1..4) sets the persistent grid; `order` (2 or 3) is the
+ * far-field expansion order (quadrupole, or octupole as well; default 3).
+ * No counterpart in the reference; set by the autotuner (tree_b200/tune.py). */
 int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
-                        int32_t blocks_per_sm);
+                        int32_t blocks_per_sm, int32_t order);
 
 /* ---- learned multipole acceptance criterion (no counterpart in the
  * reference, whose criterion is the fixed s/theta + dx < r of tree.f90:743).
  * A 16 -> 64 -> 64 -> 1 network predicts log10 of the error of accepting a
- * cell for a target group, relative to the cell's gross monopole field; in the
- * band rho_lo <= s/(d - dx) <= rho_hi the mixed walk accepts a cell when the
- * predicted error is at most eta * (smallest |F| of the group at the previous
- * step), and uses the fixed-theta test elsewhere or when the features fall
- * outside the training range.  Active when precision = MIXED and mac =
- * LEARNED and a model is loaded. */
+ * cell for a target group, relative to the cell's gross monopole field.  A
+ * cell that the fixed-theta test would open, with s/(d - dx) <= rho_hi, is
+ * accepted anyway when the predicted error is at most eta * (smallest |F| of
+ * the group at the previous step); features outside the training range keep
+ * the fixed-theta decision.  Active when precision = MIXED and mac = LEARNED
+ * and a model is loaded. */
 #define TREE_GPU_MLP_PARAMS 5313 /* W1[16][64] b1[64] W2[64][64] b2[64] w3[64] b3 */
-#define TREE_GPU_MLP_STATS 64    /* feature mean[16], 1/std[16], min[16], max[16] */
+#define TREE_GPU_MLP_STATS 72    /* feature mean[16], 1/std[16], min[16], max[16],
+                                    margins m_lo, m_hi (quantiles of label minus
+                                    the analytic estimate), 6 reserved */
 
 /* Walks the combined tree of the current device positions with a fixed
  * theta drawn per target group from [theta_lo, theta_hi] and appends one
@@ -221,7 +224,8 @@ int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
  * the number held. */
 int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
                          double rho_lo, double rho_hi, int32_t max_count,
-                         uint64_t seed, int64_t cap, int64_t* n_total);
+                         float keep, uint64_t seed, int64_t cap,
+                         int64_t* n_total);
 /* Copies the collected samples out (NULL buffers: count only). */
 int tree_gpu_mac_samples(tree_gpu_handle* h, float* feats, float* labels,
                          float* extra, int64_t cap, int64_t* n);

@@ -31,7 +31,8 @@ def test_device_inference_matches_oracle(device_lib):
     p = mlp.init_params(9)
     mean = rng.standard_normal(16).astype(np.float32)
     inv_std = rng.uniform(0.5, 2.0, 16).astype(np.float32)
-    stats = np.concatenate([mean, inv_std, np.full(16, -1e30), np.full(16, 1e30)]).astype(np.float32)
+    stats = np.concatenate([mean, inv_std, np.full(16, -1e30), np.full(16, 1e30),
+                            np.zeros(8)]).astype(np.float32)
     y_d = api.mlp_infer(X, p, stats)
     y_o, _ = mlp.forward(p, (X - mean) * inv_std, bf16_emulation=True)
     np.testing.assert_allclose(y_d, y_o, rtol=1e-4, atol=1e-4 * np.abs(y_o).max())

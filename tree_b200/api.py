@@ -99,12 +99,12 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.POINTER(Params), vp,
                                          ctypes.c_int64, vp, vp, vp]
     L.tree_gpu_set_stream.argtypes = [vp, vp]
-    L.tree_gpu_set_tuning.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+    L.tree_gpu_set_tuning.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
     fp = ctypes.POINTER(ctypes.c_float)
     L.tree_gpu_mac_collect.argtypes = [vp, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_double,
-                                       ctypes.c_int32, ctypes.c_uint64,
-                                       ctypes.c_int64, lp]
+                                       ctypes.c_int32, ctypes.c_float,
+                                       ctypes.c_uint64, ctypes.c_int64, lp]
     L.tree_gpu_mac_samples.argtypes = [vp, fp, fp, fp, ctypes.c_int64, lp]
     L.tree_gpu_mac_clear.argtypes = [vp]
     L.tree_gpu_mac_train.argtypes = [vp, ctypes.c_int32, ctypes.c_int32,
@@ -127,7 +127,7 @@ def load_library(path: str = LIB_PATH):
 
 
 MLP_PARAMS = 5313
-MLP_STATS = 64
+MLP_STATS = 72
 
 
 def _fp(a):
@@ -317,15 +317,15 @@ class TreeForce:
         handle's own stream."""
         self._check(self.lib.tree_gpu_set_stream(self.h, stream_handle or None))
 
-    def set_tuning(self, bucket: int = 4, blocks_per_sm: int = 4):
-        self._check(self.lib.tree_gpu_set_tuning(self.h, bucket, blocks_per_sm))
+    def set_tuning(self, bucket: int = 8, blocks_per_sm: int = 4, order: int = 3):
+        self._check(self.lib.tree_gpu_set_tuning(self.h, bucket, blocks_per_sm, order))
 
     # ---- learned MAC ----
-    def mac_collect(self, theta_lo=0.2, theta_hi=0.9, rho_lo=0.2, rho_hi=0.9,
-                    max_count=16384, seed=1, cap=1 << 22):
+    def mac_collect(self, theta_lo=0.2, theta_hi=0.9, rho_lo=0.05, rho_hi=0.9,
+                    max_count=16384, keep=1.0, seed=1, cap=1 << 22):
         n = ctypes.c_int64()
         self._check(self.lib.tree_gpu_mac_collect(self.h, theta_lo, theta_hi,
-                                                  rho_lo, rho_hi, max_count,
+                                                  rho_lo, rho_hi, max_count, keep,
                                                   seed, cap, ctypes.byref(n)))
         return n.value
 
@@ -362,7 +362,7 @@ class TreeForce:
         self._check(self.lib.tree_gpu_mac_get_model(self.h, _fp(p), _fp(s)))
         return p, s
 
-    def mac_config(self, eta=1e-5, rho_lo=0.2, rho_hi=0.9):
+    def mac_config(self, eta=1e-5, rho_lo=0.05, rho_hi=0.9):
         self._check(self.lib.tree_gpu_mac_config(self.h, eta, rho_lo, rho_hi))
 
     def timings(self) -> Timing:

@@ -683,6 +683,11 @@ __global__ void k_upward(const double* __restrict__ x,
 }
 
 // ------------------------------------------------ net-charge upward pass ----
+// unique index triples of a symmetric 3-tensor and their multiplicities
+__constant__ int kTI[10][3] = {{0, 0, 0}, {1, 1, 1}, {2, 2, 2}, {0, 0, 1}, {0, 0, 2},
+                               {0, 1, 1}, {1, 1, 2}, {0, 2, 2}, {1, 2, 2}, {0, 1, 2}};
+__constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
+
 // Combined tree (both species in one tree) for the mixed-precision walk.  Per
 // node: particle count n, centroid X (the expansion centre), net charge Q,
 // dipole D = sum q (x - X), second moment S = 1/2 sum q (x - X)(x - X)^T and
@@ -692,9 +697,16 @@ __global__ void k_upward(const double* __restrict__ x,
 // In a quasi-neutral plasma Q ~ 0 for large cells and the far field is the
 // small net (dipole/quadrupole) field, so its truncation error is relative to
 // that net field rather than to each species' monopole.
-// m64 per node (6 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
-// (Szz, Sxy) | (Syz, Szx).  mom per node (3 x float4): (Q, Dx, Dy, Dz),
-// (Sxx, Syy, Szz, Sxy), (Syz, Szx, trace S, q_ion).
+// Also the third moment T_ijk = sum q a_i a_j a_k (a = x - X), combined with
+//   T += T_c + d_i S2_jk + d_j S2_ik + d_k S2_ij + d_i d_j D_k + d_i D_j d_k
+//        + D_i d_j d_k + Q_c d_i d_j d_k      (S2 = 2 S of the child)
+// -- the octupole the quadrupole expansion leaves out, whose size sets the
+// error of accepting the cell.
+// m64 per node (11 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
+// (Szz, Sxy) | (Syz, Szx) | T in the order xxx yyy zzz xxy xxz xyy yyz xzz
+// yzz xyz.  mom per node (3 x float4): (Q, Dx, Dy, Dz), (Sxx, Syy, Szz, Sxy),
+// (Syz, Szx, trace S, q_ion); mom3 per node (3 x float4): (Txxx, Tyyy, Tzzz,
+// Txxy), (Txxz, Txyy, Tyyz, Txzz), (Tyzz, Txyz, |T|_F, 0).
 __global__ void k_upward_net(const double* __restrict__ x,
                              const uint32_t* __restrict__ vals,
                              const int8_t* __restrict__ L,
@@ -722,13 +734,16 @@ __global__ void k_upward_net(const double* __restrict__ x,
                pz = x[3 * (int64_t)o + 2];
   node_c[leaf] = make_double4(px, py, pz, -1.0);
   {
-    double2* m = mx.m64 + 6 * (int64_t)leaf;
+    double2* m = mx.m64 + kM64 * (int64_t)leaf;
     m[0] = make_double2(1.0, q);
     m[1] = make_double2(0.0, 0.0);
     m[2] = make_double2(0.0, ion ? 1.0 : 0.0);
-    m[3] = make_double2(0.0, 0.0);
-    m[4] = make_double2(0.0, 0.0);
-    m[5] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 3; u < kM64; ++u) m[u] = make_double2(0.0, 0.0);
+    float4* f3 = mx.mom3 + 3 * (int64_t)leaf;
+    f3[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f3[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f3[2] = make_float4(0.f, 0.f, 0.f, 0.f);
     float4* f = mx.mom + 3 * (int64_t)leaf;
     f[0] = make_float4((float)q, 0.f, 0.f, 0.f);
     f[1] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -756,7 +771,7 @@ __global__ void k_upward_net(const double* __restrict__ x,
     int c = cur + 1;
     while (c < end) {
       const double4 cc = ldcg_d4(&node_c[c]);
-      const double nc = __ldcg(mx.m64 + 6 * (int64_t)c).x;
+      const double nc = __ldcg(mx.m64 + kM64 * (int64_t)c).x;
       nsum += nc;
       X0 += nc * cc.x;
       X1 += nc * cc.y;
@@ -774,14 +789,36 @@ __global__ void k_upward_net(const double* __restrict__ x,
     // pass 2: moments about the centroid
     double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
     double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
+    double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     c = cur + 1;
     while (c < end) {
       const double4 cc = ldcg_d4(&node_c[c]);
-      const double2* cm = mx.m64 + 6 * (int64_t)c;
+      const double2* cm = mx.m64 + kM64 * (int64_t)c;
       const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
                     a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
       const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
       const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
+      {  // third moment, parallel axis
+        const double d[3] = {ex, ey, ez};
+        const double Dc[3] = {dcx, dcy, dcz};
+        const double S2[3][3] = {{2 * a3.x, 2 * a4.y, 2 * a5.y},
+                                 {2 * a4.y, 2 * a3.y, 2 * a5.x},
+                                 {2 * a5.y, 2 * a5.x, 2 * a4.x}};
+        double Tc[10];
+#pragma unroll
+        for (int u = 0; u < 5; ++u) {
+          const double2 t2 = __ldcg(cm + 6 + u);
+          Tc[2 * u] = t2.x;
+          Tc[2 * u + 1] = t2.y;
+        }
+#pragma unroll
+        for (int u = 0; u < 10; ++u) {
+          const int i = kTI[u][0], j = kTI[u][1], k = kTI[u][2];
+          T[u] += Tc[u] + d[i] * S2[j][k] + d[j] * S2[i][k] + d[k] * S2[i][j] +
+                  d[i] * d[j] * Dc[k] + d[i] * Dc[j] * d[k] + Dc[i] * d[j] * d[k] +
+                  qc * d[i] * d[j] * d[k];
+        }
+      }
       Q += qc;
       qi += a2.y;
       Dx += dcx + qc * ex;
@@ -801,13 +838,22 @@ __global__ void k_upward_net(const double* __restrict__ x,
     double smax = smax0;
     for (int l = 0; l < lev; ++l) smax = smax * 0.5;
     node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
-    double2* m = mx.m64 + 6 * (int64_t)cur;
+    double2* m = mx.m64 + kM64 * (int64_t)cur;
     m[0] = make_double2(nsum, Q);
     m[1] = make_double2(Dx, Dy);
     m[2] = make_double2(Dz, qi);
     m[3] = make_double2(Sxx, Syy);
     m[4] = make_double2(Szz, Sxy);
     m[5] = make_double2(Syz, Szx);
+    double tn = 0.0;
+#pragma unroll
+    for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+#pragma unroll
+    for (int u = 0; u < 10; ++u) tn += kTMult[u] * T[u] * T[u];
+    float4* f3 = mx.mom3 + 3 * (int64_t)cur;
+    f3[0] = make_float4((float)T[0], (float)T[1], (float)T[2], (float)T[3]);
+    f3[1] = make_float4((float)T[4], (float)T[5], (float)T[6], (float)T[7]);
+    f3[2] = make_float4((float)T[8], (float)T[9], (float)sqrt(tn), 0.f);
     float4* f = mx.mom + 3 * (int64_t)cur;
     f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
     f[1] = make_float4((float)Sxx, (float)Syy, (float)Szz, (float)Sxy);

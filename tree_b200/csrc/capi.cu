@@ -252,6 +252,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
       lm.packed = h->mlp_packed;
       lm.fmin = h->mlp_stats + 32;
       lm.fmax = h->mlp_stats + 48;
+      lm.margins = h->mlp_stats + 64;
       lm.f_prev = h->f;  // each target's previous force, read before it is overwritten
       lm.eta = h->mac_eta;
       lm.rho_lo = h->mac_rho_lo;
@@ -662,12 +663,15 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream) {
 }
 
 int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
-                        int32_t blocks_per_sm) {
+                        int32_t blocks_per_sm, int32_t order) {
   if (!h) return TREE_GPU_ERR_ARG;
-  if (bucket < 1 || bucket > 8 || blocks_per_sm < 1 || blocks_per_sm > 4)
-    return fail(h, TREE_GPU_ERR_ARG, "bucket must be 1..8, blocks_per_sm 1..4");
+  if (bucket < 1 || bucket > 8 || blocks_per_sm < 1 || blocks_per_sm > 4 ||
+      order < 2 || order > 3)
+    return fail(h, TREE_GPU_ERR_ARG,
+                "bucket must be 1..8, blocks_per_sm 1..4, order 2..3");
   h->tune.bucket = bucket;
   h->tune.blocks_per_sm = blocks_per_sm;
+  h->tune.order = order;
   return TREE_GPU_OK;
 }
 
@@ -704,7 +708,7 @@ namespace {
 int ensure_model_buffers(tree_gpu_handle* h) {
   if (h->mlp_params) return TREE_GPU_OK;
   CK(cudaMalloc(&h->mlp_params, sizeof(float) * tg::kMlpParams));
-  CK(cudaMalloc(&h->mlp_stats, sizeof(float) * 64));
+  CK(cudaMalloc(&h->mlp_stats, sizeof(float) * TREE_GPU_MLP_STATS));
   CK(cudaMalloc(&h->mlp_packed, sizeof(tg::MlpPacked)));
   return TREE_GPU_OK;
 }
@@ -715,10 +719,11 @@ extern "C" {
 
 int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
                          double rho_lo, double rho_hi, int32_t max_count,
-                         uint64_t seed, int64_t cap, int64_t* n_total) {
+                         float keep, uint64_t seed, int64_t cap,
+                         int64_t* n_total) {
   if (!h) return TREE_GPU_ERR_ARG;
   if (!(theta_lo > 0 && theta_hi >= theta_lo && rho_lo > 0 && rho_hi >= rho_lo) ||
-      cap <= 0 || cap > (int64_t)0x7fffffff || max_count < 2)
+      cap <= 0 || cap > (int64_t)0x7fffffff || max_count < 2 || !(keep > 0.f && keep <= 1.f))
     return fail(h, TREE_GPU_ERR_ARG, "bad sampling arguments");
   if (h->n == 0) return fail(h, TREE_GPU_ERR_STATE, "no particles");
   if (h->smp_cap != cap) {
@@ -749,6 +754,7 @@ int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
   tg::SampleArgs a;
   a.node_c = h->b.node_c;
   a.mom = h->mb.mom;
+  a.mom3 = h->mb.mom3;
   a.geom = h->mb.geom;
   a.m64 = h->mb.m64;
   a.kids = h->mb.kids;
@@ -765,6 +771,8 @@ int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
   a.rho_hi = (float)rho_hi;
   a.seed = (uint32_t)(seed ^ (seed >> 32));
   a.max_count = max_count;
+  a.keep = keep;
+  a.order = h->tune.order;
   a.lam_ei = (float)h->lam[1];
   a.feats = h->smp_feats;
   a.labels = h->smp_labels;
@@ -835,7 +843,8 @@ int tree_gpu_mac_set_model(tree_gpu_handle* h, const float* params,
   if (rc) return rc;
   CK(cudaMemcpyAsync(h->mlp_params, params, sizeof(float) * tg::kMlpParams,
                      cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->mlp_stats, stats, sizeof(float) * 64, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->mlp_stats, stats, sizeof(float) * TREE_GPU_MLP_STATS,
+                     cudaMemcpyHostToDevice, h->st));
   h->timing.launches += tg::mlp_pack(h->mlp_params, h->mlp_stats, h->mlp_stats + 16,
                                      h->mlp_packed, h->st);
   CK(cudaStreamSynchronize(h->st));
@@ -847,7 +856,8 @@ int tree_gpu_mac_get_model(tree_gpu_handle* h, float* params, float* stats) {
   if (!h || !params || !stats) return TREE_GPU_ERR_ARG;
   if (!h->has_model) return fail(h, TREE_GPU_ERR_STATE, "no model");
   CK(cudaMemcpy(params, h->mlp_params, sizeof(float) * tg::kMlpParams, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(stats, h->mlp_stats, sizeof(float) * 64, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(stats, h->mlp_stats, sizeof(float) * TREE_GPU_MLP_STATS,
+                cudaMemcpyDeviceToHost));
   return TREE_GPU_OK;
 }
 
@@ -900,13 +910,13 @@ int tree_gpu_mlp_infer(const float* X, int64_t n, const float* params,
   auto al = [&](float** q, size_t cnt) { if (e == cudaSuccess) e = cudaMalloc(q, cnt * sizeof(float)); };
   al(&dX, 16 * (size_t)n);
   al(&dP, tg::kMlpParams);
-  al(&dS, 64);
+  al(&dS, TREE_GPU_MLP_STATS);
   al(&dY, (size_t)n);
   if (e == cudaSuccess) e = cudaMalloc(&dK, sizeof(tg::MlpPacked));
   if (e == cudaSuccess) {
     cudaMemcpy(dX, X, sizeof(float) * 16 * n, cudaMemcpyHostToDevice);
     cudaMemcpy(dP, params, sizeof(float) * tg::kMlpParams, cudaMemcpyHostToDevice);
-    cudaMemcpy(dS, stats, sizeof(float) * 64, cudaMemcpyHostToDevice);
+    cudaMemcpy(dS, stats, sizeof(float) * TREE_GPU_MLP_STATS, cudaMemcpyHostToDevice);
     tg::mlp_pack(dP, dS, dS + 16, dK, 0);
     tg::mlp_infer(dX, (int)n, dK, dY, 0);
     e = cudaDeviceSynchronize();

@@ -5,14 +5,16 @@
 // All 16 features are dimensionless.  With X the cell centroid, d the
 // distance from X to the group's bounding box, u the unit vector from X to
 // the group centre, s the cell's box side, dx = |X - geometric centre|, n the
-// particle count, Q/D/S the net monopole/dipole/second moment and q_ion the
-// ion count:
+// particle count, Q/D/S/T the net monopole/dipole/second/third moments and
+// q_ion the ion count:
 //   0 s/d            1 dx/d              2 |h|/d (group half-diagonal)
 //   3 log2(n)/16     4 Q/n               5 |D|/(n s)
-//   6 |S|_F/(n s^2)  7 tr S/(n s^2)      8 q_ion/n (species mix)
-//   9 D.u/(n s)      10 u.S.u/(n s^2)    11 log10(lambda_ei/d)/8
+//   6 |S|_F/(n s^2)  7 log10(|T|_F/(n s^3))/4   8 q_ion/n (species mix)
+//   9 D.u/(n s)      10 u.S.u/(n s^2)    11 T(u,u,u)/(n s^3)
 //   12 group fill    13 |G-X|/d - 1      14 log10(s/d)
-//   15 |D|/(|Q| s + |D|)
+//   15 log10(|T|_F / (n d^3)): the size of the omitted octupole field
+//      relative to the gross monopole field n/d^2 -- the analytic estimate of
+//      the label, which the network refines.
 // The label is log10(max over the group of |F_multipole - F_exact| /
 // (n / d^2)), i.e. the acceptance error relative to the cell's gross
 // monopole field (charges in units of e, Coulomb constant dropped).
@@ -29,20 +31,25 @@ struct CellGeom {   // mx.geom: (s, dx, n, -)
   float s, dx, n, pad;
 };
 
+__device__ __forceinline__ float mac_estimate(float tnorm, float n, float d) {
+  return log10f(tnorm / (n * d * d * d) + 1e-30f);
+}
+
 __device__ __forceinline__ void mac_features(
     double cx, double cy, double cz, const float4 g4, const float4 m0,
-    const float4 m1, const float4 m2, double Gx, double Gy, double Gz,
-    float hlen, float d, float n_act, float lam_ei, float f[kMacFeatures]) {
+    const float4 m1, const float4 m2, const float4 t0, const float4 t1,
+    const float4 t2, double Gx, double Gy, double Gz, float hlen, float d,
+    float n_act, float* f) {
   const float s = g4.x, dxo = g4.y, n = g4.z;
   const float Q = m0.x, Dx = m0.y, Dy = m0.z, Dz = m0.w;
   const float Sxx = m1.x, Syy = m1.y, Szz = m1.z, Sxy = m1.w;
-  const float Syz = m2.x, Szx = m2.y, trS = m2.z, qi = m2.w;
+  const float Syz = m2.x, Szx = m2.y, qi = m2.w;
   const float ux0 = (float)(Gx - cx), uy0 = (float)(Gy - cy), uz0 = (float)(Gz - cz);
   const float ul = sqrtf(ux0 * ux0 + uy0 * uy0 + uz0 * uz0);
   const float iu = ul > 0.f ? 1.f / ul : 0.f;
   const float ux = ux0 * iu, uy = uy0 * iu, uz = uz0 * iu;
   const float id = 1.f / d;
-  const float ns = n * s, ns2 = n * s * s;
+  const float ns = n * s, ns2 = ns * s, ns3 = ns2 * s;
   const float Dn = sqrtf(Dx * Dx + Dy * Dy + Dz * Dz);
   const float SF = sqrtf(Sxx * Sxx + Syy * Syy + Szz * Szz +
                          2.f * (Sxy * Sxy + Syz * Syz + Szx * Szx));
@@ -51,6 +58,12 @@ __device__ __forceinline__ void mac_features(
   const float Suy = Sxy * ux + Syy * uy + Syz * uz;
   const float Suz = Szx * ux + Syz * uy + Szz * uz;
   const float uSu = ux * Sux + uy * Suy + uz * Suz;
+  // T(u,u,u) from the 10 unique components xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz
+  const float Tuuu = t0.x * ux * ux * ux + t0.y * uy * uy * uy + t0.z * uz * uz * uz +
+                     3.f * (t0.w * ux * ux * uy + t1.x * ux * ux * uz + t1.y * ux * uy * uy +
+                            t1.z * uy * uy * uz + t1.w * ux * uz * uz + t2.x * uy * uz * uz) +
+                     6.f * t2.y * ux * uy * uz;
+  const float TF = t2.z;
   f[0] = s * id;
   f[1] = dxo * id;
   f[2] = hlen * id;
@@ -58,15 +71,15 @@ __device__ __forceinline__ void mac_features(
   f[4] = Q / n;
   f[5] = Dn / ns;
   f[6] = SF / ns2;
-  f[7] = trS / ns2;
+  f[7] = log10f(TF / ns3 + 1e-12f) * 0.25f;
   f[8] = qi / n;
   f[9] = Du / ns;
   f[10] = uSu / ns2;
-  f[11] = fmaxf(log10f(lam_ei * id), -8.f) * 0.125f;
+  f[11] = Tuuu / ns3;
   f[12] = n_act * (1.f / 32.f);
   f[13] = ul * id - 1.f;
   f[14] = log10f(s * id);
-  f[15] = Dn / (fabsf(Q) * s + Dn + 1e-30f);
+  f[15] = mac_estimate(TF, n, d);
 }
 
 // Distance from a point to an axis-aligned box (centre G, half extents h).

@@ -5,11 +5,14 @@
 // opening angle theta_g drawn per group from [theta_lo, theta_hi].  Every cell
 // it tests whose acceptance ratio rho = s / (d - dx) lies in the band
 // [rho_lo, rho_hi] becomes one sample: its 16 features (mac.cuh) and the
-// exact error of accepting it for the group -- the FP64 multipole field
-// (net monopole + dipole + quadrupole about the centroid) minus the FP64
-// Coulomb sum over the cell's particles, maximised over the group's targets.
+// exact error of accepting it for the group -- the FP64 multipole field at
+// the walk's expansion order (net monopole + dipole + quadrupole, and the
+// octupole for order 3, about the centroid) minus the FP64 Coulomb sum over
+// the cell's particles, maximised over the group's targets.
 // Cells with more than max_count particles are not sampled; the walk treats
 // them with the fixed-theta test (they fall outside the training range).
+// Each candidate is kept with probability `keep` (hash of cell and group) so
+// that a bounded sample buffer spans many clouds.
 #include "build.h"
 #include "internal.cuh"
 #include "mac.cuh"
@@ -76,7 +79,8 @@ __global__ void __launch_bounds__(32 * kSmpWarps)
           d = dist_to_box(c.x, c.y, c.z, Gx, Gy, Gz, hx, hy, hz);
           const double margin = d - (double)g4.y;
           const double rho = margin > 0.0 ? (double)g4.x / margin : 1e30;
-          sample = rho >= a.rho_lo && rho <= a.rho_hi && g4.z <= (float)a.max_count;
+          sample = rho >= a.rho_lo && rho <= a.rho_hi && g4.z <= (float)a.max_count &&
+                   hash_unit((uint32_t)node * 2654435761u + (uint32_t)g, a.seed ^ 0x5bd1e995u) < a.keep;
           open = !(rho < (double)theta_g);
         }
       }
@@ -95,16 +99,15 @@ __global__ void __launch_bounds__(32 * kSmpWarps)
         if (lane == L) {
           const float4 g4 = __ldg(&a.geom[cn]);
           const float4* mp = a.mom + 3 * (int64_t)cn;
-          float f[kMacFeatures];
+          const float4* tp = a.mom3 + 3 * (int64_t)cn;
           mac_features(c.x, c.y, c.z, g4, __ldg(mp), __ldg(mp + 1), __ldg(mp + 2),
-                       Gx, Gy, Gz, hlen, (float)dd, (float)n_act, a.lam_ei, f);
-#pragma unroll
-          for (int k = 0; k < kMacFeatures; ++k) a.feats[(int64_t)idx * kMacFeatures + k] = f[k];
+                       __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), Gx, Gy, Gz, hlen,
+                       (float)dd, (float)n_act, a.feats + (int64_t)idx * kMacFeatures);
           a.extra[2 * (int64_t)idx] = (float)theta_g;
           a.extra[2 * (int64_t)idx + 1] = (float)(g4.x / (dd - g4.y));
         }
         // exact error of accepting cn for every target of the group (FP64)
-        const double2* m = a.m64 + 6 * (int64_t)cn;
+        const double2* m = a.m64 + kM64 * (int64_t)cn;
         const double2 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3], m4 = m[4], m5 = m[5];
         const double Q = m0.y, Dx = m1.x, Dy = m1.y, Dz = m2.x;
         const double Sxx = m3.x, Syy = m3.y, Szz = m4.x, Sxy = m4.y, Syz = m5.x, Szx = m5.y;
@@ -121,6 +124,27 @@ __global__ void __launch_bounds__(32 * kSmpWarps)
         double fx = gg * ex - ri3 * Dx - 6.0 * ri5 * Sx;
         double fy = gg * ey - ri3 * Dy - 6.0 * ri5 * Sy;
         double fz = gg * ez - ri3 * Dz - 6.0 * ri5 * Sz;
+        if (a.order >= 3) {  // octupole term, as in the walk (walk_mixed.cu)
+          double T[10];
+#pragma unroll
+          for (int u2 = 0; u2 < 5; ++u2) {
+            const double2 t2 = m[6 + u2];
+            T[2 * u2] = t2.x;
+            T[2 * u2 + 1] = t2.y;
+          }
+          const double xx = ex * ex, yy = ey * ey, zz = ez * ez;
+          const double xy2 = 2 * ex * ey, xz2 = 2 * ex * ez, yz2 = 2 * ey * ez;
+          const double Tx = T[0] * xx + T[5] * yy + T[7] * zz + T[3] * xy2 + T[4] * xz2 + T[9] * yz2;
+          const double Ty = T[3] * xx + T[1] * yy + T[8] * zz + T[5] * xy2 + T[9] * xz2 + T[6] * yz2;
+          const double Tz = T[4] * xx + T[6] * yy + T[2] * zz + T[9] * xy2 + T[7] * xz2 + T[8] * yz2;
+          const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
+          const double T3 = ex * Tx + ey * Ty + ez * Tz, Vd = Vx * ex + Vy * ey + Vz * ez;
+          const double ri7 = ri5 * ri2;
+          const double g3 = ri7 * (17.5 * ri2 * T3 - 7.5 * Vd);
+          fx += g3 * ex - 7.5 * ri7 * Tx + 1.5 * ri5 * Vx;
+          fy += g3 * ey - 7.5 * ri7 * Ty + 1.5 * ri5 * Vy;
+          fz += g3 * ez - 7.5 * ri7 * Tz + 1.5 * ri5 * Vz;
+        }
         const int j0 = __ldg(&a.first[cn]), j1 = j0 + __ldg(&a.count[cn]);
         for (int j = j0; j < j1; ++j) {
           const double4 s = a.xs[j];

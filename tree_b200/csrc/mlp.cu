@@ -265,10 +265,9 @@ __global__ void k_mlp_infer(const float* __restrict__ X, int n,
   const int ntiles = (n + 31) / 32;
   for (int tile = blockIdx.x * kMlpWarps + w; tile < ntiles; tile += gridDim.x * kMlpWarps) {
     const int s = tile * 32 + lane;
-    float x[kMlpIn];
 #pragma unroll
-    for (int k = 0; k < kMlpIn; ++k) x[k] = s < n ? X[(int64_t)s * kMlpIn + k] : 0.f;
-    const float yy = mlp_forward_warp(x, xs[w], h1[w], P, lane);
+    for (int k = 0; k < kMlpIn; ++k) xs[w][lane * kMlpIn + k] = s < n ? X[(int64_t)s * kMlpIn + k] : 0.f;
+    const float yy = mlp_forward_warp(xs[w], h1[w], P, lane);
     if (s < n) y[s] = yy;
   }
 }
@@ -362,6 +361,32 @@ __global__ void k_feat_stats(const float* __restrict__ X, int n, float* stats) {
   }
 }
 
+// Keys ordering label - estimate (feature 15) for the margin quantiles.
+__global__ void k_margin_keys(const float* __restrict__ X, const float* __restrict__ Y,
+                              int n, uint64_t* keys, uint32_t* vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float d = Y[i] - X[(int64_t)i * kMlpIn + (kMlpIn - 1)];
+  uint32_t u = __float_as_uint(d);
+  u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  keys[i] = u;
+  vals[i] = (uint32_t)i;
+}
+
+__global__ void k_margin_store(const uint64_t* __restrict__ keys, int n,
+                               float* stats) {
+  if (threadIdx.x != 0) return;
+  auto val = [&](double q) {
+    int64_t i = (int64_t)(q * (n - 1));
+    uint32_t u = (uint32_t)keys[i];
+    u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    return __uint_as_float(u);
+  };
+  stats[4 * kMlpIn] = val(0.01);       // m_lo
+  stats[4 * kMlpIn + 1] = val(0.99);   // m_hi
+  for (int k = 2; k < 8; ++k) stats[4 * kMlpIn + k] = 0.f;
+}
+
 __global__ void k_shuffle_keys(uint64_t* keys, uint32_t* vals, int n, uint64_t seed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -437,6 +462,10 @@ int mlp_train(const float* X, const float* Y, int n, int epochs, int batch,
     k_shuffle_keys<<<(n + 255) / 256, 256, 0, st>>>(k0, v0, n, seed);
     radix_sort(k0, v0, k1, v1, n, hist, part, st);
     k_normalize_gather<<<(n + 255) / 256, 256, 0, st>>>(X, Y, v0, n, stats, Xn, Yn);
+    // margins: 1% and 99% quantiles of (label - analytic estimate)
+    k_margin_keys<<<(n + 255) / 256, 256, 0, st>>>(X, Y, n, k0, v0);
+    radix_sort(k0, v0, k1, v1, n, hist, part, st);
+    k_margin_store<<<1, 32, 0, st>>>(k0, n, stats);
     const int nb = (n + batch - 1) / batch;
     int t = 0;
     for (int ep = 0; ep < epochs; ++ep) {

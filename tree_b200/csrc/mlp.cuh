@@ -83,12 +83,12 @@ __device__ __forceinline__ void load_b_f32(uint32_t b[2], const float* buf,
   b[1] = pack_bf16x2(buf[(k + 8) * sk + n * sn], buf[(k + 9) * sk + n * sn]);
 }
 
-// Inference for the 32 lanes' feature vectors.  x: this lane's 16 raw
-// features; xs_tile: 32x16 FP32 per-warp scratch; h1_tile: 32x64 BF16
-// per-warp scratch; P: packed weights in shared memory.  Returns this lane's
-// prediction.  All 32 lanes must call it.
-__device__ __forceinline__ float mlp_forward_warp(const float x[kMlpIn],
-                                                  float* xs_tile,
+// Inference for the 32 lanes' feature vectors.  xs_tile: 32x16 FP32
+// per-warp scratch whose row `lane` holds this lane's raw features on entry
+// (normalised in place); h1_tile: 32x64 BF16 per-warp scratch; P: packed
+// weights in shared memory.  Returns this lane's prediction.  All 32 lanes
+// must call it.
+__device__ __forceinline__ float mlp_forward_warp(float* xs_tile,
                                                   __nv_bfloat16* h1_tile,
                                                   const MlpPacked& P,
                                                   int lane) {
@@ -99,7 +99,8 @@ __device__ __forceinline__ float mlp_forward_warp(const float x[kMlpIn],
   const float* mu = P.vec + 3 * kMlpH + 1;
   const float* isd = mu + kMlpIn;
 #pragma unroll
-  for (int k = 0; k < kMlpIn; ++k) xs_tile[lane * kMlpIn + k] = (x[k] - mu[k]) * isd[k];
+  for (int k = 0; k < kMlpIn; ++k)
+    xs_tile[lane * kMlpIn + k] = (xs_tile[lane * kMlpIn + k] - mu[k]) * isd[k];
   __syncwarp();
   const int g = lane >> 2, t = lane & 3;
   // layer 1: H1 = relu(X W1 + b1), stored as BF16 rows
@@ -107,7 +108,7 @@ __device__ __forceinline__ float mlp_forward_warp(const float x[kMlpIn],
   for (int mt = 0; mt < 2; ++mt) {
     uint32_t a[4];
     load_a_f32<false>(a, xs_tile, kMlpIn, 1, 16 * mt, 0, lane);
-#pragma unroll
+#pragma unroll 2
     for (int nt = 0; nt < 8; ++nt) {
       const uint2 bb = P.w1f[nt * 32 + lane];
       const uint32_t b[2] = {bb.x, bb.y};
@@ -125,27 +126,21 @@ __device__ __forceinline__ float mlp_forward_warp(const float x[kMlpIn],
   __syncwarp();
   // layer 2 + 3: y = relu(H1 W2 + b2) . w3 + b3, one 16x8 tile at a time
   float part[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [mt][row g / g+8]
+  const uint32_t* h = reinterpret_cast<const uint32_t*>(h1_tile);
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
-    uint32_t a[4][4];
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      const int r0 = 16 * mt + g, r1 = r0 + 8;
-      const int c0 = 16 * kt + 2 * t, c1 = c0 + 8;
-      const uint32_t* h = reinterpret_cast<const uint32_t*>(h1_tile);
-      a[kt][0] = h[(r0 * kMlpH + c0) >> 1];
-      a[kt][1] = h[(r1 * kMlpH + c0) >> 1];
-      a[kt][2] = h[(r0 * kMlpH + c1) >> 1];
-      a[kt][3] = h[(r1 * kMlpH + c1) >> 1];
-    }
-#pragma unroll
+#pragma unroll 1
     for (int nt = 0; nt < 8; ++nt) {
       float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int kt = 0; kt < 4; ++kt) {
+        const int r0 = 16 * mt + g, r1 = r0 + 8;
+        const int c0 = 16 * kt + 2 * t, c1 = c0 + 8;
+        const uint32_t a[4] = {h[(r0 * kMlpH + c0) >> 1], h[(r1 * kMlpH + c0) >> 1],
+                               h[(r0 * kMlpH + c1) >> 1], h[(r1 * kMlpH + c1) >> 1]};
         const uint2 bb = P.w2f[(kt * 8 + nt) * 32 + lane];
         const uint32_t b[2] = {bb.x, bb.y};
-        mma_bf16_16816(c, a[kt], b, c);
+        mma_bf16_16816(c, a, b, c);
       }
       const int col = 8 * nt + 2 * t;
       part[mt][0] += fmaxf(c[0] + b2[col], 0.f) * w3[col] +
@@ -158,9 +153,9 @@ __device__ __forceinline__ float mlp_forward_warp(const float x[kMlpIn],
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      part[mt][h] += __shfl_xor_sync(0xffffffffu, part[mt][h], 1);
-      part[mt][h] += __shfl_xor_sync(0xffffffffu, part[mt][h], 2);
+    for (int hh = 0; hh < 2; ++hh) {
+      part[mt][hh] += __shfl_xor_sync(0xffffffffu, part[mt][hh], 1);
+      part[mt][hh] += __shfl_xor_sync(0xffffffffu, part[mt][hh], 2);
     }
   // row r = 16 mt + 8 h + g lives in lanes 4g..4g+3
   const int src = 4 * (lane & 7);

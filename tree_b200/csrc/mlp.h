@@ -20,8 +20,8 @@ int mlp_infer(const float* X, int n, const MlpPacked* packed, float* y,
               cudaStream_t st);
 
 // Trains from scratch on n device samples (raw features X, labels Y):
-// computes the feature statistics into stats (64 floats: mean, 1/std, min,
-// max), shuffles, runs `epochs` of Adam with mini-batches of `batch` and a
+// computes the feature statistics into stats (72 floats: mean, 1/std, min,
+// max, then the 1% and 99% quantiles of label minus feature 15), shuffles, runs `epochs` of Adam with mini-batches of `batch` and a
 // cosine learning-rate decay, and leaves the parameters in params.  Returns
 // 0 or a CUDA error code; loss_per_epoch (host, may be null) gets the mean
 // pinball loss of every epoch.
@@ -32,6 +32,7 @@ int mlp_train(const float* X, const float* Y, int n, int epochs, int batch,
 struct SampleArgs {
   const double4* node_c;
   const float4* mom;
+  const float4* mom3;
   const float4* geom;
   const double2* m64;
   const int32_t* kids;
@@ -45,6 +46,8 @@ struct SampleArgs {
   float theta_lo, theta_hi, rho_lo, rho_hi;
   uint32_t seed;
   int max_count;
+  float keep;     // probability of keeping a candidate sample
+  int order;      // expansion order of the labels (the walk's)
   float lam_ei;
   float* feats;   // cap x 16
   float* labels;  // cap

@@ -37,10 +37,18 @@ constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
 constexpr int kMaxBucket = 8;
 constexpr int kMaxBlocksPerSm = 4;
 
+constexpr int kCandRing = 64;     // power of two, > 31 + 32
+
 struct WarpSmem {
   int m2p[kM2pRing];
   int p2p[kP2pRing];
-  float4 cell[32 * 4];   // (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion), (Sxx, Syy, Szz, Sxy), (Syz, Szx, tr, -)
+  int cq_node[kCandRing];  // learned-MAC candidates waiting for a full batch
+  float cq_d[kCandRing];
+  float cq_b[kCandRing];
+  // staged cells, 8 float4 each: (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion),
+  // (Sxx, Syy, Szz, Sxy), (Syz, Szx, tr S, -), (Txxx, Tyyy, Tzzz, Txxy),
+  // (Txxz, Txyy, Tyyz, Txzz), (Tyzz, Txyz, -, -), (Vx, Vy, Vz, -)
+  float4 cell[32 * 8];
   float4 part[32 * 2];   // (hi xyz, sorted index bits), (lo xyz, ion?)
 };
 
@@ -59,6 +67,7 @@ struct MixedArgs {
   int32_t* control;
   int32_t* stack;
   int bucket;
+  int p2p_max;  // accepted cells with at most this many particles go to P2P
   int physics;
   float inv_lam2_ee, inv_lam2_ei, inv_lam2_ii;
   float inv_lam_ee, inv_lam_ei, inv_lam_ii;
@@ -74,6 +83,8 @@ struct MixedArgs {
   const float* fmin;
   const float* fmax;
   const float4* geom;
+  const float4* mom3;
+  const float* margins;  // (m_lo, m_hi) of the model
   const double* f_prev;
   float eta_over_eps;
   float rho_lo, rho_hi;
@@ -115,12 +126,17 @@ __device__ __forceinline__ double warp_max_d(double v) {
 }
 
 // ---------------------------------------------------------------- M2P ----
-// 74 flop per entry (FMA = 2): net monopole Q, dipole D and traceful second
-// moment S about the cell centroid.  With d = target - centroid:
+// Net monopole Q, dipole D, second moment S = 1/2 sum q a a^T (traceful) and,
+// for ORDER 3, third moment T = sum q a a a about the cell centroid.  With
+// d = target - centroid, r = |d|:
 //   phi = Q/r + D.d/r^3 + (3 d.S.d - r^2 tr S)/r^5
-//   -grad phi = g d - D/r^3 - 6 S d/r^5,  g = Q/r^3 + (3 D.d + 15 d.S.d/r^2 - 3 tr S)/r^5
-// The ion part of phi for the Epot_e/Epot_i split is taken at monopole order
-// (q_ion / r).
+//         + (5 T(d,d,d) - 3 r^2 V.d)/(2 r^7),      V_k = T_iik
+//   -grad phi = g d - D/r^3 - 6 S d/r^5 - 7.5 T(.,d,d)/r^7 + 1.5 V/r^5,
+//   g = Q/r^3 + (3 D.d + 15 d.S.d/r^2 - 3 tr S)/r^5
+//       + (17.5 T(d,d,d)/r^2 - 7.5 V.d)/r^7.
+// 60 flop per entry at ORDER 2, 110 at ORDER 3 (FMA = 2).  The ion part of
+// phi for the Epot_e/Epot_i split is taken at monopole order (q_ion / r).
+template <int ORDER>
 __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
                                          const MixedArgs& a, double Gx,
                                          double Gy, double Gz, float tx,
@@ -131,18 +147,27 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     double4 c = ldg_d4(&a.node_c[node]);
     const float4* mp = a.mom + 3 * (int64_t)node;
     float4 m0 = __ldg(mp), m1 = __ldg(mp + 1), m2 = __ldg(mp + 2);
-    sm.cell[4 * lane] = make_float4((float)(c.x - Gx), (float)(c.y - Gy),
-                                    (float)(c.z - Gz), m0.x);
-    sm.cell[4 * lane + 1] = make_float4(m0.y, m0.z, m0.w, m2.w);
-    sm.cell[4 * lane + 2] = m1;
-    sm.cell[4 * lane + 3] = make_float4(m2.x, m2.y, m2.z, 0.f);
+    float4* cl = sm.cell + 8 * lane;
+    cl[0] = make_float4((float)(c.x - Gx), (float)(c.y - Gy), (float)(c.z - Gz), m0.x);
+    cl[1] = make_float4(m0.y, m0.z, m0.w, m2.w);
+    cl[2] = m1;
+    cl[3] = make_float4(m2.x, m2.y, m2.z, 0.f);
+    if (ORDER >= 3) {
+      const float4* tp = a.mom3 + 3 * (int64_t)node;
+      const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+      cl[4] = t0;
+      cl[5] = t1;
+      cl[6] = t2;
+      // V_k = T_iik: order xxx yyy zzz xxy | xxz xyy yyz xzz | yzz xyz
+      cl[7] = make_float4(t0.x + t1.y + t1.w, t0.w + t0.y + t2.x, t1.x + t1.z + t0.z, 0.f);
+    }
   }
   __syncwarp();
   float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
 #pragma unroll 2
   for (int k = 0; k < cnt; ++k) {
-    const float4 A = sm.cell[4 * k], B = sm.cell[4 * k + 1];
-    const float4 C = sm.cell[4 * k + 2], E = sm.cell[4 * k + 3];
+    const float4* cl = sm.cell + 8 * k;
+    const float4 A = cl[0], B = cl[1], C = cl[2], E = cl[3];
     const float dx = tx - A.x, dy = ty - A.y, dz = tz - A.z;
     // accepted cells are farther than rcrit >= 0; the floor only guards a
     // zero-size cell against an FP32 distance of 0
@@ -158,13 +183,33 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     const float u = fmaf(dx, Sx, fmaf(dy, Sy, dz * Sz));
     const float Dd = fmaf(B.x, dx, fmaf(B.y, dy, B.z * dz));
     const float ur2 = u * rinv2;
-    const float g = fmaf(A.w, rinv3,
-                         rinv5 * fmaf(3.f, Dd, fmaf(15.f, ur2, -3.f * E.z)));
+    float g = fmaf(A.w, rinv3, rinv5 * fmaf(3.f, Dd, fmaf(15.f, ur2, -3.f * E.z)));
     const float h6 = 6.f * rinv5;
-    fx = fmaf(g, dx, fmaf(-h6, Sx, fmaf(-rinv3, B.x, fx)));
-    fy = fmaf(g, dy, fmaf(-h6, Sy, fmaf(-rinv3, B.y, fy)));
-    fz = fmaf(g, dz, fmaf(-h6, Sz, fmaf(-rinv3, B.z, fz)));
-    const float ph = fmaf(A.w, rinv, rinv3 * (Dd + fmaf(3.f, ur2, -E.z)));
+    float gx = fmaf(-h6, Sx, -rinv3 * B.x);
+    float gy = fmaf(-h6, Sy, -rinv3 * B.y);
+    float gz = fmaf(-h6, Sz, -rinv3 * B.z);
+    float ph = fmaf(A.w, rinv, rinv3 * (Dd + fmaf(3.f, ur2, -E.z)));
+    if (ORDER >= 3) {
+      const float4 T0 = cl[4], T1 = cl[5], T2 = cl[6], V = cl[7];
+      // T(., d, d): xxx yyy zzz xxy | xxz xyy yyz xzz | yzz xyz
+      const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+      const float xy2 = 2.f * dx * dy, xz2 = 2.f * dx * dz, yz2 = 2.f * dy * dz;
+      const float Tx = fmaf(T0.x, xx, fmaf(T1.y, yy, fmaf(T1.w, zz, fmaf(T0.w, xy2, fmaf(T1.x, xz2, T2.y * yz2)))));
+      const float Ty = fmaf(T0.w, xx, fmaf(T0.y, yy, fmaf(T2.x, zz, fmaf(T1.y, xy2, fmaf(T2.y, xz2, T1.z * yz2)))));
+      const float Tz = fmaf(T1.x, xx, fmaf(T1.z, yy, fmaf(T0.z, zz, fmaf(T2.y, xy2, fmaf(T1.w, xz2, T2.x * yz2)))));
+      const float T3 = fmaf(dx, Tx, fmaf(dy, Ty, dz * Tz));
+      const float Vd = fmaf(V.x, dx, fmaf(V.y, dy, V.z * dz));
+      const float rinv7 = rinv5 * rinv2;
+      g = fmaf(rinv7, fmaf(17.5f * rinv2, T3, -7.5f * Vd), g);
+      const float h75 = -7.5f * rinv7, h15 = 1.5f * rinv5;
+      gx = fmaf(h75, Tx, fmaf(h15, V.x, gx));
+      gy = fmaf(h75, Ty, fmaf(h15, V.y, gy));
+      gz = fmaf(h75, Tz, fmaf(h15, V.z, gz));
+      ph = fmaf(rinv7, fmaf(2.5f, T3, -1.5f * r2 * Vd), ph);
+    }
+    fx += fmaf(g, dx, gx);
+    fy += fmaf(g, dy, gy);
+    fz += fmaf(g, dz, gz);
     pa += ph;
     pi = fmaf(B.w, rinv, pi);
   }
@@ -292,10 +337,12 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
 template <bool LEARNED>
 constexpr size_t walk_smem_bytes() {
   return sizeof(WarpSmem) * kMxWarps +
-         (LEARNED ? sizeof(MlpPacked) + sizeof(__nv_bfloat16) * 32 * kMlpH * kMxWarps : 0);
+         (LEARNED ? sizeof(MlpPacked) + sizeof(__nv_bfloat16) * 32 * kMlpH * kMxWarps +
+                        sizeof(float) * 2 * kMacFeatures
+                  : 0);
 }
 
-template <int PHYS, bool RDF, bool LEARNED>
+template <int PHYS, bool RDF, bool LEARNED, int ORDER>
 __global__ void __launch_bounds__(kMxThreads, 2)
     k_walk_mixed(MixedArgs a) {
   extern __shared__ float4 dyn_smem[];
@@ -312,13 +359,17 @@ __global__ void __launch_bounds__(kMxThreads, 2)
     __syncthreads();
   }
   __nv_bfloat16* h1_tile = h1_all + (size_t)wib * 32 * kMlpH;
-  float fmin_r[kMacFeatures], fmax_r[kMacFeatures];
+  // training range of the features (fmin | fmax), shared by the block
+  float* frange = reinterpret_cast<float*>(h1_all + (size_t)kMxWarps * 32 * kMlpH);
+  float m_lo = 0.f, m_hi = 0.f;
   if (LEARNED) {
-#pragma unroll
-    for (int k = 0; k < kMacFeatures; ++k) {
-      fmin_r[k] = __ldg(&a.fmin[k]);
-      fmax_r[k] = __ldg(&a.fmax[k]);
+    m_lo = __ldg(&a.margins[0]);
+    m_hi = __ldg(&a.margins[1]);
+    if (threadIdx.x < kMacFeatures) {
+      frange[threadIdx.x] = __ldg(&a.fmin[threadIdx.x]);
+      frange[kMacFeatures + threadIdx.x] = __ldg(&a.fmax[threadIdx.x]);
     }
+    __syncthreads();
   }
   const int gwarp = blockIdx.x * kMxWarps + wib;
   int32_t* stack = a.stack + (int64_t)gwarp * kStackCap;
@@ -364,97 +415,128 @@ __global__ void __launch_bounds__(kMxThreads, 2)
     long long n_m2p = 0, n_p2p = 0;
     unsigned n_mlp = 0, n_fallback = 0;  // per lane: cells this lane sent to the MLP
     bool overflow = false;
-    while (ssize > 0) {
-      const int nb = min(32, ssize);
-      const int node = lane < nb ? stack[ssize - 1 - lane] : -1;
-      ssize -= nb;
-      __syncwarp();
+    int cqh = 0, cqt = 0;  // learned-MAC candidate ring (warp-uniform)
+    while (ssize > 0 || cqt > cqh) {
+      int node = -1;
       int action = 0, pfirst = 0, pcnt = 0;  // 1 far field, 2 particles, 3 open
-      bool cand = false;                       // 4: left to the learned MAC
-      float cand_d = 0.f;
-      double4 c;
-      if (node >= 0) {
-        c = ldg_d4(&a.node_c[node]);
-        if (c.w < 0.0) {
-          action = 2;
-          pfirst = __ldg(&a.first[node]);
-          pcnt = 1;
-        } else {
-          // group MAC: rcrit below the distance from the centroid to the box
-          const double ex = fmax(fabs(c.x - Gx) - hx, 0.0);
-          const double ey = fmax(fabs(c.y - Gy) - hy, 0.0);
-          const double ez = fmax(fabs(c.z - Gz) - hz, 0.0);
-          const double d2 = ex * ex + ey * ey + ez * ez;
-          bool accept = c.w * c.w < d2;
-          if (LEARNED && budget > 0.f) {
-            // band of the learned criterion: rho = s / (d - dx)
-            const float4 g4 = __ldg(&a.geom[node]);
-            const double dd = sqrt(d2);
-            const double margin = dd - (double)g4.y;
-            const float rho = margin > 0.0 ? (float)((double)g4.x / margin) : 3.0e38f;
-            if (rho < a.rho_lo) accept = true;
-            else if (rho > a.rho_hi) accept = false;
-            else {
-              cand = true;
-              cand_d = (float)dd;
-            }
-          }
-          if (accept && !cand) {
-            action = 1;
-          } else if (cand) {
-            action = 4;  // decided by the network below
-          } else {
-            const int cnt = __ldg(&a.count[node]);
-            if (cnt <= a.bucket) {
-              action = 2;
-              pfirst = __ldg(&a.first[node]);
-              pcnt = cnt;
-            } else {
-              action = 3;
-            }
-          }
-        }
-      }
-      if (LEARNED && __any_sync(0xffffffffu, cand)) {
-        float feat[kMacFeatures];
+      if (LEARNED && (cqt - cqh >= 32 || (ssize == 0 && cqt > cqh))) {
+        // ---- a batch of queued candidates goes through the network ----
+        const int nb = min(32, cqt - cqh);
+        bool cand = lane < nb;
+        float cand_d = 0.f, cand_B = 0.f;
         if (cand) {
+          const int q = (cqh + lane) & (kCandRing - 1);
+          node = sm.cq_node[q];
+          cand_d = sm.cq_d[q];
+          cand_B = sm.cq_b[q];
+        }
+        cqh += nb;
+        __syncwarp();
+        float* feat = reinterpret_cast<float*>(sm.cell) + lane * kMacFeatures;
+        if (cand) {
+          const double4 c = ldg_d4(&a.node_c[node]);
           const float4* mp = a.mom + 3 * (int64_t)node;
+          const float4* tp = a.mom3 + 3 * (int64_t)node;
           mac_features(c.x, c.y, c.z, __ldg(&a.geom[node]), __ldg(mp), __ldg(mp + 1),
-                       __ldg(mp + 2), Gx, Gy, Gz, hlen, cand_d, (float)n_act,
-                       a.lam_ei, feat);
+                       __ldg(mp + 2), __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), Gx,
+                       Gy, Gz, hlen, cand_d, (float)n_act, feat);
         } else {
 #pragma unroll
           for (int k = 0; k < kMacFeatures; ++k) feat[k] = 0.f;
         }
-        const float y = mlp_forward_warp(feat, reinterpret_cast<float*>(sm.cell),
-                                         h1_tile, *mlp, lane);
-        if (cand) {
-          bool in_range = true;
+        // range check on the raw features before the network normalises them
+        bool in_range = true;
 #pragma unroll
-          for (int k = 0; k < kMacFeatures; ++k)
-            in_range = in_range && feat[k] >= fmin_r[k] && feat[k] <= fmax_r[k];
-          bool accept;
-          if (in_range) {
-            // predicted |dF| = 10^y * n / d^2 against the group's budget
-            const float n = __ldg(&a.geom[node]).z;
-            accept = y <= log10f(budget * cand_d * cand_d / n);
+        for (int k = 0; k < kMacFeatures; ++k)
+          in_range = in_range && feat[k] >= frange[k] && feat[k] <= frange[kMacFeatures + k];
+        __syncwarp();
+        const float y = mlp_forward_warp(reinterpret_cast<float*>(sm.cell), h1_tile, *mlp, lane);
+        if (cand) {
+          // predicted |dF| = 10^y * n / d^2 against the group's budget; out
+          // of the training range the fixed-theta decision (open) stands
+          action = (in_range && y <= cand_B) ? 1 : 3;  // candidates exceed a bucket
+          n_mlp += 1;
+          n_fallback += in_range ? 0 : 1;
+        }
+      } else {
+        // ---- a batch of nodes from the stack ----
+        const int nb = min(32, ssize);
+        node = lane < nb ? stack[ssize - 1 - lane] : -1;
+        ssize -= nb;
+        __syncwarp();
+        bool cand = false;  // queued for the learned MAC
+        float cand_d = 0.f, cand_B = 0.f;
+        if (node >= 0) {
+          const double4 c = ldg_d4(&a.node_c[node]);
+          if (c.w < 0.0) {
+            action = 2;
+            pfirst = __ldg(&a.first[node]);
+            pcnt = 1;
           } else {
-            accept = c.w < (double)cand_d;  // fixed-theta fallback
-          }
-          if (accept) {
-            action = 1;
-          } else {
+            // group MAC: rcrit below the distance from the centroid to the box
+            const double ex = fmax(fabs(c.x - Gx) - hx, 0.0);
+            const double ey = fmax(fabs(c.y - Gy) - hy, 0.0);
+            const double ez = fmax(fabs(c.z - Gz) - hz, 0.0);
+            const double d2 = ex * ex + ey * ey + ez * ez;
+            bool accept = c.w * c.w < d2;  // the fixed-theta test
+            if (LEARNED && !accept && budget > 0.f) {
+              // learned criterion, on top of the fixed test: a cell the fixed
+              // test opens is accepted anyway when its predicted acceptance
+              // error is within the group's budget.  rho = s / (d - dx) places
+              // it against the training band; est = log10(|T|/(n d^3)) is the
+              // analytic size of the octupole field; B is the budget in the
+              // same units.  Cells whose estimate is clearly on one side of B
+              // (training quantiles m_lo, m_hi of label - est) are decided at
+              // once; the rest are queued for the network.  Only cells that
+              // would otherwise open into more than a bucket of particle
+              // pairs are worth a far-field evaluation.
+              const float4 g4 = __ldg(&a.geom[node]);
+              const double dd = sqrt(d2);
+              const double margin = dd - (double)g4.y;
+              const float rho = margin > 0.0 ? (float)((double)g4.x / margin) : 3.0e38f;
+              if (rho <= a.rho_hi && g4.z > (float)a.bucket) {
+                const float ddf = (float)dd;
+                const float tn = __ldg(&a.mom3[3 * (int64_t)node + 2]).z;
+                const float est = mac_estimate(tn, g4.z, ddf);
+                const float B = log10f(budget * ddf * ddf / g4.z);
+                if (est + m_hi <= B) {
+                  accept = true;
+                } else if (est + m_lo <= B) {
+                  cand = true;
+                  cand_d = ddf;
+                  cand_B = B;
+                }
+              }
+            }
+            // a small accepted cell is cheaper and exact as particle pairs: an
+            // M2P costs about as much as p2p_max pair interactions
             const int cnt = __ldg(&a.count[node]);
-            if (cnt <= a.bucket) {
+            if (accept && cnt <= a.p2p_max) {
               action = 2;
               pfirst = __ldg(&a.first[node]);
               pcnt = cnt;
-            } else {
-              action = 3;
+            } else if (accept) {
+              action = 1;
+            } else if (!cand) {
+              if (cnt <= a.bucket) {
+                action = 2;
+                pfirst = __ldg(&a.first[node]);
+                pcnt = cnt;
+              } else {
+                action = 3;
+              }
             }
           }
-          n_mlp += 1;
-          n_fallback += in_range ? 0 : 1;
+        }
+        if (LEARNED) {
+          const unsigned cm = __ballot_sync(0xffffffffu, cand);
+          if (cand) {
+            const int q = (cqt + __popc(cm & lt)) & (kCandRing - 1);
+            sm.cq_node[q] = node;
+            sm.cq_d[q] = cand_d;
+            sm.cq_b[q] = cand_B;
+          }
+          cqt += __popc(cm);
         }
       }
       // far-field entries
@@ -501,7 +583,7 @@ __global__ void __launch_bounds__(kMxThreads, 2)
         n_p2p += 32;
       }
       while (m2t - m2h >= 32) {
-        eval_m2p(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+        eval_m2p<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
         m2h += 32;
         n_m2p += 32;
       }
@@ -516,7 +598,7 @@ __global__ void __launch_bounds__(kMxThreads, 2)
       n_p2p += p2t - p2h;
     }
     if (m2t > m2h) {
-      eval_m2p(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+      eval_m2p<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
       n_m2p += m2t - m2h;
     }
     if (act) {
@@ -566,7 +648,8 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.first, (size_t)cap);
   rc |= realloc_dev(&mb.count, (size_t)cap);
   rc |= realloc_dev(&mb.digit, (size_t)cap);
-  rc |= realloc_dev(&mb.m64, 6 * (size_t)cap);
+  rc |= realloc_dev(&mb.m64, (size_t)kM64 * cap);
+  rc |= realloc_dev(&mb.mom3, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.geom, (size_t)cap);
   return rc;
@@ -588,7 +671,7 @@ int mixed_alloc_particles(MixedBuffers& mb, int n) {
 
 void mixed_free(MixedBuffers& mb) {
   void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
-                  mb.geom, mb.xs, mb.groups, mb.stack, mb.control};
+                  mb.mom3, mb.geom, mb.xs, mb.groups, mb.stack, mb.control};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   mb = MixedBuffers();
@@ -602,6 +685,7 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
   m.digit = mb.digit;
   m.m64 = mb.m64;
   m.mom = mb.mom;
+  m.mom3 = mb.mom3;
   m.geom = mb.geom;
   m.xs = mb.xs;
   m.groups = mb.groups;
@@ -633,6 +717,9 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.control = mb.control;
   a.stack = mb.stack;
   a.bucket = tune.bucket < 1 ? 1 : (tune.bucket > kMaxBucket ? kMaxBucket : tune.bucket);
+  // an octupole M2P costs ~110 flop, a quadrupole one ~60, a pair ~24
+  a.p2p_max = tune.order >= 3 ? 4 : 2;
+  if (a.p2p_max > a.bucket) a.p2p_max = a.bucket;
   a.physics = wp.physics;
   a.inv_lam2_ee = (float)(1.0 / (wp.lam_ee * wp.lam_ee));
   a.inv_lam2_ei = (float)(1.0 / (wp.lam_ei * wp.lam_ei));
@@ -657,6 +744,8 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.fmin = L ? learned->fmin : nullptr;
   a.fmax = L ? learned->fmax : nullptr;
   a.geom = mb.geom;
+  a.mom3 = mb.mom3;
+  a.margins = L ? learned->margins : nullptr;
   a.f_prev = L ? learned->f_prev : nullptr;
   a.eta_over_eps = L ? (float)(learned->eta / kEps) : 0.f;
   a.rho_lo = L ? learned->rho_lo : 0.f;
@@ -666,21 +755,27 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   int grid = (mb.grid_warps / (kMaxBlocksPerSm * kMxWarps)) * bps;
   const bool r = rdf != nullptr;
   const size_t s0 = walk_smem_bytes<false>(), s1 = walk_smem_bytes<true>();
-#define TG_LAUNCH(P, R, LL)                                                   \
+#define TG_LAUNCH(P, R, LL, O)                                                \
   do {                                                                        \
-    auto kfn = k_walk_mixed<P, R, LL>;                                        \
+    auto kfn = k_walk_mixed<P, R, LL, O>;                                     \
     const size_t sb = LL ? s1 : s0;                                           \
     cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                          (int)sb);                                            \
     kfn<<<grid, kMxThreads, sb, st>>>(a);                                     \
   } while (0)
+#define TG_LAUNCH_O(P, R, LL)                                                 \
+  do {                                                                        \
+    if (tune.order >= 3) TG_LAUNCH(P, R, LL, 3);                              \
+    else TG_LAUNCH(P, R, LL, 2);                                              \
+  } while (0)
   if (wp.physics == 1) {
-    if (L) { if (r) TG_LAUNCH(1, true, true); else TG_LAUNCH(1, false, true); }
-    else { if (r) TG_LAUNCH(1, true, false); else TG_LAUNCH(1, false, false); }
+    if (L) { if (r) TG_LAUNCH_O(1, true, true); else TG_LAUNCH_O(1, false, true); }
+    else { if (r) TG_LAUNCH_O(1, true, false); else TG_LAUNCH_O(1, false, false); }
   } else {
-    if (L) { if (r) TG_LAUNCH(0, true, true); else TG_LAUNCH(0, false, true); }
-    else { if (r) TG_LAUNCH(0, true, false); else TG_LAUNCH(0, false, false); }
+    if (L) { if (r) TG_LAUNCH_O(0, true, true); else TG_LAUNCH_O(0, false, true); }
+    else { if (r) TG_LAUNCH_O(0, true, false); else TG_LAUNCH_O(0, false, false); }
   }
+#undef TG_LAUNCH_O
 #undef TG_LAUNCH
   return 1;
 }

@@ -18,6 +18,7 @@ struct MixedBuffers {
   int8_t* digit = nullptr;
   double2* m64 = nullptr;
   float4* mom = nullptr;
+  float4* mom3 = nullptr;
   float4* geom = nullptr;
   double4* xs = nullptr;
   int2* groups = nullptr;
@@ -28,17 +29,20 @@ struct MixedBuffers {
 
 // Tunables of the walk (picked by tree_b200/tune.py; defaults below).
 struct MixedTuning {
-  int bucket = 4;          // twigs with <= bucket particles are summed directly
+  int bucket = 8;          // twigs with <= bucket particles are summed directly
   int blocks_per_sm = 4;   // persistent grid: SMs x blocks_per_sm blocks
+  int order = 3;           // far-field order: 2 quadrupole, 3 octupole
 };
 
-// Learned acceptance: inside the band rho_lo <= s/(d - dx) <= rho_hi a cell
-// is accepted when the predicted error 10^y * n/d^2 (units of e, Coulomb
-// constant dropped) is at most eta * min over the group of |F_prev| / eps.
+// Learned acceptance: a cell the fixed-theta test opens, with s/(d - dx) <=
+// rho_hi, is accepted when the predicted error 10^y * n/d^2 (units of e,
+// Coulomb constant dropped) is at most eta * min over the group of
+// |F_prev| / eps.
 struct LearnedMac {
   const MlpPacked* packed = nullptr;  // device
   const float* fmin = nullptr;        // device, 16: training range
   const float* fmax = nullptr;        // device, 16
+  const float* margins = nullptr;     // device, 2: quantiles of label - estimate
   const double* f_prev = nullptr;     // device forces of the previous step
   float eta = 1e-5f;
   float rho_lo = 0.2f, rho_hi = 0.9f;

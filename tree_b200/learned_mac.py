@@ -9,8 +9,8 @@ walks the combined tree with opening angles drawn from [0.2, 0.9], recording
 for every tested cell in the acceptance band its features and the exact FP64
 error of accepting it.  The network (16 -> 64 -> 64 -> 1) is then trained by
 the library's own BF16 tensor-core kernels (`tree_gpu_mac_train`) with a
-0.9-quantile pinball loss, so its predictions lean to over-estimating the
-error.  The model file holds the FP32 parameters, the feature statistics and
+0.99-quantile pinball loss: the walk uses the prediction to accept cells the
+fixed-theta test would open, so an under-estimate is the costly mistake.  The model file holds the FP32 parameters, the feature statistics and
 a short training report.
 """
 import argparse
@@ -28,12 +28,13 @@ DEFAULT_MODEL = os.path.join(HERE, "data", "mac_model.npz")
 
 def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
                       steps_list=(2, 6, 20), theta=(0.2, 0.9), rho=(0.2, 0.9),
-                      max_count=16384, cap=12_000_000, epochs=10, batch=8192,
-                      lr=2e-3, tau=0.9, seed=11, verbose=True):
+                      max_count=16384, keep=0.1, cap=12_000_000, epochs=10,
+                      batch=8192, lr=2e-3, tau=0.99, seed=11, verbose=True):
     dt = units.dt_code(1e-11)
     half = n // 2
     report = {"n": n, "te_list": list(te_list), "steps_list": list(steps_list),
               "theta": list(theta), "rho": list(rho), "max_count": max_count,
+              "keep": keep,
               "tau": tau, "epochs": epochs, "batch": batch, "lr": lr, "collects": []}
     t0 = time.time()
     cfg = api.Config(theta=0.5, te=te_list[0], physics=api.PHYS_KELBG,
@@ -51,7 +52,7 @@ def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
                 done = s
                 k += 1
                 tot = tf.mac_collect(theta[0], theta[1], rho[0], rho[1], max_count,
-                                     seed * 1000 + k, cap)
+                                     keep, seed * 1000 + k, cap)
                 report["collects"].append({"te": te, "step": s, "total": tot})
                 if verbose:
                     print(f"collect te={te:g} step={s}: {tot} samples", flush=True)
@@ -60,7 +61,10 @@ def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
         t2 = time.time()
         params, stats = tf.mac_get_model()
         feats, labels, extra = tf.mac_samples()
+    est = feats[:, 15]
     report.update({"samples": int(len(labels)), "collect_s": t1 - t0,
+                   "margins": [float(stats[64]), float(stats[65])],
+                   "corr_label_estimate": float(np.corrcoef(labels, est)[0, 1]),
                    "train_s": t2 - t1, "loss_per_epoch": [float(x) for x in losses],
                    "label_quantiles": {str(q): float(np.quantile(labels, q))
                                        for q in (0.01, 0.1, 0.5, 0.9, 0.99)}})
@@ -92,7 +96,7 @@ def main():
     params, stats, report, (f, y, e) = collect_and_train(n=args.n, epochs=args.epochs)
     save_model(args.out, params, stats, report)
     if args.dump_samples:
-        idx = np.random.default_rng(0).choice(len(y), min(len(y), 2_000_000), replace=False)
+        idx = np.random.default_rng(0).choice(len(y), min(len(y), 150_000), replace=False)
         np.savez_compressed(args.dump_samples, feats=f[idx], labels=y[idx], extra=e[idx])
     print("saved", args.out)
 
