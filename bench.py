@@ -36,15 +36,15 @@ UNIT = "particle-steps/s"
 # (FMA = 2; divisions, square roots and exponentials count as one flop each).
 FLOPS_M2P_REF = 194    # tree.f90:736-779 evaluated literally (FP64 path)
 FLOPS_P2P_REF = 30     # leaf laws of tree.f90 / erf-Kelbg with the x^2>40 shortcut
-FLOPS_M2P_MIXED = {2: 60, 3: 110}  # FP32 far field to quadrupole / octupole order
+FLOPS_M2P_MIXED = {2: 50, 3: 100}  # FP32 trace-free far field to quadrupole / octupole
 FLOPS_P2P_MIXED = 24   # FP32 erf-Kelbg pair with hi/lo offsets
 FLOPS_MLP = 2 * (16 * 64 + 64 * 64 + 64)  # one learned-MAC evaluation (BF16 mma + FP32)
 
-# Headline configuration: mixed precision, learned MAC on top of theta = 0.32,
+# Headline configuration: mixed precision, learned MAC on top of theta = 0.30,
 # octupole far field; chosen so the rms relative force error against the FP64
 # direct sum stays below 1e-4 at this workload (measured by the accuracy audit
 # below, which every run reports).
-HEADLINE = dict(theta=0.32, eta=1e-5, order=3, bucket=8)
+HEADLINE = dict(theta=0.30, eta=3e-5, order=3, bucket=8)
 
 
 def parse():

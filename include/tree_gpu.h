@@ -212,8 +212,9 @@ int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
  * and a model is loaded. */
 #define TREE_GPU_MLP_PARAMS 5313 /* W1[16][64] b1[64] W2[64][64] b2[64] w3[64] b3 */
 #define TREE_GPU_MLP_STATS 72    /* feature mean[16], 1/std[16], min[16], max[16],
-                                    margins m_lo, m_hi (quantiles of label minus
-                                    the analytic estimate), 6 reserved */
+                                    margins m_lo, m_hi (20% and 99.5% quantiles
+                                    of label minus the pre-filter estimate),
+                                    pre-filter coefficients c0..c4, 1 reserved */
 
 /* Walks the combined tree of the current device positions with a fixed
  * theta drawn per target group from [theta_lo, theta_hi] and appends one

@@ -16,7 +16,7 @@ from tree_b200 import api, cloud, learned_mac, units
 pytestmark = pytest.mark.gpu
 
 DT = units.dt_code(1e-11)
-FLOPS_M2P, FLOPS_P2P = 110, 24  # octupole M2P, FP32 erf-Kelbg pair
+FLOPS_M2P, FLOPS_P2P = 100, 24  # trace-free octupole M2P, FP32 erf-Kelbg pair
 
 
 def _evolved_state(n, seed, steps=3):

@@ -704,9 +704,14 @@ __constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
 // error of accepting the cell.
 // m64 per node (11 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
 // (Szz, Sxy) | (Syz, Szx) | T in the order xxx yyy zzz xxy xxz xyy yyz xzz
-// yzz xyz.  mom per node (3 x float4): (Q, Dx, Dy, Dz), (Sxx, Syy, Szz, Sxy),
-// (Syz, Szx, trace S, q_ion); mom3 per node (3 x float4): (Txxx, Tyyy, Tzzz,
-// Txxy), (Txxz, Txyy, Tyyz, Txzz), (Tyzz, Txyz, |T|_F, 0).
+// yzz xyz (all raw, for the FP64 labels of the learned criterion).  The FP32
+// copies the walk evaluates are trace-free, which drops every trace term from
+// the far-field formula (phi = Q/r + D.d/r^3 + 3 d.S'.d/r^5 + 5/2 T'(d,d,d)/r^7):
+// S' = S - tr(S)/3 I and T'_ijk = T_ijk - (d_ij V_k + d_ik V_j + d_jk V_i)/5
+// with V_k = T_iik.  mom per node (3 x float4): (Q, Dx, Dy, Dz),
+// (S'xx, S'yy, S'zz, Sxy), (Syz, Szx, trace S, q_ion); mom3 per node
+// (3 x float4): (T'xxx, T'yyy, T'zzz, T'xxy), (T'xxz, T'xyy, T'yyz, T'xzz),
+// (T'yzz, Txyz, |T'|_F, 0); geom (s, dx, n, |S'|_F).
 __global__ void k_upward_net(const double* __restrict__ x,
                              const uint32_t* __restrict__ vals,
                              const int8_t* __restrict__ L,
@@ -845,20 +850,37 @@ __global__ void k_upward_net(const double* __restrict__ x,
     m[3] = make_double2(Sxx, Syy);
     m[4] = make_double2(Szz, Sxy);
     m[5] = make_double2(Syz, Szx);
-    double tn = 0.0;
 #pragma unroll
     for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+    // trace-free parts (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz)
+    const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
+    double Tt[10];
+    Tt[0] = T[0] - 0.6 * Vx;
+    Tt[1] = T[1] - 0.6 * Vy;
+    Tt[2] = T[2] - 0.6 * Vz;
+    Tt[3] = T[3] - 0.2 * Vy;
+    Tt[4] = T[4] - 0.2 * Vz;
+    Tt[5] = T[5] - 0.2 * Vx;
+    Tt[6] = T[6] - 0.2 * Vz;
+    Tt[7] = T[7] - 0.2 * Vx;
+    Tt[8] = T[8] - 0.2 * Vy;
+    Tt[9] = T[9];
+    double tn = 0.0;
 #pragma unroll
-    for (int u = 0; u < 10; ++u) tn += kTMult[u] * T[u] * T[u];
+    for (int u = 0; u < 10; ++u) tn += kTMult[u] * Tt[u] * Tt[u];
+    const double trS = Sxx + Syy + Szz;
+    const double Sxxt = Sxx - trS / 3.0, Syyt = Syy - trS / 3.0, Szzt = Szz - trS / 3.0;
+    const double sn = sqrt(Sxxt * Sxxt + Syyt * Syyt + Szzt * Szzt +
+                           2.0 * (Sxy * Sxy + Syz * Syz + Szx * Szx));
     float4* f3 = mx.mom3 + 3 * (int64_t)cur;
-    f3[0] = make_float4((float)T[0], (float)T[1], (float)T[2], (float)T[3]);
-    f3[1] = make_float4((float)T[4], (float)T[5], (float)T[6], (float)T[7]);
-    f3[2] = make_float4((float)T[8], (float)T[9], (float)sqrt(tn), 0.f);
+    f3[0] = make_float4((float)Tt[0], (float)Tt[1], (float)Tt[2], (float)Tt[3]);
+    f3[1] = make_float4((float)Tt[4], (float)Tt[5], (float)Tt[6], (float)Tt[7]);
+    f3[2] = make_float4((float)Tt[8], (float)Tt[9], (float)sqrt(tn), 0.f);
     float4* f = mx.mom + 3 * (int64_t)cur;
     f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
-    f[1] = make_float4((float)Sxx, (float)Syy, (float)Szz, (float)Sxy);
-    f[2] = make_float4((float)Syz, (float)Szx, (float)(Sxx + Syy + Szz), (float)qi);
-    mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, 0.f);
+    f[1] = make_float4((float)Sxxt, (float)Syyt, (float)Szzt, (float)Sxy);
+    f[2] = make_float4((float)Syz, (float)Szx, (float)trS, (float)qi);
+    mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, (float)sn);
     __threadfence();
     cur = node_parent[cur];
   }

@@ -12,12 +12,18 @@
 //   6 |S|_F/(n s^2)  7 log10(|T|_F/(n s^3))/4   8 q_ion/n (species mix)
 //   9 D.u/(n s)      10 u.S.u/(n s^2)    11 T(u,u,u)/(n s^3)
 //   12 group fill    13 |G-X|/d - 1      14 log10(s/d)
-//   15 log10(|T|_F / (n d^3)): the size of the omitted octupole field
-//      relative to the gross monopole field n/d^2 -- the analytic estimate of
-//      the label, which the network refines.
+//   15 log10(|T|_F / (n d^3)): the octupole field relative to the gross
+//      monopole field n/d^2.
+// S and T are the trace-free net moments (|S|_F is stored in geom.w).
 // The label is log10(max over the group of |F_multipole - F_exact| /
 // (n / d^2)), i.e. the acceptance error relative to the cell's gross
 // monopole field (charges in units of e, Coulomb constant dropped).
+//
+// Pre-filter: before a cell is queued for the network the walk compares a
+// log-linear estimate of its label, est = c0 f14 + c1 f3 + c2 f7 + c3 f6 + c4,
+// with the budget.  The coefficients are a least-squares fit to the training
+// labels and the margins (m_lo, m_hi) are low and high quantiles of
+// label - est; both are stored with the model (mlp.cu: mlp_train).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -31,8 +37,29 @@ struct CellGeom {   // mx.geom: (s, dx, n, -)
   float s, dx, n, pad;
 };
 
+constexpr int kEstCoef = 5;  // pre-filter coefficients (stats[66..70])
+
 __device__ __forceinline__ float mac_estimate(float tnorm, float n, float d) {
   return log10f(tnorm / (n * d * d * d) + 1e-30f);
+}
+
+// Features 3, 6, 7 and 14, computed identically for the network and the
+// pre-filter.  s, n, |S|_F from geom; tnorm = |T|_F.
+__device__ __forceinline__ float mac_f3(float n) { return log2f(n) * (1.f / 16.f); }
+__device__ __forceinline__ float mac_f6(float snorm, float n, float s) {
+  return snorm / (n * s * s);
+}
+__device__ __forceinline__ float mac_f7(float tnorm, float n, float s) {
+  return log10f(tnorm / (n * s * s * s) + 1e-12f) * 0.25f;
+}
+__device__ __forceinline__ float mac_f14(float s, float d) { return log10f(s / d); }
+
+__device__ __forceinline__ float mac_prefilter(const float4 g4, float tnorm, float d,
+                                               const float* c) {
+  const float s = g4.x, n = g4.z;
+  return fmaf(c[0], mac_f14(s, d),
+              fmaf(c[1], mac_f3(n),
+                   fmaf(c[2], mac_f7(tnorm, n, s), fmaf(c[3], mac_f6(g4.w, n, s), c[4]))));
 }
 
 __device__ __forceinline__ void mac_features(
@@ -51,8 +78,6 @@ __device__ __forceinline__ void mac_features(
   const float id = 1.f / d;
   const float ns = n * s, ns2 = ns * s, ns3 = ns2 * s;
   const float Dn = sqrtf(Dx * Dx + Dy * Dy + Dz * Dz);
-  const float SF = sqrtf(Sxx * Sxx + Syy * Syy + Szz * Szz +
-                         2.f * (Sxy * Sxy + Syz * Syz + Szx * Szx));
   const float Du = Dx * ux + Dy * uy + Dz * uz;
   const float Sux = Sxx * ux + Sxy * uy + Szx * uz;
   const float Suy = Sxy * ux + Syy * uy + Syz * uz;
@@ -67,18 +92,18 @@ __device__ __forceinline__ void mac_features(
   f[0] = s * id;
   f[1] = dxo * id;
   f[2] = hlen * id;
-  f[3] = log2f(n) * (1.f / 16.f);
+  f[3] = mac_f3(n);
   f[4] = Q / n;
   f[5] = Dn / ns;
-  f[6] = SF / ns2;
-  f[7] = log10f(TF / ns3 + 1e-12f) * 0.25f;
+  f[6] = mac_f6(g4.w, n, s);
+  f[7] = mac_f7(TF, n, s);
   f[8] = qi / n;
   f[9] = Du / ns;
   f[10] = uSu / ns2;
   f[11] = Tuuu / ns3;
   f[12] = n_act * (1.f / 32.f);
   f[13] = ul * id - 1.f;
-  f[14] = log10f(s * id);
+  f[14] = mac_f14(s, d);
   f[15] = mac_estimate(TF, n, d);
 }
 

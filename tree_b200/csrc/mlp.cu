@@ -254,7 +254,6 @@ __global__ void k_mlp_infer(const float* __restrict__ X, int n,
                             const MlpPacked* __restrict__ packed, float* y) {
   __shared__ MlpPacked P;
   __shared__ float xs[kMlpWarps][32 * kMlpIn];
-  __shared__ __nv_bfloat16 h1[kMlpWarps][32 * kMlpH];
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(packed);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&P);
@@ -267,7 +266,7 @@ __global__ void k_mlp_infer(const float* __restrict__ X, int n,
     const int s = tile * 32 + lane;
 #pragma unroll
     for (int k = 0; k < kMlpIn; ++k) xs[w][lane * kMlpIn + k] = s < n ? X[(int64_t)s * kMlpIn + k] : 0.f;
-    const float yy = mlp_forward_warp(xs[w], h1[w], P, lane);
+    const float yy = mlp_forward_warp(xs[w], P, lane);
     if (s < n) y[s] = yy;
   }
 }
@@ -361,30 +360,77 @@ __global__ void k_feat_stats(const float* __restrict__ X, int n, float* stats) {
   }
 }
 
-// Keys ordering label - estimate (feature 15) for the margin quantiles.
+// Labels at the floor (an acceptance error below 1e-12 of the monopole
+// field: exact cancellation) carry no information for the pre-filter fit.
+constexpr float kLabelFloor = -11.99f;
+
+// Normal equations of the pre-filter fit  label ~ c . (f14, f3, f7, f6, 1)
+// over the samples above the floor: acc[0..14] the upper triangle of X^T X,
+// acc[15..19] X^T y, acc[20] the count.
+__global__ void k_est_normal_eq(const float* __restrict__ X, const float* __restrict__ Y,
+                                int n, double* acc) {
+  double a[21];
+#pragma unroll
+  for (int k = 0; k < 21; ++k) a[k] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float y = Y[i];
+    if (!(y > kLabelFloor)) continue;
+    const float* x = X + (int64_t)i * kMlpIn;
+    const double q[5] = {x[14], x[3], x[7], x[6], 1.0};
+    int idx = 0;
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int c = r; c < 5; ++c) a[idx++] += q[r] * q[c];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) a[15 + r] += q[r] * (double)y;
+    a[20] += 1.0;
+  }
+#pragma unroll
+  for (int k = 0; k < 21; ++k) {
+    double v = a[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&acc[k], v);
+  }
+}
+
+// Keys ordering label - pre-filter estimate for the margin quantiles; floor
+// labels sort last and are not counted.
 __global__ void k_margin_keys(const float* __restrict__ X, const float* __restrict__ Y,
-                              int n, uint64_t* keys, uint32_t* vals) {
+                              int n, const float* __restrict__ coef, uint64_t* keys,
+                              uint32_t* vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float d = Y[i] - X[(int64_t)i * kMlpIn + (kMlpIn - 1)];
-  uint32_t u = __float_as_uint(d);
-  u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  const float* x = X + (int64_t)i * kMlpIn;
+  const float est = fmaf(coef[0], x[14], fmaf(coef[1], x[3], fmaf(coef[2], x[7],
+                         fmaf(coef[3], x[6], coef[4]))));
+  uint32_t u = 0xffffffffu;
+  if (Y[i] > kLabelFloor) {
+    u = __float_as_uint(Y[i] - est);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  }
   keys[i] = u;
   vals[i] = (uint32_t)i;
 }
 
-__global__ void k_margin_store(const uint64_t* __restrict__ keys, int n,
+// m_lo: 20% quantile -- a cell whose estimate is m_lo or more above the
+// budget is opened without the network; the network's own 99% quantile
+// prediction would accept fewer than 1% of those, and a missed acceptance
+// only costs time.  m_hi: 99.5% quantile -- a cell whose estimate is m_hi or
+// more below the budget is accepted without the network.
+__global__ void k_margin_store(const uint64_t* __restrict__ keys, int n_valid,
                                float* stats) {
   if (threadIdx.x != 0) return;
   auto val = [&](double q) {
-    int64_t i = (int64_t)(q * (n - 1));
+    if (n_valid <= 0) return 0.f;
+    int64_t i = (int64_t)(q * (n_valid - 1));
     uint32_t u = (uint32_t)keys[i];
     u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
     return __uint_as_float(u);
   };
-  stats[4 * kMlpIn] = val(0.01);       // m_lo
-  stats[4 * kMlpIn + 1] = val(0.99);   // m_hi
-  for (int k = 2; k < 8; ++k) stats[4 * kMlpIn + k] = 0.f;
+  stats[4 * kMlpIn] = n_valid > 0 ? val(0.20) : 3.0e38f;      // m_lo
+  stats[4 * kMlpIn + 1] = n_valid > 0 ? val(0.995) : 3.0e38f; // m_hi
+  stats[4 * kMlpIn + 7] = 0.f;
 }
 
 __global__ void k_shuffle_keys(uint64_t* keys, uint32_t* vals, int n, uint64_t seed) {
@@ -415,10 +461,43 @@ __global__ void k_normalize_gather(const float* __restrict__ X,
 
 #include <cmath>
 #include <random>
+#include <utility>
 #include <vector>
 #include "build.h"
+#include "mac.cuh"
 
 namespace tg {
+
+// Least-squares pre-filter coefficients from the accumulated normal
+// equations (Gaussian elimination with partial pivoting and a small ridge).
+static void solve_prefilter(const double* acc, float* coef) {
+  double A[5][6];
+  int idx = 0;
+  for (int r = 0; r < 5; ++r)
+    for (int c = r; c < 5; ++c) A[r][c] = A[c][r] = acc[idx++];
+  double tr = 0.0;
+  for (int r = 0; r < 5; ++r) tr += A[r][r];
+  for (int r = 0; r < 5; ++r) {
+    A[r][r] += 1e-9 * tr;
+    A[r][5] = acc[15 + r];
+  }
+  for (int c = 0; c < 5; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < 5; ++r)
+      if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+    for (int k = 0; k < 6; ++k) std::swap(A[c][k], A[piv][k]);
+    if (A[c][c] == 0.0) {
+      for (int k = 0; k < 5; ++k) coef[k] = 0.f;
+      return;
+    }
+    for (int r = 0; r < 5; ++r) {
+      if (r == c) continue;
+      const double f = A[r][c] / A[c][c];
+      for (int k = c; k < 6; ++k) A[r][k] -= f * A[c][k];
+    }
+  }
+  for (int r = 0; r < 5; ++r) coef[r] = (float)(A[r][5] / A[r][r]);
+}
 
 int mlp_train(const float* X, const float* Y, int n, int epochs, int batch,
               float lr, float tau, uint64_t seed, float* params, float* stats,
@@ -462,10 +541,20 @@ int mlp_train(const float* X, const float* Y, int n, int epochs, int batch,
     k_shuffle_keys<<<(n + 255) / 256, 256, 0, st>>>(k0, v0, n, seed);
     radix_sort(k0, v0, k1, v1, n, hist, part, st);
     k_normalize_gather<<<(n + 255) / 256, 256, 0, st>>>(X, Y, v0, n, stats, Xn, Yn);
-    // margins: 1% and 99% quantiles of (label - analytic estimate)
-    k_margin_keys<<<(n + 255) / 256, 256, 0, st>>>(X, Y, n, k0, v0);
+    // pre-filter: least-squares coefficients, then margins of label - est
+    double* acc = reinterpret_cast<double*>(grad);  // 21 doubles of scratch
+    cudaMemsetAsync(acc, 0, 21 * sizeof(double), st);
+    k_est_normal_eq<<<256, 256, 0, st>>>(X, Y, n, acc);
+    double hacc[21];
+    cudaMemcpyAsync(hacc, acc, sizeof(hacc), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    float coef[kEstCoef] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    if (hacc[20] >= 16.0) solve_prefilter(hacc, coef);
+    cudaMemcpyAsync(stats + 4 * kMlpIn + 2, coef, sizeof(coef), cudaMemcpyHostToDevice, st);
+    k_margin_keys<<<(n + 255) / 256, 256, 0, st>>>(X, Y, n, stats + 4 * kMlpIn + 2, k0, v0);
     radix_sort(k0, v0, k1, v1, n, hist, part, st);
-    k_margin_store<<<1, 32, 0, st>>>(k0, n, stats);
+    k_margin_store<<<1, 32, 0, st>>>(k0, (int)hacc[20], stats);
+    cudaMemsetAsync(grad, 0, sizeof(float) * kMlpParams, st);
     const int nb = (n + batch - 1) / batch;
     int t = 0;
     for (int ep = 0; ep < epochs; ++ep) {

@@ -85,11 +85,13 @@ __device__ __forceinline__ void load_b_f32(uint32_t b[2], const float* buf,
 
 // Inference for the 32 lanes' feature vectors.  xs_tile: 32x16 FP32
 // per-warp scratch whose row `lane` holds this lane's raw features on entry
-// (normalised in place); h1_tile: 32x64 BF16 per-warp scratch; P: packed
-// weights in shared memory.  Returns this lane's prediction.  All 32 lanes
-// must call it.
+// (normalised in place); P: packed weights in shared memory.  Returns this
+// lane's prediction.  All 32 lanes must call it.
+// The hidden layer never leaves registers: the accumulator fragment of two
+// adjacent 16x8 output tiles of layer 1 (rows g, g+8; columns 2t, 2t+1 of each
+// tile) is exactly the A fragment of one 16x16 k-tile of layer 2, so H1 is
+// rounded to BF16 and packed in place.
 __device__ __forceinline__ float mlp_forward_warp(float* xs_tile,
-                                                  __nv_bfloat16* h1_tile,
                                                   const MlpPacked& P,
                                                   int lane) {
   const float* b1 = P.vec;
@@ -102,13 +104,15 @@ __device__ __forceinline__ float mlp_forward_warp(float* xs_tile,
   for (int k = 0; k < kMlpIn; ++k)
     xs_tile[lane * kMlpIn + k] = (xs_tile[lane * kMlpIn + k] - mu[k]) * isd[k];
   __syncwarp();
-  const int g = lane >> 2, t = lane & 3;
-  // layer 1: H1 = relu(X W1 + b1), stored as BF16 rows
+  const int t = lane & 3;
+  float part[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [mt][row g / g+8]
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
     uint32_t a[4];
     load_a_f32<false>(a, xs_tile, kMlpIn, 1, 16 * mt, 0, lane);
-#pragma unroll 2
+    // layer 1: H1 = relu(X W1 + b1) for rows 16 mt .. 16 mt + 15
+    uint32_t h[4][4];
+#pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
       const uint2 bb = P.w1f[nt * 32 + lane];
       const uint32_t b[2] = {bb.x, bb.y};
@@ -116,37 +120,34 @@ __device__ __forceinline__ float mlp_forward_warp(float* xs_tile,
       float c[4];
       mma_bf16_16816(c, a, b, z);
       const int col = 8 * nt + 2 * t;
-      const int r0 = 16 * mt + g, r1 = r0 + 8;
-      reinterpret_cast<__nv_bfloat162*>(h1_tile)[(r0 * kMlpH + col) >> 1] =
-          __floats2bfloat162_rn(fmaxf(c[0] + b1[col], 0.f), fmaxf(c[1] + b1[col + 1], 0.f));
-      reinterpret_cast<__nv_bfloat162*>(h1_tile)[(r1 * kMlpH + col) >> 1] =
-          __floats2bfloat162_rn(fmaxf(c[2] + b1[col], 0.f), fmaxf(c[3] + b1[col + 1], 0.f));
+      const uint32_t lo = pack_bf16x2(fmaxf(c[0] + b1[col], 0.f), fmaxf(c[1] + b1[col + 1], 0.f));
+      const uint32_t hi = pack_bf16x2(fmaxf(c[2] + b1[col], 0.f), fmaxf(c[3] + b1[col + 1], 0.f));
+      h[nt >> 1][(nt & 1) * 2] = lo;
+      h[nt >> 1][(nt & 1) * 2 + 1] = hi;
     }
-  }
-  __syncwarp();
-  // layer 2 + 3: y = relu(H1 W2 + b2) . w3 + b3, one 16x8 tile at a time
-  float part[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [mt][row g / g+8]
-  const uint32_t* h = reinterpret_cast<const uint32_t*>(h1_tile);
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
+    // layers 2 + 3: y = relu(H1 W2 + b2) . w3 + b3, four 16x8 output tiles
+    // at a time so that four independent mma chains overlap
 #pragma unroll 1
-    for (int nt = 0; nt < 8; ++nt) {
-      float c[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int half = 0; half < 2; ++half) {
+      float c[4][4];
 #pragma unroll
-      for (int kt = 0; kt < 4; ++kt) {
-        const int r0 = 16 * mt + g, r1 = r0 + 8;
-        const int c0 = 16 * kt + 2 * t, c1 = c0 + 8;
-        const uint32_t a[4] = {h[(r0 * kMlpH + c0) >> 1], h[(r1 * kMlpH + c0) >> 1],
-                               h[(r0 * kMlpH + c1) >> 1], h[(r1 * kMlpH + c1) >> 1]};
-        const uint2 bb = P.w2f[(kt * 8 + nt) * 32 + lane];
-        const uint32_t b[2] = {bb.x, bb.y};
-        mma_bf16_16816(c, a, b, c);
+      for (int j = 0; j < 4; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.f;
+#pragma unroll
+      for (int kt = 0; kt < 4; ++kt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint2 bb = P.w2f[(kt * 8 + 4 * half + j) * 32 + lane];
+          const uint32_t b[2] = {bb.x, bb.y};
+          mma_bf16_16816(c[j], h[kt], b, c[j]);
+        }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int col = 8 * (4 * half + j) + 2 * t;
+        part[mt][0] += fmaxf(c[j][0] + b2[col], 0.f) * w3[col] +
+                       fmaxf(c[j][1] + b2[col + 1], 0.f) * w3[col + 1];
+        part[mt][1] += fmaxf(c[j][2] + b2[col], 0.f) * w3[col] +
+                       fmaxf(c[j][3] + b2[col + 1], 0.f) * w3[col + 1];
       }
-      const int col = 8 * nt + 2 * t;
-      part[mt][0] += fmaxf(c[0] + b2[col], 0.f) * w3[col] +
-                     fmaxf(c[1] + b2[col + 1], 0.f) * w3[col + 1];
-      part[mt][1] += fmaxf(c[2] + b2[col], 0.f) * w3[col] +
-                     fmaxf(c[3] + b2[col + 1], 0.f) * w3[col + 1];
     }
   }
   // rows are shared by the 4 threads of a quad

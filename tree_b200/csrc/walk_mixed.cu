@@ -19,10 +19,11 @@
 // two-float (hi + lo) split of the FP64 offsets, so a pair separation keeps
 // ~1e-7 relative accuracy even for the closest e-i pairs.  Chunk sums of 32
 // terms are added into Kahan-compensated per-lane accumulators.
-// Far field: net monopole + dipole + exact quadrupole about the centroid
-// (Coulomb, the expansion of tree.f90:744-779 carried one order further for
-// cells whose net charge nearly cancels).  Near field: erf-Kelbg (or the
-// reference laws) for every particle pair.
+// Far field: net monopole, dipole and trace-free quadrupole (and octupole at
+// order 3) about the centroid -- the Coulomb expansion of tree.f90:744-779
+// carried to full subtree moments and one order further, for cells whose net
+// charge nearly cancels.  Near field: erf-Kelbg (or the reference laws) for
+// every particle pair.
 #include <cstdio>
 #include "mac.cuh"
 #include "walk_mixed.h"
@@ -36,8 +37,10 @@ constexpr int kM2pRing = 64;      // power of two, > 31 + 32
 constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
 constexpr int kMaxBucket = 8;
 constexpr int kMaxBlocksPerSm = 4;
+constexpr int kMinBlocksPerSm = 3;  // 80 registers: 24 resident warps per SM
 
 constexpr int kCandRing = 64;     // power of two, > 31 + 32
+constexpr int kCellF4 = 6;        // float4 per staged far-field cell
 
 struct WarpSmem {
   int m2p[kM2pRing];
@@ -45,11 +48,11 @@ struct WarpSmem {
   int cq_node[kCandRing];  // learned-MAC candidates waiting for a full batch
   float cq_d[kCandRing];
   float cq_b[kCandRing];
-  // staged cells, 8 float4 each: (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion),
-  // (Sxx, Syy, Szz, Sxy), (Syz, Szx, tr S, -), (Txxx, Tyyy, Tzzz, Txxy),
-  // (Txxz, Txyy, Tyyz, Txzz), (Tyzz, Txyz, -, -), (Vx, Vy, Vz, -)
-  float4 cell[32 * 8];
-  float4 part[32 * 2];   // (hi xyz, sorted index bits), (lo xyz, ion?)
+  // staged cells, kCellF4 float4 each: (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion),
+  // (Sxx, Syy, Szz, Sxy), (Syz, Szx, Txxx, Tyyy), (Tzzz, Txxy, Txxz, Txyy),
+  // (Tyyz, Txzz, Tyzz, Txyz) -- S and T trace-free
+  float4 cell[32 * kCellF4];
+  float4 part[32 * 2];   // (hi xyz, sorted index bits), (lo xyz, charge)
 };
 
 struct MixedArgs {
@@ -84,7 +87,7 @@ struct MixedArgs {
   const float* fmax;
   const float4* geom;
   const float4* mom3;
-  const float* margins;  // (m_lo, m_hi) of the model
+  const float* margins;  // m_lo, m_hi, pre-filter coefficients c0..c4
   const double* f_prev;
   float eta_over_eps;
   float rho_lo, rho_hi;
@@ -126,16 +129,14 @@ __device__ __forceinline__ double warp_max_d(double v) {
 }
 
 // ---------------------------------------------------------------- M2P ----
-// Net monopole Q, dipole D, second moment S = 1/2 sum q a a^T (traceful) and,
-// for ORDER 3, third moment T = sum q a a a about the cell centroid.  With
-// d = target - centroid, r = |d|:
-//   phi = Q/r + D.d/r^3 + (3 d.S.d - r^2 tr S)/r^5
-//         + (5 T(d,d,d) - 3 r^2 V.d)/(2 r^7),      V_k = T_iik
-//   -grad phi = g d - D/r^3 - 6 S d/r^5 - 7.5 T(.,d,d)/r^7 + 1.5 V/r^5,
-//   g = Q/r^3 + (3 D.d + 15 d.S.d/r^2 - 3 tr S)/r^5
-//       + (17.5 T(d,d,d)/r^2 - 7.5 V.d)/r^7.
-// 60 flop per entry at ORDER 2, 110 at ORDER 3 (FMA = 2).  The ion part of
-// phi for the Epot_e/Epot_i split is taken at monopole order (q_ion / r).
+// Net monopole Q, dipole D, trace-free second moment S (from 1/2 sum q a a^T)
+// and, for ORDER 3, trace-free third moment T (from sum q a a a) about the
+// cell centroid.  With d = target - centroid, r = |d|:
+//   phi = Q/r + D.d/r^3 + 3 d.S.d/r^5 + 5/2 T(d,d,d)/r^7
+//   -grad phi = g d - D/r^3 - 6 S d/r^5 - 7.5 T(.,d,d)/r^7,
+//   g = Q/r^3 + 3 D.d/r^5 + 15 d.S.d/r^7 + 17.5 T(d,d,d)/r^9.
+// About 50 flop per entry at ORDER 2, 100 at ORDER 3 (FMA = 2).  The ion part
+// of phi for the Epot_e/Epot_i split is taken at monopole order (q_ion / r).
 template <int ORDER>
 __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
                                          const MixedArgs& a, double Gx,
@@ -147,31 +148,31 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     double4 c = ldg_d4(&a.node_c[node]);
     const float4* mp = a.mom + 3 * (int64_t)node;
     float4 m0 = __ldg(mp), m1 = __ldg(mp + 1), m2 = __ldg(mp + 2);
-    float4* cl = sm.cell + 8 * lane;
+    float4* cl = sm.cell + kCellF4 * lane;
     cl[0] = make_float4((float)(c.x - Gx), (float)(c.y - Gy), (float)(c.z - Gz), m0.x);
     cl[1] = make_float4(m0.y, m0.z, m0.w, m2.w);
     cl[2] = m1;
-    cl[3] = make_float4(m2.x, m2.y, m2.z, 0.f);
     if (ORDER >= 3) {
       const float4* tp = a.mom3 + 3 * (int64_t)node;
       const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
-      cl[4] = t0;
-      cl[5] = t1;
-      cl[6] = t2;
-      // V_k = T_iik: order xxx yyy zzz xxy | xxz xyy yyz xzz | yzz xyz
-      cl[7] = make_float4(t0.x + t1.y + t1.w, t0.w + t0.y + t2.x, t1.x + t1.z + t0.z, 0.f);
+      cl[3] = make_float4(m2.x, m2.y, t0.x, t0.y);
+      cl[4] = make_float4(t0.z, t0.w, t1.x, t1.y);
+      cl[5] = make_float4(t1.z, t1.w, t2.x, t2.y);
+    } else {
+      cl[3] = make_float4(m2.x, m2.y, 0.f, 0.f);
     }
   }
   __syncwarp();
   float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
 #pragma unroll 2
   for (int k = 0; k < cnt; ++k) {
-    const float4* cl = sm.cell + 8 * k;
+    const float4* cl = sm.cell + kCellF4 * k;
     const float4 A = cl[0], B = cl[1], C = cl[2], E = cl[3];
     const float dx = tx - A.x, dy = ty - A.y, dz = tz - A.z;
+    const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
     // accepted cells are farther than rcrit >= 0; the floor only guards a
     // zero-size cell against an FP32 distance of 0
-    const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+    const float r2 = fmaxf(xx + yy + zz, 1e-30f);
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
     const float rinv3 = rinv * rinv2;
@@ -183,29 +184,29 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     const float u = fmaf(dx, Sx, fmaf(dy, Sy, dz * Sz));
     const float Dd = fmaf(B.x, dx, fmaf(B.y, dy, B.z * dz));
     const float ur2 = u * rinv2;
-    float g = fmaf(A.w, rinv3, rinv5 * fmaf(3.f, Dd, fmaf(15.f, ur2, -3.f * E.z)));
-    const float h6 = 6.f * rinv5;
-    float gx = fmaf(-h6, Sx, -rinv3 * B.x);
-    float gy = fmaf(-h6, Sy, -rinv3 * B.y);
-    float gz = fmaf(-h6, Sz, -rinv3 * B.z);
-    float ph = fmaf(A.w, rinv, rinv3 * (Dd + fmaf(3.f, ur2, -E.z)));
+    float g = fmaf(A.w, rinv3, rinv5 * fmaf(3.f, Dd, 15.f * ur2));
+    float ph = fmaf(A.w, rinv, rinv3 * fmaf(3.f, ur2, Dd));
+    const float c3 = -rinv3, c5 = -6.f * rinv5;
+    float gx = fmaf(c5, Sx, c3 * B.x);
+    float gy = fmaf(c5, Sy, c3 * B.y);
+    float gz = fmaf(c5, Sz, c3 * B.z);
     if (ORDER >= 3) {
-      const float4 T0 = cl[4], T1 = cl[5], T2 = cl[6], V = cl[7];
-      // T(., d, d): xxx yyy zzz xxy | xxz xyy yyz xzz | yzz xyz
-      const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
-      const float xy2 = 2.f * dx * dy, xz2 = 2.f * dx * dz, yz2 = 2.f * dy * dz;
-      const float Tx = fmaf(T0.x, xx, fmaf(T1.y, yy, fmaf(T1.w, zz, fmaf(T0.w, xy2, fmaf(T1.x, xz2, T2.y * yz2)))));
-      const float Ty = fmaf(T0.w, xx, fmaf(T0.y, yy, fmaf(T2.x, zz, fmaf(T1.y, xy2, fmaf(T2.y, xz2, T1.z * yz2)))));
-      const float Tz = fmaf(T1.x, xx, fmaf(T1.z, yy, fmaf(T0.z, zz, fmaf(T2.y, xy2, fmaf(T1.w, xz2, T2.x * yz2)))));
+      const float4 T1 = cl[4], T2 = cl[5];
+      // T order: xxx = E.z, yyy = E.w, zzz = T1.x, xxy = T1.y, xxz = T1.z,
+      // xyy = T1.w, yyz = T2.x, xzz = T2.y, yzz = T2.z, xyz = T2.w
+      const float x2 = dx + dx, y2 = dy + dy;
+      const float xy2 = x2 * dy, xz2 = x2 * dz, yz2 = y2 * dz;
+      const float Tx = fmaf(E.z, xx, fmaf(T1.w, yy, fmaf(T2.y, zz, fmaf(T1.y, xy2, fmaf(T1.z, xz2, T2.w * yz2)))));
+      const float Ty = fmaf(T1.y, xx, fmaf(E.w, yy, fmaf(T2.z, zz, fmaf(T1.w, xy2, fmaf(T2.w, xz2, T2.x * yz2)))));
+      const float Tz = fmaf(T1.z, xx, fmaf(T2.x, yy, fmaf(T1.x, zz, fmaf(T2.w, xy2, fmaf(T2.y, xz2, T2.z * yz2)))));
       const float T3 = fmaf(dx, Tx, fmaf(dy, Ty, dz * Tz));
-      const float Vd = fmaf(V.x, dx, fmaf(V.y, dy, V.z * dz));
       const float rinv7 = rinv5 * rinv2;
-      g = fmaf(rinv7, fmaf(17.5f * rinv2, T3, -7.5f * Vd), g);
-      const float h75 = -7.5f * rinv7, h15 = 1.5f * rinv5;
-      gx = fmaf(h75, Tx, fmaf(h15, V.x, gx));
-      gy = fmaf(h75, Ty, fmaf(h15, V.y, gy));
-      gz = fmaf(h75, Tz, fmaf(h15, V.z, gz));
-      ph = fmaf(rinv7, fmaf(2.5f, T3, -1.5f * r2 * Vd), ph);
+      g = fmaf(17.5f * rinv7, T3 * rinv2, g);
+      ph = fmaf(2.5f * rinv7, T3, ph);
+      const float c7 = -7.5f * rinv7;
+      gx = fmaf(c7, Tx, gx);
+      gy = fmaf(c7, Ty, gy);
+      gz = fmaf(c7, Tz, gz);
     }
     fx += fmaf(g, dx, gx);
     fy += fmaf(g, dy, gy);
@@ -238,11 +239,14 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
     sm.part[2 * lane] = make_float4(hx, hy, hz, __int_as_float(s));
     sm.part[2 * lane + 1] =
         make_float4((float)(rx - (double)hx), (float)(ry - (double)hy),
-                    (float)(rz - (double)hz), (float)xs.w);
+                    (float)(rz - (double)hz), xs.w > 0.5 ? 1.f : -1.f);
   }
   __syncwarp();
-  const float tspf = (float)tsp;
-  float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
+  const float tq = tsp ? 1.f : -1.f;  // target charge
+  // pair constants of the target's own species and of the other species
+  const float il2_same = PHYS == 1 ? (tsp ? a.inv_lam2_ii : a.inv_lam2_ee) : 0.f;
+  const float il_same = PHYS == 1 ? (tsp ? a.inv_lam_ii : a.inv_lam_ee) : 0.f;
+  float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pq = 0.f;
   for (int k = 0; k < cnt; ++k) {
     const float4 P = sm.part[2 * k], Q = sm.part[2 * k + 1];
     const int s = __float_as_int(P.w);
@@ -250,13 +254,13 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
     const float dy = (thy - P.y) + (tly - Q.y);
     const float dz = (thz - P.z) + (tlz - Q.z);
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const bool same = Q.w == tspf;
-    const float ssign = Q.w * 2.f - 1.f;  // source charge: -1 e, +1 ion
+    const float ssign = Q.w;  // source charge: -1 e, +1 ion
+    const bool same = ssign == tq;
     const bool self = s == p_self;
     bool rare;
     float wc;  // weight of the plain Coulomb term
     if (PHYS == 1) {
-      const float il2 = same ? (tsp ? a.inv_lam2_ii : a.inv_lam2_ee) : a.inv_lam2_ei;
+      const float il2 = same ? il2_same : a.inv_lam2_ei;
       rare = !self && r2 * il2 < 40.f;  // exp(-x^2) still visible in FP32
       wc = (self || rare) ? 0.f : ssign;
     } else {
@@ -277,7 +281,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
     if (rare) {
       float rfs = 0.f, ve;
       if (PHYS == 1) {
-        const float il = same ? (tsp ? a.inv_lam_ii : a.inv_lam_ee) : a.inv_lam_ei;
+        const float il = same ? il_same : a.inv_lam_ei;
         const float sqrtpi = 1.77245385f;
         if (r2 > 0.f) {
           const float r = sqrtf(r2);
@@ -307,7 +311,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
       ph += ssign * ve;
     }
     pa += ph;
-    pi = fmaf(Q.w, ph, pi);
+    pq = fmaf(ssign, ph, pq);
     if (RDF && act) {
       bool counted = PHYS == 1 ? !self : (same ? r2 > 0.01f : true);
       if (counted && (!same || tsp == 1)) {
@@ -328,27 +332,24 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
   kahan_add(acc.sy, acc.cy, fy);
   kahan_add(acc.sz, acc.cz, fz);
   acc.phi_all += (double)pa;
-  acc.phi_ion += (double)pi;
+  acc.phi_ion += 0.5 * ((double)pa + (double)pq);  // ion sources: (all + charge-weighted) / 2
 }
 
 // --------------------------------------------------------------- walk ----
 // Dynamic shared memory: WarpSmem[kMxWarps], then (learned MAC only) the
-// packed network and one 32x64 BF16 hidden tile per warp.
+// packed network and the features' training range.
 template <bool LEARNED>
 constexpr size_t walk_smem_bytes() {
   return sizeof(WarpSmem) * kMxWarps +
-         (LEARNED ? sizeof(MlpPacked) + sizeof(__nv_bfloat16) * 32 * kMlpH * kMxWarps +
-                        sizeof(float) * 2 * kMacFeatures
-                  : 0);
+         (LEARNED ? sizeof(MlpPacked) + sizeof(float) * (2 * kMacFeatures + 8) : 0);
 }
 
 template <int PHYS, bool RDF, bool LEARNED, int ORDER>
-__global__ void __launch_bounds__(kMxThreads, 2)
+__global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
     k_walk_mixed(MixedArgs a) {
   extern __shared__ float4 dyn_smem[];
   WarpSmem* smem = reinterpret_cast<WarpSmem*>(dyn_smem);
   MlpPacked* mlp = reinterpret_cast<MlpPacked*>(smem + kMxWarps);
-  __nv_bfloat16* h1_all = reinterpret_cast<__nv_bfloat16*>(mlp + 1);
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   WarpSmem& sm = smem[wib];
@@ -358,17 +359,17 @@ __global__ void __launch_bounds__(kMxThreads, 2)
     for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 4); i += blockDim.x) dst[i] = src[i];
     __syncthreads();
   }
-  __nv_bfloat16* h1_tile = h1_all + (size_t)wib * 32 * kMlpH;
-  // training range of the features (fmin | fmax), shared by the block
-  float* frange = reinterpret_cast<float*>(h1_all + (size_t)kMxWarps * 32 * kMlpH);
-  float m_lo = 0.f, m_hi = 0.f;
+  // training range of the features (fmin | fmax), then m_lo, m_hi and the
+  // pre-filter coefficients, shared by the block
+  float* frange = reinterpret_cast<float*>(mlp + 1);
+  const float* fmodel = frange + 2 * kMacFeatures;
   if (LEARNED) {
-    m_lo = __ldg(&a.margins[0]);
-    m_hi = __ldg(&a.margins[1]);
     if (threadIdx.x < kMacFeatures) {
       frange[threadIdx.x] = __ldg(&a.fmin[threadIdx.x]);
       frange[kMacFeatures + threadIdx.x] = __ldg(&a.fmax[threadIdx.x]);
     }
+    if (threadIdx.x < 2 + kEstCoef)
+      frange[2 * kMacFeatures + threadIdx.x] = __ldg(&a.margins[threadIdx.x]);
     __syncthreads();
   }
   const int gwarp = blockIdx.x * kMxWarps + wib;
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(kMxThreads, 2)
         for (int k = 0; k < kMacFeatures; ++k)
           in_range = in_range && feat[k] >= frange[k] && feat[k] <= frange[kMacFeatures + k];
         __syncwarp();
-        const float y = mlp_forward_warp(reinterpret_cast<float*>(sm.cell), h1_tile, *mlp, lane);
+        const float y = mlp_forward_warp(reinterpret_cast<float*>(sm.cell), *mlp, lane);
         if (cand) {
           // predicted |dF| = 10^y * n / d^2 against the group's budget; out
           // of the training range the fixed-theta decision (open) stands
@@ -483,25 +484,24 @@ __global__ void __launch_bounds__(kMxThreads, 2)
               // learned criterion, on top of the fixed test: a cell the fixed
               // test opens is accepted anyway when its predicted acceptance
               // error is within the group's budget.  rho = s / (d - dx) places
-              // it against the training band; est = log10(|T|/(n d^3)) is the
-              // analytic size of the octupole field; B is the budget in the
-              // same units.  Cells whose estimate is clearly on one side of B
+              // it against the training band; est is the fitted log-linear
+              // estimate of the label (mac.cuh) and B the budget in the same
+              // units.  Cells whose estimate is clearly on one side of B
               // (training quantiles m_lo, m_hi of label - est) are decided at
               // once; the rest are queued for the network.  Only cells that
               // would otherwise open into more than a bucket of particle
               // pairs are worth a far-field evaluation.
               const float4 g4 = __ldg(&a.geom[node]);
-              const double dd = sqrt(d2);
-              const double margin = dd - (double)g4.y;
-              const float rho = margin > 0.0 ? (float)((double)g4.x / margin) : 3.0e38f;
+              const float ddf = sqrtf((float)d2);
+              const float margin = ddf - g4.y;
+              const float rho = margin > 0.f ? g4.x / margin : 3.0e38f;
               if (rho <= a.rho_hi && g4.z > (float)a.bucket) {
-                const float ddf = (float)dd;
                 const float tn = __ldg(&a.mom3[3 * (int64_t)node + 2]).z;
-                const float est = mac_estimate(tn, g4.z, ddf);
+                const float est = mac_prefilter(g4, tn, ddf, fmodel + 2);
                 const float B = log10f(budget * ddf * ddf / g4.z);
-                if (est + m_hi <= B) {
+                if (est + fmodel[1] <= B) {
                   accept = true;
-                } else if (est + m_lo <= B) {
+                } else if (est + fmodel[0] <= B) {
                   cand = true;
                   cand_d = ddf;
                   cand_B = B;

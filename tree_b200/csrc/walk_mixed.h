@@ -42,7 +42,7 @@ struct LearnedMac {
   const MlpPacked* packed = nullptr;  // device
   const float* fmin = nullptr;        // device, 16: training range
   const float* fmax = nullptr;        // device, 16
-  const float* margins = nullptr;     // device, 2: quantiles of label - estimate
+  const float* margins = nullptr;     // device, 7: m_lo, m_hi, pre-filter c0..c4
   const double* f_prev = nullptr;     // device forces of the previous step
   float eta = 1e-5f;
   float rho_lo = 0.2f, rho_hi = 0.9f;

@@ -61,9 +61,12 @@ def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
         t2 = time.time()
         params, stats = tf.mac_get_model()
         feats, labels, extra = tf.mac_samples()
-    est = feats[:, 15]
+    coef = stats[66:71].astype(np.float64)
+    est = (coef[0] * feats[:, 14] + coef[1] * feats[:, 3] + coef[2] * feats[:, 7] +
+           coef[3] * feats[:, 6] + coef[4])
     report.update({"samples": int(len(labels)), "collect_s": t1 - t0,
                    "margins": [float(stats[64]), float(stats[65])],
+                   "prefilter_coef": [float(c) for c in coef],
                    "corr_label_estimate": float(np.corrcoef(labels, est)[0, 1]),
                    "train_s": t2 - t1, "loss_per_epoch": [float(x) for x in losses],
                    "label_quantiles": {str(q): float(np.quantile(labels, q))
