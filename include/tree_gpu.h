@@ -132,9 +132,43 @@ int tree_gpu_load_state(tree_gpu_handle* h, const double* x_el,
 
 /* Step drop-in for the loop body main.f90:125-131 + VVerletNotemp2: nsteps x
  * (VVerletNotemp1 -> Force -> VVerletNotemp2) on the device with no host
- * traffic.  Kinetic sums are sampled on the last step; `out` may be NULL. */
+ * traffic.  Kinetic sums are sampled on the last step; `out` may be NULL.
+ * Each step body is replayed as a CUDA graph (tree_gpu_set_graphs). */
 int tree_gpu_step(tree_gpu_handle* h, double dt, int32_t nsteps,
                   tree_gpu_diag* out);
+
+/* One TEMPORAL sample (sample.f90:55-96 before its unit conversions): the
+ * sums VVerletNotemp2 forms on sample steps (vverlet.f90:81-106) and the
+ * potential energies of that step's Force. */
+typedef struct tree_gpu_sample {
+  int64_t nloop;   /* ttime%Nloop of the sample step */
+  double epot_e;   /* sys%Epot_e */
+  double epot_i;   /* sys%Epot_i */
+  double mv2_el;   /* sys%mv2el */
+  double mv2_ion;  /* sys%mv2ion */
+  double rad_el;   /* sys%Te_rad (sum m (x.v)^2/|x|^2) */
+  double rad_ion;  /* sys%Ti_rad */
+} tree_gpu_sample;
+
+/* The step loop main.f90:123-160 for nsteps steps with the reference's
+ * cadence.  Steps are numbered by Nloop, which tree_gpu_set_state and
+ * tree_gpu_load_state reset to 0 (main.f90:113); every step with
+ * Nloop % nsamp == 0 (nsamp > 0) forms the kinetic sums and writes one record
+ * to series[] (at most series_cap; *n_series = records written), all on the
+ * device.  rdf_ei / rdf_ii (kRdfBins = 10001 entries each, either may be
+ * NULL) accumulate the near-field pair counts of EVERY step, as NS%RDF_ei /
+ * NS%RDF_ii do in Force (tree.f90:918, 1126); the caller dumps and resets
+ * them as RDF (sample.f90:5-50) does every Ndump steps. */
+int tree_gpu_run(tree_gpu_handle* h, double dt, int32_t nsteps, int32_t nsamp,
+                 tree_gpu_sample* series, int32_t series_cap, int32_t* n_series,
+                 int64_t* rdf_ei, int64_t* rdf_ii);
+
+/* Replays each step body as a CUDA graph (enable != 0, the default) or
+ * enqueues its kernels one by one (enable = 0; per-step phase timings). */
+int tree_gpu_set_graphs(tree_gpu_handle* h, int32_t enable);
+
+/* Current Nloop of the device-resident state. */
+int tree_gpu_get_nloop(tree_gpu_handle* h, int64_t* nloop);
 
 /* Copies the device-resident state to host buffers (any may be NULL), for
  * Restart/RDF/TEMPORAL steps (print.f90:5-109, sample.f90). */

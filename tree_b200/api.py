@@ -30,6 +30,7 @@ RDF_BINS = 10001
 # Every symbol include/tree_gpu.h declares.
 EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
            "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step",
+           "tree_gpu_run", "tree_gpu_set_graphs", "tree_gpu_get_nloop",
            "tree_gpu_get_state", "tree_gpu_direct", "tree_gpu_direct_static",
            "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning",
            "tree_gpu_mac_collect", "tree_gpu_mac_samples", "tree_gpu_mac_clear",
@@ -53,6 +54,13 @@ class Diag(ctypes.Structure):
                 ("mv2_el", ctypes.c_double), ("mv2_ion", ctypes.c_double),
                 ("rad_el", ctypes.c_double), ("rad_ion", ctypes.c_double),
                 ("steps_done", ctypes.c_int64)]
+
+
+class Sample(ctypes.Structure):
+    _fields_ = [("nloop", ctypes.c_int64), ("epot_e", ctypes.c_double),
+                ("epot_i", ctypes.c_double), ("mv2_el", ctypes.c_double),
+                ("mv2_ion", ctypes.c_double), ("rad_el", ctypes.c_double),
+                ("rad_ion", ctypes.c_double)]
 
 
 class Timing(ctypes.Structure):
@@ -90,6 +98,11 @@ def load_library(path: str = LIB_PATH):
     L.tree_gpu_load_state.argtypes = [vp, dp, dp, dp, dp, dp, dp]
     L.tree_gpu_step.argtypes = [vp, ctypes.c_double, ctypes.c_int32,
                                 ctypes.POINTER(Diag)]
+    L.tree_gpu_run.argtypes = [vp, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                               ctypes.POINTER(Sample), ctypes.c_int32,
+                               ctypes.POINTER(ctypes.c_int32), lp, lp]
+    L.tree_gpu_set_graphs.argtypes = [vp, ctypes.c_int32]
+    L.tree_gpu_get_nloop.argtypes = [vp, lp]
     L.tree_gpu_get_state.argtypes = [vp, dp, dp, dp, dp, dp, dp]
     L.tree_gpu_tree_dump.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, dp,
                                      dp, dp, ctypes.POINTER(ctypes.c_int32),
@@ -261,6 +274,36 @@ class TreeForce:
         d = Diag()
         self._check(self.lib.tree_gpu_step(self.h, dt, nsteps, ctypes.byref(d)))
         return d
+
+    def run(self, dt: float, nsteps: int, nsamp: int = 0, rdf: bool = False):
+        """The step loop with the reference's sampling cadence.  Returns the
+        sample records (a structured array) and, with rdf, the (rdf_ei,
+        rdf_ii) pair counts accumulated over every step of the call."""
+        ns = max(1, nsteps // nsamp + 1) if nsamp > 0 else 1
+        buf = (Sample * ns)()
+        cnt = ctypes.c_int32(0)
+        r_ei = np.zeros(RDF_BINS, np.int64) if rdf else None
+        r_ii = np.zeros(RDF_BINS, np.int64) if rdf else None
+        lp = ctypes.POINTER(ctypes.c_int64)
+        self._check(self.lib.tree_gpu_run(
+            self.h, dt, nsteps, nsamp, buf, ns, ctypes.byref(cnt),
+            r_ei.ctypes.data_as(lp) if rdf else None,
+            r_ii.ctypes.data_as(lp) if rdf else None))
+        dtype = np.dtype([(name, np.int64 if name == "nloop" else np.float64)
+                          for name, _ in Sample._fields_])
+        rec = np.zeros(cnt.value, dtype)
+        for k in range(cnt.value):
+            for name, _ in Sample._fields_:
+                rec[name][k] = getattr(buf[k], name)
+        return (rec, (r_ei, r_ii)) if rdf else rec
+
+    def set_graphs(self, enable: bool):
+        self._check(self.lib.tree_gpu_set_graphs(self.h, 1 if enable else 0))
+
+    def nloop(self) -> int:
+        v = ctypes.c_int64(0)
+        self._check(self.lib.tree_gpu_get_nloop(self.h, ctypes.byref(v)))
+        return v.value
 
     def get_state(self):
         x_el = np.empty((self.n_el, 3))

@@ -8,9 +8,9 @@
 // per-particle "replayed" paths cut at the first level where a particle is
 // alone.  This file:
 //   1. reduces the per-species bounding box (tree.f90:52-63),
-//   2. replays each particle's path for 21 levels into a 63-bit key (3 bits
+//   2. replays each particle's path for 42 levels into a 128-bit key (3 bits
 //      per level, child digit = bx + 2 by + 4 bz, the reference's bias-1),
-//      with the species in bit 63,
+//      with the species in bit 127,
 //   3. sorts (key, index) with an LSD radix sort (8-bit digits),
 //   4. derives the reference topology from adjacent common-prefix lengths and
 //      emits nodes directly in pre-order (children 1..8 = the reference's
@@ -115,14 +115,19 @@ __global__ void k_geom(const uint64_t* bb, int n, int n_el, Geom* g) {
 
 // ---------------------------------------------------------------- keys ----
 // Replays Insert_Tree's descent (tree.f90:132-173 comparisons, 123-126 child
-// centres) for 21 levels.
-// Key layouts.  Per-species trees (lsb = 0): bit 63 = species, bits 62..0 =
-// 21 levels of 3 bits.  Combined tree (lsb = 1): bits 63..1 = 21 levels,
-// bit 0 = species, a 22nd one-bit level that separates an electron sitting
-// exactly on an ion (the t = 0 state of the clouds).
+// centres) for 42 levels.  The reference recursion has no depth limit; 42
+// levels resolve 2^-42 of the root box, so clouds whose box has grown by
+// orders of magnitude (escaping electrons) still separate every particle.
+// Key layouts (level l = 1..42, digit d_l):
+//   per-species trees (lsb = 0): bit 127 = species, d_l in bits
+//     (127 - 3l) .. (125 - 3l), bit 0 = 0;
+//   combined tree (lsb = 1): d_l in bits (128 - 3l) .. (126 - 3l), bit 1 = 0,
+//     bit 0 = species, a 43rd one-bit level that separates an electron
+//     sitting exactly on an ion (the t = 0 state of the clouds).
+// In both, the digit of level l is (key >> (127 - 3l + lsb)) & 7.
 __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
                        int lsb, int n_el_charge, const Geom* __restrict__ geom,
-                       uint64_t* keys, uint32_t* vals) {
+                       key128* keys, uint32_t* vals) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int s = i >= n_el;
@@ -134,7 +139,7 @@ __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
     c[k] = G.c0[k];
     lx[k] = G.lx0[k];
   }
-  uint64_t key = 0;
+  key128 key = 0;
   for (int l = 0; l < kMaxLevel; ++l) {
     uint32_t b = 0;
 #pragma unroll
@@ -144,10 +149,10 @@ __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
       c[k] = c[k] + (hi ? 0.25 : -0.25) * lx[k];
       lx[k] = lx[k] * 0.5;
     }
-    key = (key << 3) | b;
+    key = (key << 3) | (key128)b;
   }
-  if (lsb) key = (key << 1) | (i >= n_el_charge ? 1ull : 0ull);
-  else key |= s ? kSpeciesBit : 0ull;
+  if (lsb) key = (key << 2) | (key128)(i >= n_el_charge ? 1u : 0u);
+  else key = (key << 1) | ((key128)(s ? 1u : 0u) << 127);
   keys[i] = key;
   vals[i] = (uint32_t)i;
 }
@@ -272,7 +277,8 @@ constexpr int kRsBins = 256;
 
 int radix_blocks(int n) { return (n + kRsTile - 1) / kRsTile; }
 
-__global__ void k_rs_hist(const uint64_t* __restrict__ keys, int n, int shift,
+template <class K>
+__global__ void k_rs_hist(const K* __restrict__ keys, int n, int shift,
                           int32_t* hist /* [256][nb] */) {
   __shared__ int32_t h[kRsBins];
   for (int b = threadIdx.x; b < kRsBins; b += blockDim.x) h[b] = 0;
@@ -280,7 +286,7 @@ __global__ void k_rs_hist(const uint64_t* __restrict__ keys, int n, int shift,
   int64_t base = (int64_t)blockIdx.x * kRsTile;
   for (int j = 0; j < kRsIters; ++j) {
     int64_t i = base + (int64_t)j * kRsThreads + threadIdx.x;
-    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xff], 1);
+    if (i < n) atomicAdd(&h[(int)((keys[i] >> shift) & 0xff)], 1);
   }
   __syncthreads();
   for (int b = threadIdx.x; b < kRsBins; b += blockDim.x)
@@ -289,11 +295,12 @@ __global__ void k_rs_hist(const uint64_t* __restrict__ keys, int n, int shift,
 
 // Stable scatter: tile order is warp-major (warp w owns items
 // [w*512, w*512+512) of the tile), then iteration, then lane.
+template <class K>
 __global__ void __launch_bounds__(kRsThreads)
-    k_rs_scatter(const uint64_t* __restrict__ keys_in,
+    k_rs_scatter(const K* __restrict__ keys_in,
                  const uint32_t* __restrict__ vals_in, int n, int shift,
                  const int32_t* __restrict__ offs /* scanned [256][nb] */,
-                 uint64_t* __restrict__ keys_out,
+                 K* __restrict__ keys_out,
                  uint32_t* __restrict__ vals_out) {
   __shared__ int32_t whist[kRsWarps][kRsBins];
   __shared__ int32_t base_s[kRsBins];
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(kRsThreads)
   }
   __syncthreads();
   int64_t wbase = (int64_t)blockIdx.x * kRsTile + (int64_t)w * (32 * kRsIters);
-  uint64_t k[kRsIters];
+  K k[kRsIters];
   uint32_t v[kRsIters];
   int32_t loc[kRsIters];
   const unsigned lt = (1u << lane) - 1u;
@@ -313,7 +320,7 @@ __global__ void __launch_bounds__(kRsThreads)
   for (int j = 0; j < kRsIters; ++j) {
     int64_t i = wbase + j * 32 + lane;
     bool ok = i < n;
-    k[j] = ok ? keys_in[i] : 0ull;
+    k[j] = ok ? keys_in[i] : (K)0;
     v[j] = ok ? vals_in[i] : 0u;
     int d = ok ? (int)((k[j] >> shift) & 0xff) : kRsBins;  // sentinel bin
     unsigned peers = __match_any_sync(0xffffffffu, d);
@@ -346,49 +353,59 @@ __global__ void __launch_bounds__(kRsThreads)
   }
 }
 
-// Sorts (keys, vals) in place using the alternate buffers; 8 passes of 8
-// bits, so the result ends in the primary buffers.
-int radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
-               uint32_t* vals_alt, int n, int32_t* hist, int32_t* partial,
-               cudaStream_t st) {
+// Sorts (keys, vals) in place using the alternate buffers; an even number of
+// 8-bit passes, so the result ends in the primary buffers.
+template <class K>
+int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
+               int32_t* hist, int32_t* partial, cudaStream_t st) {
   if (n <= 1) return 0;
   int launches = 0;
   int nb = radix_blocks(n);
-  uint64_t* kin = keys;
+  K* kin = keys;
   uint32_t* vin = vals;
-  uint64_t* kout = keys_alt;
+  K* kout = keys_alt;
   uint32_t* vout = vals_alt;
-  for (int pass = 0; pass < 8; ++pass) {
+  for (int pass = 0; pass < (int)sizeof(K); ++pass) {
     int shift = pass * 8;
-    k_rs_hist<<<nb, kRsThreads, 0, st>>>(kin, n, shift, hist);
+    k_rs_hist<K><<<nb, kRsThreads, 0, st>>>(kin, n, shift, hist);
     launches += 2 + exclusive_scan(hist, hist, kRsBins * nb, partial, false, st);
-    k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kin, vin, n, shift, hist, kout,
-                                            vout);
-    uint64_t* tk = kin; kin = kout; kout = tk;
+    k_rs_scatter<K><<<nb, kRsThreads, 0, st>>>(kin, vin, n, shift, hist, kout,
+                                               vout);
+    K* tk = kin; kin = kout; kout = tk;
     uint32_t* tv = vin; vin = vout; vout = tv;
   }
   return launches;
 }
 
+template int radix_sort<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, int,
+                                  int32_t*, int32_t*, cudaStream_t);
+template int radix_sort<key128>(key128*, uint32_t*, key128*, uint32_t*, int,
+                                int32_t*, int32_t*, cudaStream_t);
+
 // ------------------------------------------------------------ topology ----
+__device__ __forceinline__ int clz128(key128 x) {
+  const uint64_t hi = (uint64_t)(x >> 64), lo = (uint64_t)x;
+  return hi ? __clzll((long long)hi) : 64 + __clzll((long long)lo);
+}
+
 // L[p] = number of leading levels that sorted keys p and p+1 share (same
-// species), else -1.  Identical keys mean the 21-level cap was hit.
-__global__ void k_common_levels(const uint64_t* __restrict__ keys, int n,
+// species), else -1.  Identical keys mean the 42-level cap was hit.
+__global__ void k_common_levels(const key128* __restrict__ keys, int n,
                                 int lsb, int8_t* L, int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int8_t r = -1;
   if (p + 1 < n) {
-    uint64_t a = keys[p], b = keys[p + 1];
-    uint64_t x = a ^ b;
-    if (lsb || (x >> 63) == 0) {
+    key128 a = keys[p], b = keys[p + 1];
+    key128 x = a ^ b;
+    if (lsb || (x >> 127) == 0) {
       if (x == 0) {
         set_error(err, kErrDepth);
         r = kMaxLevel;
       } else {
-        int lz = __clzll((long long)x);
-        // lsb = 0: lz >= 1 (species bit equal); lsb = 1: lz = 63 means only
-        // the species bit differs, i.e. all 21 spatial levels are shared
+        int lz = clz128(x);
+        // lsb = 0: lz >= 1 (species bit equal); lsb = 1: lz = 127 means only
+        // the species bit differs, i.e. all 42 spatial levels are shared
         int lev = lsb ? lz / 3 : (lz - 1) / 3;
         r = (int8_t)(lev < kMaxLevel ? lev : kMaxLevel);
       }
@@ -413,9 +430,9 @@ __global__ void k_counts(const int8_t* __restrict__ L, int n, int32_t* cnt) {
 }
 
 // first q in [lo_i, hi_i) with (keys[q] >> sh) > pre ; keys sorted
-__device__ __forceinline__ int upper_prefix(const uint64_t* __restrict__ keys,
+__device__ __forceinline__ int upper_prefix(const key128* __restrict__ keys,
                                             int lo_i, int hi_i, int sh,
-                                            uint64_t pre) {
+                                            key128 pre) {
   while (lo_i < hi_i) {
     int mid = lo_i + ((hi_i - lo_i) >> 1);
     if ((keys[mid] >> sh) > pre) hi_i = mid;
@@ -424,9 +441,9 @@ __device__ __forceinline__ int upper_prefix(const uint64_t* __restrict__ keys,
   return lo_i;
 }
 // first q in [lo_i, hi_i) with (keys[q] >> sh) >= pre
-__device__ __forceinline__ int lower_prefix(const uint64_t* __restrict__ keys,
+__device__ __forceinline__ int lower_prefix(const key128* __restrict__ keys,
                                             int lo_i, int hi_i, int sh,
-                                            uint64_t pre) {
+                                            key128 pre) {
   while (lo_i < hi_i) {
     int mid = lo_i + ((hi_i - lo_i) >> 1);
     if ((keys[mid] >> sh) >= pre) hi_i = mid;
@@ -435,20 +452,20 @@ __device__ __forceinline__ int lower_prefix(const uint64_t* __restrict__ keys,
   return lo_i;
 }
 
-// Shift that leaves the first d levels of a key (1 <= d <= 21); level 22 of
+// Shift that leaves the first d levels of a key (1 <= d <= 42); level 43 of
 // the combined layout is the whole key.
 __device__ __forceinline__ int shift_for_level(int d, int lsb) {
-  int s = 63 - 3 * d + lsb;
+  int s = 127 - 3 * d + lsb;
   return s > 0 ? s : 0;
 }
 
 // Index of the twig at level d that contains sorted particle p, given that it
 // was opened at an earlier particle (first particle of the level-d prefix).
 __device__ __forceinline__ int twig_index_before(
-    const uint64_t* __restrict__ keys, const int8_t* __restrict__ L,
+    const key128* __restrict__ keys, const int8_t* __restrict__ L,
     const int32_t* __restrict__ off, int sb, int p, int d, int lsb) {
   int sh = shift_for_level(d, lsb);
-  uint64_t pre = keys[p] >> sh;
+  key128 pre = keys[p] >> sh;
   int q = lower_prefix(keys, sb, p + 1, sh, pre);
   int lo_q = q == 0 ? -1 : (int)L[q - 1];
   return off[q] + (d - lo_q - 1);
@@ -456,7 +473,7 @@ __device__ __forceinline__ int twig_index_before(
 
 // Writes every node in pre-order.  node_c.xyz of twigs receives the
 // geometric centre (replayed like k_keys); the upward pass replaces it.
-__global__ void k_topology(const uint64_t* __restrict__ keys,
+__global__ void k_topology(const key128* __restrict__ keys,
                            const uint32_t* __restrict__ vals,
                            const int8_t* __restrict__ L,
                            const int32_t* __restrict__ off, int n, int n_el,
@@ -473,7 +490,7 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
   int sb = s ? n_el : 0, se = s ? n : n_el;
   int tree_end = off[se];
   int base = off[p];
-  uint64_t key = keys[p];
+  key128 key = keys[p];
   const Geom& G = geom[s];
   double c[3], lx[3];
 #pragma unroll
@@ -508,7 +525,7 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
       // particle range and child table used by the mixed-precision walk
       mx.first[idx] = p;
       mx.count[idx] = q_end - p;
-      mx.digit[idx] = d == 0 ? (int8_t)0 : (int8_t)((key >> (63 - 3 * d + lsb)) & 7);
+      mx.digit[idx] = d == 0 ? (int8_t)0 : (int8_t)((key >> (127 - 3 * d + lsb)) & 7);
       int4* kk = reinterpret_cast<int4*>(mx.kids + 8 * (int64_t)idx);
       kk[0] = make_int4(-1, -1, -1, -1);
       kk[1] = make_int4(-1, -1, -1, -1);
@@ -520,7 +537,7 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
     }
     // descend one level along this particle's digits
     if (d < kMaxLevel) {
-      int dig = (int)((key >> (60 - 3 * d + lsb)) & 7);
+      int dig = (int)((key >> (124 - 3 * d + lsb)) & 7);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         bool bit = (dig >> k) & 1;
@@ -543,8 +560,8 @@ __global__ void k_topology(const uint64_t* __restrict__ keys,
   node_nchild[leaf] = 0;
   mx.first[leaf] = p;
   mx.count[leaf] = 1;
-  mx.digit[leaf] = depth <= kMaxLevel ? (int8_t)((key >> (63 - 3 * depth + lsb)) & 7)
-                                      : (int8_t)(lsb ? (key & 1) : 0);
+  mx.digit[leaf] = depth <= kMaxLevel ? (int8_t)((key >> (127 - 3 * depth + lsb)) & 7)
+                                      : (int8_t)(lsb ? (int)(key & 1) : 0);
   node_parent[leaf] = ntw > 0 ? leaf - 1
                               : twig_index_before(keys, L, off, sb, p, depth - 1, lsb);
 }

@@ -25,8 +25,8 @@ struct MixedNodes {
 
 struct BuildBuffers {
   // particle-indexed (n)
-  uint64_t* keys;
-  uint64_t* keys_alt;
+  key128* keys;
+  key128* keys_alt;
   uint32_t* vals;       // sorted position -> global particle index
   uint32_t* vals_alt;
   int8_t* L;            // common levels with the next sorted key
@@ -56,9 +56,11 @@ int radix_blocks(int n);
 int scan_partials_needed(int n);
 int exclusive_scan(const int32_t* in, int32_t* out, int n, int32_t* partial,
                    bool write_total, cudaStream_t st);
-int radix_sort(uint64_t* keys, uint32_t* vals, uint64_t* keys_alt,
-                uint32_t* vals_alt, int n, int32_t* hist, int32_t* partial,
-                cudaStream_t st);
+// Stable LSD radix sort of (keys, vals) by all bytes of the key (8 passes for
+// uint64_t keys, 16 for key128); the result ends in the primary buffers.
+template <class K>
+int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
+               int32_t* hist, int32_t* partial, cudaStream_t st);
 // Builds the trees for positions x (AoS, electrons first).  mode 0: one tree
 // per species with the reference's one-level moments (parity path); mode 1:
 // one combined tree with net-charge moments and target groups (mixed path).

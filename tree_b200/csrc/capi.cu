@@ -37,6 +37,19 @@ struct EventSet {
   cudaEvent_t e[4];
 };
 
+// One captured step body (force + second kick [+ samples] [+ RDF fold]).
+struct StepGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  EventSet ev{};
+  bool has_ev = false;
+  cudaGraphNode_t ev_node[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t epoch = 0;
+  double dt = 0.0;
+  int64_t launches = 0;  // kernels in one replay
+  int64_t replays = 0;   // replays during the current call
+};
+
 }  // namespace
 
 struct tree_gpu_handle {
@@ -75,6 +88,16 @@ struct tree_gpu_handle {
   tree_gpu_timing timing{};
   std::vector<EventSet> events;
   std::string last_error;
+  // step loop: CUDA graphs of the step body, [sample][last][rdf]
+  StepGraph graphs[2][2][2];
+  bool use_graphs = true;
+  uint64_t epoch = 1;        // bumped whenever a captured argument may change
+  bool capturing = false;    // a step body is being captured into a graph
+  int64_t nloop = 0;         // ttime%Nloop: steps since the state was set
+  double* series = nullptr;  // sample records of a run, 6 doubles each
+  int32_t* series_count = nullptr;
+  int series_cap = 0;
+  unsigned long long* rdf64 = nullptr;  // RDF sums of a run (2 x kRdfBins)
 };
 
 namespace {
@@ -130,6 +153,7 @@ int dalloc(tree_gpu_handle* h, T** p, size_t count) {
 int alloc_nodes(tree_gpu_handle* h, int cap) {
   tg::BuildBuffers& b = h->b;
   b.cap = cap;
+  ++h->epoch;  // captured step graphs hold the old node pointers
   int rc = 0;
   if ((rc = dalloc(h, &b.node_c, cap))) return rc;
   if ((rc = dalloc(h, &b.node_m, 5 * (size_t)cap))) return rc;
@@ -189,7 +213,8 @@ void free_all(tree_gpu_handle* h) {
                   b.node_skip, b.node_pt, b.node_parent, b.node_nchild,
                   b.node_done, b.node_level, h->rdf, h->counters, h->partial,
                   h->diag, h->mlp_params, h->mlp_stats, h->mlp_packed,
-                  h->smp_feats, h->smp_labels, h->smp_extra, h->smp_count};
+                  h->smp_feats, h->smp_labels, h->smp_extra, h->smp_count,
+                  h->series, h->series_count, h->rdf64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   tg::mixed_free(h->mb);
@@ -227,14 +252,21 @@ EventSet& events_for(tree_gpu_handle* h, size_t i) {
   return h->events[i];
 }
 
+// Records a timing event; inside a capture it becomes an event-record node
+// of the graph, so every replay records it.
+void record(tree_gpu_handle* h, cudaEvent_t e) {
+  cudaEventRecordWithFlags(e, h->st, h->capturing ? cudaEventRecordExternal
+                                                  : cudaEventRecordDefault);
+}
+
 // Enqueues build + walk + potential-energy sum on the handle's stream.
 void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
   cudaStream_t st = h->st;
-  if (ev) cudaEventRecord(ev->e[0], st);
+  if (ev) record(h, ev->e[0]);
   const int mode = h->prm.precision == TREE_GPU_PREC_FP64 ? 0 : 1;
   h->timing.launches +=
       tg::build_trees(h->b, h->x, h->n, (int)h->n_el, h->prm.theta, mode, st);
-  if (ev) cudaEventRecord(ev->e[1], st);
+  if (ev) record(h, ev->e[1]);
   cudaMemsetAsync(h->counters, 0, 4 * sizeof(unsigned long long), st);
   if (with_rdf)
     cudaMemsetAsync(h->rdf, 0, 2 * sizeof(uint32_t) * tg::kRdfBins, st);
@@ -262,7 +294,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
                    use_learned ? &lm : nullptr, h->f, h->epot_part,
                    with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
   }
-  if (ev) cudaEventRecord(ev->e[2], st);
+  if (ev) record(h, ev->e[2]);
   h->timing.launches += (h->n > 0 ? 1 : 0) + 2;  // walk + epot partial/sum
   // (the mixed walk is one kernel as well)
   tg::epot_sum(h->epot_part, h->n, h->partial, h->diag, st);
@@ -311,7 +343,10 @@ void read_counters(tree_gpu_handle* h) {
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, a, b);
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();  // not recorded: no time, and no error left behind
+    ms = 0.f;
+  }
   return ms;
 }
 
@@ -336,6 +371,174 @@ int force_device(tree_gpu_handle* h, bool with_rdf) {
     if ((rc = grow_nodes(h))) return rc;
   }
   return fail(h, TREE_GPU_ERR_CAPACITY, "node capacity growth did not converge");
+}
+
+// One step of the main loop after the first half kick: Force, the second
+// half kick fused with the next first half kick and drift (unless last), the
+// kinetic sums and a sample record on sample steps, the RDF fold.
+void enqueue_step_body(tree_gpu_handle* h, double dt, bool sample, bool last,
+                       bool rdf, EventSet* ev) {
+  const tree_gpu_params& p = h->prm;
+  const int n = h->n, ne = (int)h->n_el;
+  enqueue_force(h, rdf, ev);
+  tg::kick2(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, sample, !last,
+            h->partial, h->diag + 4, h->st);
+  h->timing.launches += n > 0 ? (sample ? 2 : 1) : 0;
+  if (rdf) {
+    tg::rdf_fold(h->rdf, h->rdf64, h->st);
+    h->timing.launches += 1;
+  }
+  if (sample && h->series) {
+    tg::sample_append(h->diag, h->series, h->series_count, h->series_cap, h->st);
+    h->timing.launches += 1;
+  }
+  if (ev) record(h, ev->e[3]);
+}
+
+// The captured graph of a step-body variant, captured on first use or after
+// any argument it holds changed; nullptr when capture is not possible on
+// this stream (the caller then enqueues the body directly).
+StepGraph* graph_for(tree_gpu_handle* h, double dt, bool sample, bool last, bool rdf) {
+  StepGraph& g = h->graphs[sample][last][rdf];
+  if (g.exec && g.epoch == h->epoch && g.dt == dt) return &g;
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g.exec = nullptr;
+  g.graph = nullptr;
+  if (!g.has_ev) {
+    for (int k = 0; k < 4; ++k) cudaEventCreate(&g.ev.e[k]);
+    g.has_ev = true;
+  }
+  if (cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  const int64_t l0 = h->timing.launches;
+  h->capturing = true;
+  enqueue_step_body(h, dt, sample, last, rdf, &g.ev);
+  h->capturing = false;
+  g.launches = h->timing.launches - l0;
+  h->timing.launches = l0;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->st, &graph);
+  if (e != cudaSuccess || graph == nullptr) {
+    cudaGetLastError();
+    if (graph) cudaGraphDestroy(graph);
+    return nullptr;
+  }
+  // the event-record nodes, so each replay can record into its own events
+  size_t nn = 0;
+  cudaGraphGetNodes(graph, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) cudaGraphGetNodes(graph, nodes.data(), &nn);
+  for (int k = 0; k < 4; ++k) g.ev_node[k] = nullptr;
+  for (cudaGraphNode_t nd : nodes) {
+    cudaGraphNodeType ty;
+    cudaEvent_t evn = nullptr;
+    if (cudaGraphNodeGetType(nd, &ty) != cudaSuccess || ty != cudaGraphNodeTypeEventRecord)
+      continue;
+    if (cudaGraphEventRecordNodeGetEvent(nd, &evn) != cudaSuccess) continue;
+    for (int k = 0; k < 4; ++k)
+      if (evn == g.ev.e[k]) g.ev_node[k] = nd;
+  }
+  e = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(graph);
+    g.exec = nullptr;
+    return nullptr;
+  }
+  g.graph = graph;
+  g.epoch = h->epoch;
+  g.dt = dt;
+  return &g;
+}
+
+void free_graphs(tree_gpu_handle* h) {
+  for (auto& a : h->graphs)
+    for (auto& b2 : a)
+      for (StepGraph& g : b2) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        if (g.has_ev)
+          for (int k = 0; k < 4; ++k) cudaEventDestroy(g.ev.e[k]);
+        g = StepGraph();
+      }
+}
+
+// The step loop of main.f90:123-160 for nsteps steps.  Step Nloop samples
+// when nsamp > 0 and Nloop % nsamp == 0 (vverlet.f90:81, main.f90:150), and
+// always on the last step when sample_last; samples go to the series buffer
+// when it is set.  With rdf, the near-field pair counts of every step are
+// added to h->rdf64.
+int run_impl(tree_gpu_handle* h, double dt, int32_t nsteps, int32_t nsamp,
+             bool sample_last, bool rdf) {
+  const int n = h->n, ne = (int)h->n_el;
+  const tree_gpu_params& p = h->prm;
+  events_for(h, (size_t)nsteps + 1);  // grow first: references below stay valid
+  EventSet& et = events_for(h, 0);
+  for (auto& a : h->graphs)
+    for (auto& b2 : a)
+      for (StepGraph& g : b2) g.replays = 0;
+  std::vector<char> own_ev((size_t)nsteps, 0);  // step s recorded events[1 + s]
+  cudaEventRecord(et.e[0], h->st);
+  tg::kick_drift(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, h->st);
+  h->timing.launches += n > 0 ? 1 : 0;
+  for (int s = 0; s < nsteps; ++s) {
+    const int64_t nl = h->nloop + s + 1;
+    const bool last = s == nsteps - 1;
+    const bool sample = (nsamp > 0 && nl % nsamp == 0) || (sample_last && last);
+    StepGraph* g = h->use_graphs ? graph_for(h, dt, sample, last, rdf) : nullptr;
+    EventSet& ev = events_for(h, 1 + (size_t)s);
+    if (g) {
+      // point the replay's event-record nodes at this step's events
+      bool own = true;
+      for (int k = 0; k < 4; ++k)
+        own = own && g->ev_node[k] &&
+              cudaGraphExecEventRecordNodeSetEvent(g->exec, g->ev_node[k], ev.e[k]) ==
+                  cudaSuccess;
+      if (!own) cudaGetLastError();
+      own_ev[s] = own ? 1 : 0;
+      CK(cudaGraphLaunch(g->exec, h->st));
+      g->replays += own ? 0 : 1;
+      h->timing.launches += g->launches;
+    } else {
+      own_ev[s] = 1;
+      enqueue_step_body(h, dt, sample, last, rdf, &ev);
+    }
+  }
+  cudaEventRecord(et.e[1], h->st);
+  CK(cudaGetLastError());
+  bool grow = false;
+  int rc = check_device_status(h, &grow);
+  if (rc) return rc;
+  if (grow) {
+    // The positions already moved; a capacity miss means the forces of this
+    // batch are invalid.  Report it: the caller restores state and retries.
+    if ((rc = grow_nodes(h))) return rc;
+    return fail(h, TREE_GPU_ERR_CAPACITY,
+                "node capacity grew during step; state must be reloaded");
+  }
+  // phase times from each step's own events; a replay whose event nodes could
+  // not be retargeted counts with its variant's last replay
+  for (int s = 0; s < nsteps; ++s) {
+    if (!own_ev[s]) continue;
+    EventSet& ev = events_for(h, 1 + (size_t)s);
+    h->timing.ms_build += elapsed(ev.e[0], ev.e[1]);
+    h->timing.ms_walk += elapsed(ev.e[1], ev.e[2]);
+  }
+  for (auto& a : h->graphs)
+    for (auto& b2 : a)
+      for (StepGraph& g : b2)
+        if (g.replays > 0) {
+          h->timing.ms_build += g.replays * elapsed(g.ev.e[0], g.ev.e[1]);
+          h->timing.ms_walk += g.replays * elapsed(g.ev.e[1], g.ev.e[2]);
+        }
+  h->timing.ms_total += elapsed(et.e[0], et.e[1]);
+  h->timing.calls += nsteps;
+  h->nloop += nsteps;
+  read_counters(h);
+  return TREE_GPU_OK;
 }
 
 }  // namespace
@@ -387,6 +590,7 @@ int tree_gpu_set_params(tree_gpu_handle* h, const tree_gpu_params* params) {
     return fail(h, TREE_GPU_ERR_ARG, "invalid parameters");
   h->prm = *params;
   set_lambdas(h);
+  ++h->epoch;
   return TREE_GPU_OK;
 }
 
@@ -458,6 +662,7 @@ int tree_gpu_set_state(tree_gpu_handle* h, const double* x_el,
   if (rc) return rc;
   h->has_state = true;
   h->has_fprev = true;
+  h->nloop = 0;
   return TREE_GPU_OK;
 }
 
@@ -484,6 +689,7 @@ int tree_gpu_load_state(tree_gpu_handle* h, const double* x_el,
   }
   h->has_state = true;
   h->has_fprev = true;
+  h->nloop = 0;
   return TREE_GPU_OK;
 }
 
@@ -493,59 +699,98 @@ int tree_gpu_step(tree_gpu_handle* h, double dt, int32_t nsteps,
   if (!h->has_state) return fail(h, TREE_GPU_ERR_STATE, "tree_gpu_set_state first");
   if (nsteps < 0 || !std::isfinite(dt)) return fail(h, TREE_GPU_ERR_ARG, "bad dt/nsteps");
   if (nsteps == 0) return TREE_GPU_OK;
-  const tree_gpu_params& p = h->prm;
-  const int n = h->n, ne = (int)h->n_el;
-  for (int attempt = 0; attempt < 3; ++attempt) {
-    events_for(h, (size_t)nsteps);  // grow first: references below stay valid
-    EventSet& e0 = events_for(h, 0);
-    cudaEventRecord(e0.e[3], h->st);
-    tg::kick_drift(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, h->st);
-    h->timing.launches += n > 0 ? 1 : 0;
-    for (int s = 0; s < nsteps; ++s) {
-      EventSet& ev = events_for(h, 1 + (size_t)s);
-      enqueue_force(h, false, &ev);
-      bool last = s == nsteps - 1;
-      tg::kick2(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, last, !last,
-                h->partial, h->diag + 4, h->st);
-      h->timing.launches += n > 0 ? (last ? 2 : 1) : 0;
-      cudaEventRecord(ev.e[3], h->st);
-    }
-    CK(cudaGetLastError());
-    bool grow = false;
-    int rc = check_device_status(h, &grow);
-    if (rc) return rc;
-    if (grow) {
-      // The positions already moved; a capacity miss means the forces of this
-      // batch are invalid.  Report it: the caller restores state and retries.
-      if ((rc = grow_nodes(h))) return rc;
-      return fail(h, TREE_GPU_ERR_CAPACITY,
-                  "node capacity grew during step; state must be reloaded");
-    }
-    for (int s = 0; s < nsteps; ++s) {
-      EventSet& ev = events_for(h, 1 + (size_t)s);
-      h->timing.ms_build += elapsed(ev.e[0], ev.e[1]);
-      h->timing.ms_walk += elapsed(ev.e[1], ev.e[2]);
-    }
-    EventSet& elast = events_for(h, (size_t)nsteps);
-    float tot = elapsed(e0.e[3], elast.e[3]);
-    h->timing.ms_total += tot;
-    h->timing.ms_kdk += 0.0;
-    h->timing.calls += nsteps;
-    read_counters(h);
-    if (out) {
-      double d[8];
-      CK(cudaMemcpy(d, h->diag, sizeof(d), cudaMemcpyDeviceToHost));
-      out->epot_e = d[0];
-      out->epot_i = d[1];
-      out->mv2_el = d[4];
-      out->rad_el = d[5];
-      out->mv2_ion = d[6];
-      out->rad_ion = d[7];
-      out->steps_done = nsteps;
-    }
-    return TREE_GPU_OK;
+  double* keep = h->series;
+  h->series = nullptr;  // no sample records, only the last step's sums
+  int rc = run_impl(h, dt, nsteps, 0, true, false);
+  h->series = keep;
+  if (rc) return rc;
+  if (out) {
+    double d[8];
+    CK(cudaMemcpy(d, h->diag, sizeof(d), cudaMemcpyDeviceToHost));
+    out->epot_e = d[0];
+    out->epot_i = d[1];
+    out->mv2_el = d[4];
+    out->rad_el = d[5];
+    out->mv2_ion = d[6];
+    out->rad_ion = d[7];
+    out->steps_done = nsteps;
   }
-  return fail(h, TREE_GPU_ERR_CAPACITY, "capacity");
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_run(tree_gpu_handle* h, double dt, int32_t nsteps, int32_t nsamp,
+                 tree_gpu_sample* series, int32_t series_cap, int32_t* n_series,
+                 int64_t* rdf_ei, int64_t* rdf_ii) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (!h->has_state) return fail(h, TREE_GPU_ERR_STATE, "tree_gpu_set_state first");
+  if (nsteps < 0 || nsamp < 0 || series_cap < 0 || !std::isfinite(dt))
+    return fail(h, TREE_GPU_ERR_ARG, "bad dt/nsteps/nsamp");
+  if (n_series) *n_series = 0;
+  if (nsteps == 0) return TREE_GPU_OK;
+  const bool rdf = rdf_ei || rdf_ii;
+  // sample steps of this call, and room for their records
+  int64_t nsamples = 0;
+  if (nsamp > 0) nsamples = (h->nloop + nsteps) / nsamp - h->nloop / nsamp;
+  const bool want_series = series && series_cap > 0 && nsamples > 0;
+  if (want_series && nsamples > h->series_cap) {
+    const int cap = (int)std::min<int64_t>(nsamples + 16, 1 << 24);
+    if (dalloc(h, &h->series, 6 * (size_t)cap)) return TREE_GPU_ERR_CUDA;
+    if (!h->series_count && dalloc(h, &h->series_count, 1)) return TREE_GPU_ERR_CUDA;
+    h->series_cap = cap;
+    ++h->epoch;
+  }
+  if (rdf && !h->rdf64) {
+    if (dalloc(h, &h->rdf64, 2 * (size_t)tg::kRdfBins)) return TREE_GPU_ERR_CUDA;
+    ++h->epoch;
+  }
+  if (rdf) CK(cudaMemsetAsync(h->rdf64, 0, 2 * sizeof(unsigned long long) * tg::kRdfBins, h->st));
+  if (h->series_count) CK(cudaMemsetAsync(h->series_count, 0, sizeof(int32_t), h->st));
+  double* keep = h->series;
+  if (!want_series) h->series = nullptr;  // sample steps still refresh the sums
+  const int64_t nloop0 = h->nloop;
+  int rc = run_impl(h, dt, nsteps, nsamp, false, rdf);
+  h->series = keep;
+  if (rc) return rc;
+  if (want_series) {
+    int32_t cnt = 0;
+    CK(cudaMemcpy(&cnt, h->series_count, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    const int32_t m = std::min<int32_t>(cnt, series_cap);
+    std::vector<double> buf(6 * (size_t)std::max<int32_t>(m, 1));
+    if (m) CK(cudaMemcpy(buf.data(), h->series, 6 * sizeof(double) * m, cudaMemcpyDeviceToHost));
+    int64_t nl = (nloop0 / nsamp + 1) * nsamp;  // first sample step of the call
+    for (int32_t k = 0; k < m; ++k, nl += nsamp) {
+      series[k].nloop = nl;
+      series[k].epot_e = buf[6 * k];
+      series[k].epot_i = buf[6 * k + 1];
+      series[k].mv2_el = buf[6 * k + 2];
+      series[k].mv2_ion = buf[6 * k + 3];
+      series[k].rad_el = buf[6 * k + 4];
+      series[k].rad_ion = buf[6 * k + 5];
+    }
+    if (n_series) *n_series = m;
+  }
+  if (rdf) {
+    std::vector<unsigned long long> hr(2 * (size_t)tg::kRdfBins);
+    CK(cudaMemcpy(hr.data(), h->rdf64, hr.size() * sizeof(unsigned long long),
+                  cudaMemcpyDeviceToHost));
+    for (int i = 0; i < tg::kRdfBins; ++i) {
+      if (rdf_ei) rdf_ei[i] += (int64_t)hr[i];
+      if (rdf_ii) rdf_ii[i] += (int64_t)hr[tg::kRdfBins + i];
+    }
+  }
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_set_graphs(tree_gpu_handle* h, int32_t enable) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  h->use_graphs = enable != 0;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_get_nloop(tree_gpu_handle* h, int64_t* nloop) {
+  if (!h || !nloop) return TREE_GPU_ERR_ARG;
+  *nloop = h->nloop;
+  return TREE_GPU_OK;
 }
 
 int tree_gpu_get_state(tree_gpu_handle* h, double* x_el, double* v_el,
@@ -672,6 +917,7 @@ int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
   h->tune.bucket = bucket;
   h->tune.blocks_per_sm = blocks_per_sm;
   h->tune.order = order;
+  ++h->epoch;
   return TREE_GPU_OK;
 }
 
@@ -689,6 +935,7 @@ int tree_gpu_destroy(tree_gpu_handle* h) {
   if (!h) return TREE_GPU_OK;
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->own_st && h->own_st != h->st) cudaStreamSynchronize(h->own_st);
+  free_graphs(h);
   free_all(h);
   for (auto& es : h->events)
     for (int k = 0; k < 4; ++k) cudaEventDestroy(es.e[k]);
@@ -833,6 +1080,7 @@ int tree_gpu_mac_train(tree_gpu_handle* h, int32_t epochs, int32_t batch,
                                      h->mlp_packed, h->st);
   CK(cudaStreamSynchronize(h->st));
   h->has_model = true;
+  ++h->epoch;
   return TREE_GPU_OK;
 }
 
@@ -849,6 +1097,7 @@ int tree_gpu_mac_set_model(tree_gpu_handle* h, const float* params,
                                      h->mlp_packed, h->st);
   CK(cudaStreamSynchronize(h->st));
   h->has_model = true;
+  ++h->epoch;
   return TREE_GPU_OK;
 }
 
@@ -866,6 +1115,7 @@ int tree_gpu_mac_config(tree_gpu_handle* h, float eta, float rho_lo, float rho_h
   if (!(eta > 0) || !(rho_lo > 0) || !(rho_hi >= rho_lo))
     return fail(h, TREE_GPU_ERR_ARG, "bad learned-MAC configuration");
   h->mac_eta = eta;
+  ++h->epoch;
   h->mac_rho_lo = rho_lo;
   h->mac_rho_hi = rho_hi;
   return TREE_GPU_OK;

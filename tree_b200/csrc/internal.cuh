@@ -8,8 +8,10 @@ namespace tg {
 
 constexpr double kEps = 0.0014399835661145824;  // data.f90:40 (eV*um)
 constexpr int kRdfBins = 10001;                  // Ndist+1 (data.f90:38)
-constexpr int kMaxLevel = 21;                    // 3 bits per level in 63 bits
-constexpr uint64_t kSpeciesBit = 1ull << 63;
+constexpr int kMaxLevel = 42;                    // 3 bits per level in 126 bits
+
+// Particle path keys: 42 levels of 3 bits in an unsigned 128-bit integer.
+typedef unsigned __int128 key128;
 
 // error flag bits (device word, read by the host after a call)
 enum : int32_t {

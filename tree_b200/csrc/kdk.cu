@@ -160,4 +160,35 @@ void epot_sum(const double2* ep, int n, double* partial, double* out4,
   k_sum_partials4<<<1, kKdkThreads, 0, st>>>(partial, g, out4);
 }
 
+__global__ void k_sample_append(const double* __restrict__ diag, double* series,
+                                int32_t* count, int cap) {
+  if (threadIdx.x != 0) return;
+  const int k = *count;
+  if (k >= cap) return;
+  double* r = series + 6 * (int64_t)k;
+  r[0] = diag[0];  // Epot_e
+  r[1] = diag[1];  // Epot_i
+  r[2] = diag[4];  // mv2_el
+  r[3] = diag[6];  // mv2_ion
+  r[4] = diag[5];  // rad_el
+  r[5] = diag[7];  // rad_ion
+  *count = k + 1;
+}
+
+__global__ void k_rdf_fold(const uint32_t* __restrict__ bins32,
+                           unsigned long long* acc64, int nbins) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nbins) acc64[i] += bins32[i];
+}
+
+void sample_append(const double* diag, double* series, int32_t* count, int cap,
+                   cudaStream_t st) {
+  k_sample_append<<<1, 32, 0, st>>>(diag, series, count, cap);
+}
+
+void rdf_fold(const uint32_t* bins32, unsigned long long* acc64, cudaStream_t st) {
+  const int nb = 2 * kRdfBins;
+  k_rdf_fold<<<(nb + 255) / 256, 256, 0, st>>>(bins32, acc64, nb);
+}
+
 }  // namespace tg

@@ -1,5 +1,6 @@
 // kdk.h -- integrator and diagnostic reductions.
 #pragma once
+#include <cstdint>
 #include <cuda_runtime.h>
 
 namespace tg {
@@ -16,5 +17,11 @@ void kick2(double* x, double* v, const double* f, int n, int n_el, double dt,
 // out4 = (Epot_e, Epot_i, 0, 0)
 void epot_sum(const double2* ep, int n, double* partial, double* out4,
               cudaStream_t st);
+// Appends (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion) from diag[8]
+// to series[*count] while *count < cap (one record per sample step).
+void sample_append(const double* diag, double* series, int32_t* count, int cap,
+                   cudaStream_t st);
+// acc64[i] += bins32[i] for 2 * kRdfBins bins (running RDF sums of a run).
+void rdf_fold(const uint32_t* bins32, unsigned long long* acc64, cudaStream_t st);
 
 }  // namespace tg

@@ -21,7 +21,7 @@
 namespace tg {
 
 constexpr int kSmpWarps = 4;
-constexpr int kSmpStack = 4096;
+constexpr int kSmpStack = 8192;
 
 __device__ __forceinline__ float hash_unit(uint32_t a, uint32_t b) {
   uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u);

@@ -32,7 +32,7 @@ namespace tg {
 
 constexpr int kMxWarps = 8;
 constexpr int kMxThreads = 32 * kMxWarps;
-constexpr int kStackCap = 4096;   // node indices per warp
+constexpr int kStackCap = 8192;   // node indices per warp
 constexpr int kM2pRing = 64;      // power of two, > 31 + 32
 constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
 constexpr int kMaxBucket = 8;
@@ -755,12 +755,18 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   int grid = (mb.grid_warps / (kMaxBlocksPerSm * kMxWarps)) * bps;
   const bool r = rdf != nullptr;
   const size_t s0 = walk_smem_bytes<false>(), s1 = walk_smem_bytes<true>();
+  int dev = 0;
+  cudaGetDevice(&dev);
 #define TG_LAUNCH(P, R, LL, O)                                                \
   do {                                                                        \
     auto kfn = k_walk_mixed<P, R, LL, O>;                                     \
     const size_t sb = LL ? s1 : s0;                                           \
-    cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                         (int)sb);                                            \
+    static unsigned attr_set = 0; /* devices with the smem limit raised */    \
+    if (dev < 32 && !(attr_set & (1u << dev))) {                              \
+      cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                           (int)sb);                                          \
+      attr_set |= 1u << dev;                                                  \
+    }                                                                         \
     kfn<<<grid, kMxThreads, sb, st>>>(a);                                     \
   } while (0)
 #define TG_LAUNCH_O(P, R, LL)                                                 \
