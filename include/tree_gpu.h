@@ -67,7 +67,8 @@ typedef struct tree_gpu_params {
   int32_t physics;   /* TREE_GPU_PHYS_* */
   int32_t precision; /* TREE_GPU_PREC_* */
   int32_t mac;       /* TREE_GPU_MAC_* */
-  int32_t group;     /* targets per group in the mixed walk (0 = default 32) */
+  int32_t group;     /* reserved, 0 (target groups of the mixed walk are
+                        maximal cells of at most 32 particles) */
 } tree_gpu_params;
 
 typedef struct tree_gpu_diag {
@@ -231,7 +232,7 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
  * particles (1..8) are summed particle by particle instead of being opened;
  * `blocks_per_sm` (1..4) sets the persistent grid; `order` (2 or 3) is the
  * far-field expansion order (quadrupole, or octupole as well; default 3).
- * No counterpart in the reference; set by the autotuner (tree_b200/tune.py). */
+ * No counterpart in the reference; chosen by the autotuner (tree_b200/tune.py). */
 int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
                         int32_t blocks_per_sm, int32_t order);
 

@@ -62,3 +62,11 @@ def test_null_handle_calls_are_errors(device_lib):
     assert device_lib.tree_gpu_step(None, 0.1, 1, None) == -1
     assert device_lib.tree_gpu_destroy(None) == 0
     assert b"null" in device_lib.tree_gpu_last_error(None)
+
+
+def test_fortran_module_declares_every_function():
+    """include/tree_gpu_mod.f90 has a BIND(C) interface for each function of
+    the header (the module cannot be compiled here: no Fortran compiler)."""
+    mod = open(os.path.join(ROOT, "include", "tree_gpu_mod.f90")).read()
+    declared = set(re.findall(r"FUNCTION\s+(tree_gpu_\w+)\s*\(", mod))
+    assert set(declared_functions()) == declared

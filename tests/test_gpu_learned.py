@@ -145,3 +145,24 @@ def test_collect_and_train_on_gpu(device_lib):
                                  precision=api.PREC_MIXED, mac=api.MAC_LEARNED))
         tf.step(DT, 1)
         assert tf.timings().n_mac_net > 0
+
+
+def test_autotuner_meets_the_accuracy_target(device_lib):
+    """The tuner's choice meets the target on the audit and is the fastest
+    candidate that does; the handle is left configured with it."""
+    from tree_b200.tune import Candidate, autotune
+    st = _evolved_state(65536, 14)
+    params, stats, _ = learned_mac.load_model()
+    space = [Candidate(t, e) for t in (0.3, 0.45, 0.7) for e in (0.0, 3e-5)]
+    cfg = api.Config(theta=0.5, physics=api.PHYS_KELBG, precision=api.PREC_MIXED)
+    with api.TreeForce(len(st["x_el"]), len(st["x_ion"]), cfg) as tf:
+        tf.load_state(st["x_el"], st["v_el"], st["f_el"], st["x_ion"], st["v_ion"],
+                      st["f_ion"])
+        best, trials = autotune(tf, DT, space=space, target=2e-4, audit=4096,
+                                model=(params, stats))
+        assert len(trials) == len(space)
+        assert best is not None and best.rms <= 0.9 * 2e-4
+        assert all(t.ms >= best.ms for t in trials if t.rms <= 0.9 * 2e-4)
+        assert tf.config.theta == best.cand.theta
+        tf.step(DT, 1)
+        assert (tf.timings().n_mac_net > 0) == (best.cand.eta > 0)

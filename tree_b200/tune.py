@@ -1,0 +1,147 @@
+"""Accuracy-constrained autotuner of the mixed-precision walk.
+
+    python -m tree_b200.tune [--n 1048576] [--target 1e-4]
+
+Picks, on the caller's own state, the fastest combination of opening angle,
+learned-MAC budget eta, bucket size, expansion order and persistent-grid size
+whose rms relative force error against the FP64 direct sum stays below a
+target.  Every candidate is timed on the same step from the same state:
+
+  1. the state is saved (tree_gpu_get_state);
+  2. for each candidate: load the state, one step (kick-drift, Force, kick),
+     load again and time a second step (its build + walk, CUDA events inside
+     the library), audit the forces of that step on seeded targets against
+     the FP64 direct sum at the same positions (computed once: every
+     candidate steps from the same state with the same first half kick, so the
+     positions of the force evaluation are identical);
+  3. the fastest candidate with rms <= margin * target is applied and the
+     state restored.
+
+The reference has no tunables of this kind (its only knob is sd_ratio,
+tree.f90:743); the tuner replaces hand-picking the headline configuration.
+"""
+import argparse
+import dataclasses
+import itertools
+import json
+
+import numpy as np
+
+from . import api
+
+
+@dataclasses.dataclass(frozen=True)
+class Candidate:
+    theta: float
+    eta: float          # 0: fixed-theta test only
+    bucket: int = 8
+    order: int = 3
+    blocks_per_sm: int = 4
+
+
+@dataclasses.dataclass
+class Trial:
+    cand: Candidate
+    ms: float           # build + walk of one step
+    rms: float
+    n_m2p: int = 0
+    n_p2p: int = 0
+
+
+def default_space(learned=True):
+    thetas = (0.26, 0.28, 0.30, 0.32, 0.35)
+    etas = (0.0, 1e-5, 3e-5, 1e-4) if learned else (0.0,)
+    return [Candidate(t, e, b, 3, g) for t, e, b, g in
+            itertools.product(thetas, etas, (6, 8), (3, 4))]
+
+
+def select(trials, target, margin=0.9):
+    """The fastest trial whose rms is at most margin * target (ties: lower
+    rms); None when no trial meets it."""
+    ok = [t for t in trials if np.isfinite(t.rms) and t.rms <= margin * target]
+    if not ok:
+        return None
+    return min(ok, key=lambda t: (t.ms, t.rms))
+
+
+def _apply(tf, cand, physics, te, model):
+    mac = api.MAC_LEARNED if cand.eta > 0 else api.MAC_FIXED
+    tf.set_config(api.Config(theta=cand.theta, te=te, physics=physics,
+                             precision=api.PREC_MIXED, mac=mac))
+    tf.set_tuning(cand.bucket, cand.blocks_per_sm, cand.order)
+    if mac == api.MAC_LEARNED:
+        if model is None:
+            raise ValueError("a learned candidate needs a model (params, stats)")
+        tf.mac_set_model(*model)
+        tf.mac_config(cand.eta, 0.05, 0.9)
+
+
+def autotune(tf, dt, space=None, target=1e-4, margin=0.9, audit=4096, seed=0,
+             physics=api.PHYS_KELBG, te=50.0, model=None, verbose=False):
+    """Times every candidate of `space` on tf's current state and applies the
+    fastest one that meets the accuracy target.  Returns (best Trial or None,
+    all trials).  tf's state is restored before returning."""
+    space = list(space or default_space(model is not None))
+    snap = tf.get_state()
+    n = tf.n_el + tf.n_ion
+    idx = np.sort(np.random.default_rng(seed).choice(n, min(audit, n), replace=False))
+
+    def load():
+        tf.load_state(snap["x_el"], snap["v_el"], snap["f_el"], snap["x_ion"],
+                      snap["v_ion"], snap["f_ion"])
+
+    fd = None
+    trials = []
+    for cand in space:
+        if cand.eta > 0 and model is None:
+            continue
+        _apply(tf, cand, physics, te, model)
+        load()
+        tf.step(dt, 1)  # graph capture and warm-up of this variant
+        load()
+        t0 = tf.timings()
+        tf.step(dt, 1)
+        t1 = tf.timings()
+        st = tf.get_state()
+        if fd is None:
+            fd, _ = tf.direct(idx)
+        f = np.vstack([st["f_el"], st["f_ion"]])[idx]
+        err = np.linalg.norm(f - fd, axis=1) / np.linalg.norm(fd, axis=1)
+        tr = Trial(cand, (t1.ms_build - t0.ms_build) + (t1.ms_walk - t0.ms_walk),
+                   float(np.sqrt(np.mean(err ** 2))), t1.n_m2p, t1.n_p2p)
+        trials.append(tr)
+        if verbose:
+            print(json.dumps({**dataclasses.asdict(cand), "ms": tr.ms, "rms": tr.rms}),
+                  flush=True)
+    best = select(trials, target, margin)
+    load()
+    if best is not None:
+        _apply(tf, best.cand, physics, te, model)
+    return best, trials
+
+
+def main():
+    from . import cloud, learned_mac, units
+    ap = argparse.ArgumentParser(description="autotune the mixed walk on a seeded cloud")
+    ap.add_argument("--n", type=int, default=1048576)
+    ap.add_argument("--te", type=float, default=50.0)
+    ap.add_argument("--warm", type=int, default=3, help="steps before tuning")
+    ap.add_argument("--target", type=float, default=1e-4)
+    ap.add_argument("--seed", type=int, default=2024)
+    args = ap.parse_args()
+    dt = units.dt_code(1e-11)
+    c = cloud.make_cloud(args.n, seed=args.seed, te_k=args.te)
+    params, stats, _ = learned_mac.load_model()
+    cfg = api.Config(theta=0.35, te=args.te, precision=api.PREC_MIXED)
+    with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
+        tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
+        tf.step(dt, args.warm)
+        best, trials = autotune(tf, dt, target=args.target, te=args.te,
+                                model=(params, stats), verbose=True)
+    print(json.dumps({"best": dataclasses.asdict(best.cand) if best else None,
+                      "ms": best.ms if best else None, "rms": best.rms if best else None,
+                      "trials": len(trials)}))
+
+
+if __name__ == "__main__":
+    main()
