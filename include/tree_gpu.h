@@ -292,6 +292,38 @@ int tree_gpu_destroy(tree_gpu_handle* h);
 /* Library build identifier (sm_100a + git describe at build time). */
 const char* tree_gpu_version(void);
 
+/* ---- ensembles of independent clouds (no counterpart in the reference,
+ * which runs one cloud per job).  ncloud clouds (1..256) of uneven size share
+ * one handle: one build (a forest, each cloud with its own root box), one
+ * persistent walk launch and one integrator launch per step, replayed as a
+ * CUDA graph.  Particles are cloud-major: cloud c holds n_el[c] electrons
+ * then n_ion[c] ions; x, v, f are AoS double xyz over all particles.  Each
+ * cloud keeps its own te, rs and RDF bin widths; theta, physics, mac and the
+ * masses must agree across clouds; precision must be MIXED.  tree_gpu_step,
+ * tree_gpu_run (without RDF), tree_gpu_set_tuning, tree_gpu_set_params
+ * (theta and mac only), tree_gpu_mac_set_model / _config and
+ * tree_gpu_timings work on ensemble handles; the species-split calls
+ * (force, set/load/get_state, direct, tree_dump, mac_collect) return
+ * TREE_GPU_ERR_ARG. */
+int tree_gpu_ensemble_create(const tree_gpu_params* params, int32_t ncloud,
+                             const int64_t* n_el, const int64_t* n_ion,
+                             tree_gpu_handle** out);
+/* Positions and velocities in, initial forces computed (Vinit). */
+int tree_gpu_ensemble_set_state(tree_gpu_handle* h, const double* x,
+                                const double* v);
+/* Full state in (f NULL: forces computed as by set_state). */
+int tree_gpu_ensemble_load_state(tree_gpu_handle* h, const double* x,
+                                 const double* v, const double* f);
+int tree_gpu_ensemble_get_state(tree_gpu_handle* h, double* x, double* v,
+                                double* f);
+/* Per-cloud (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion) of the
+ * current state, 6 x ncloud doubles (TEMPORAL per cloud). */
+int tree_gpu_ensemble_sums(tree_gpu_handle* h, double* out);
+/* FP64 direct sum inside one cloud; targets are cloud-local indices. */
+int tree_gpu_ensemble_direct(tree_gpu_handle* h, int32_t cloud,
+                             const int64_t* targets, int64_t nt, double* f,
+                             double* epot);
+
 #ifdef __cplusplus
 }
 #endif

@@ -252,5 +252,48 @@ MODULE TREE_GPU_MOD
      TYPE(C_PTR) FUNCTION tree_gpu_version() BIND(C)
        IMPORT :: C_PTR
      END FUNCTION
+
+     ! ensembles of independent clouds; particles cloud-major
+     INTEGER(C_INT) FUNCTION tree_gpu_ensemble_create(p, ncloud, n_el, n_ion, h) BIND(C)
+       IMPORT :: C_INT, C_INT32_T, C_INT64_T, C_PTR, tree_gpu_params
+       TYPE(tree_gpu_params), INTENT(IN) :: p(*)
+       INTEGER(C_INT32_T), VALUE :: ncloud
+       INTEGER(C_INT64_T), INTENT(IN) :: n_el(*), n_ion(*)
+       TYPE(C_PTR), INTENT(OUT) :: h
+     END FUNCTION
+
+     INTEGER(C_INT) FUNCTION tree_gpu_ensemble_set_state(h, x, v) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_DOUBLE
+       TYPE(C_PTR), VALUE :: h
+       REAL(C_DOUBLE), INTENT(IN) :: x(*), v(*)
+     END FUNCTION
+
+     INTEGER(C_INT) FUNCTION tree_gpu_ensemble_load_state(h, x, v, f) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_DOUBLE
+       TYPE(C_PTR), VALUE :: h
+       REAL(C_DOUBLE), INTENT(IN) :: x(*), v(*)
+       TYPE(C_PTR), VALUE :: f   ! C_LOC(forces) or C_NULL_PTR
+     END FUNCTION
+
+     INTEGER(C_INT) FUNCTION tree_gpu_ensemble_get_state(h, x, v, f) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_DOUBLE
+       TYPE(C_PTR), VALUE :: h
+       REAL(C_DOUBLE), INTENT(OUT) :: x(*), v(*), f(*)
+     END FUNCTION
+
+     INTEGER(C_INT) FUNCTION tree_gpu_ensemble_sums(h, sums) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_DOUBLE
+       TYPE(C_PTR), VALUE :: h
+       REAL(C_DOUBLE), INTENT(OUT) :: sums(6, *)
+     END FUNCTION
+
+     INTEGER(C_INT) FUNCTION tree_gpu_ensemble_direct(h, cloud, targets, nt, f, epot) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_DOUBLE, C_INT32_T, C_INT64_T
+       TYPE(C_PTR), VALUE :: h
+       INTEGER(C_INT32_T), VALUE :: cloud
+       INTEGER(C_INT64_T), INTENT(IN) :: targets(*)
+       INTEGER(C_INT64_T), VALUE :: nt
+       REAL(C_DOUBLE), INTENT(OUT) :: f(*), epot(*)
+     END FUNCTION
   END INTERFACE
 END MODULE TREE_GPU_MOD

@@ -37,7 +37,10 @@ EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
            "tree_gpu_mac_train", "tree_gpu_mac_set_model",
            "tree_gpu_mac_get_model", "tree_gpu_mac_config", "tree_gpu_mlp_grad",
            "tree_gpu_mlp_infer", "tree_gpu_timings", "tree_gpu_last_error",
-           "tree_gpu_destroy", "tree_gpu_version")
+           "tree_gpu_destroy", "tree_gpu_version", "tree_gpu_ensemble_create",
+           "tree_gpu_ensemble_set_state", "tree_gpu_ensemble_load_state",
+           "tree_gpu_ensemble_get_state", "tree_gpu_ensemble_sums",
+           "tree_gpu_ensemble_direct")
 
 
 class Params(ctypes.Structure):
@@ -133,6 +136,13 @@ def load_library(path: str = LIB_PATH):
     L.tree_gpu_last_error.restype = ctypes.c_char_p
     L.tree_gpu_destroy.argtypes = [vp]
     L.tree_gpu_version.restype = ctypes.c_char_p
+    L.tree_gpu_ensemble_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, lp, lp,
+                                           ctypes.POINTER(vp)]
+    L.tree_gpu_ensemble_set_state.argtypes = [vp, dp, dp]
+    L.tree_gpu_ensemble_load_state.argtypes = [vp, dp, dp, dp]
+    L.tree_gpu_ensemble_get_state.argtypes = [vp, dp, dp, dp]
+    L.tree_gpu_ensemble_sums.argtypes = [vp, dp]
+    L.tree_gpu_ensemble_direct.argtypes = [vp, ctypes.c_int32, lp, ctypes.c_int64, dp, dp]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int
     _lib = L
@@ -429,3 +439,71 @@ class TreeForce:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Ensemble(TreeForce):
+    """Independent clouds of uneven size in one handle: one build, one
+    persistent walk launch and one integrator launch per step.  Particles are
+    cloud-major (cloud c: n_el[c] electrons, then n_ion[c] ions); every
+    TreeForce call that does not depend on the species split (step, run
+    without RDF, timings, tuning, learned-MAC model and budget) works."""
+
+    def __init__(self, configs, n_el, n_ion):
+        self.lib = load_library()
+        self.configs = list(configs)
+        self.config = self.configs[0]
+        self.n_el_c = np.asarray(n_el, np.int64)
+        self.n_ion_c = np.asarray(n_ion, np.int64)
+        self.n_el, self.n_ion = int(self.n_el_c.sum()), int(self.n_ion_c.sum())
+        self.ncloud = len(self.configs)
+        self.offsets = np.concatenate([[0], np.cumsum(self.n_el_c + self.n_ion_c)])
+        arr = (Params * self.ncloud)(*[c.to_c() for c in self.configs])
+        self._p = arr[0]
+        h = ctypes.c_void_p()
+        lp = ctypes.POINTER(ctypes.c_int64)
+        rc = self.lib.tree_gpu_ensemble_create(arr, self.ncloud,
+                                               self.n_el_c.ctypes.data_as(lp),
+                                               self.n_ion_c.ctypes.data_as(lp),
+                                               ctypes.byref(h))
+        if rc != OK:
+            raise TreeGpuError(rc, "tree_gpu_ensemble_create failed")
+        self.h = h
+
+    @property
+    def n(self):
+        return self.n_el + self.n_ion
+
+    def set_state(self, x, v):
+        self._check(self.lib.tree_gpu_ensemble_set_state(self.h, _dp(x), _dp(v)))
+
+    def load_state(self, x, v, f=None):
+        self._check(self.lib.tree_gpu_ensemble_load_state(
+            self.h, _dp(x), _dp(v), _dp(f) if f is not None else None))
+
+    def get_state(self):
+        x = np.empty((self.n, 3))
+        v = np.empty_like(x)
+        f = np.empty_like(x)
+        self._check(self.lib.tree_gpu_ensemble_get_state(self.h, _dp(x), _dp(v), _dp(f)))
+        return dict(x=x, v=v, f=f)
+
+    def sums(self):
+        """Per-cloud (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion)."""
+        out = np.zeros((self.ncloud, 6))
+        self._check(self.lib.tree_gpu_ensemble_sums(self.h, _dp(out)))
+        return out
+
+    def direct(self, cloud, targets):
+        """FP64 direct sum inside one cloud at cloud-local target indices."""
+        t = np.ascontiguousarray(targets, np.int64)
+        f = np.zeros((len(t), 3))
+        e = np.zeros(len(t))
+        lp = ctypes.POINTER(ctypes.c_int64)
+        self._check(self.lib.tree_gpu_ensemble_direct(self.h, int(cloud), t.ctypes.data_as(lp),
+                                                      len(t), _dp(f), _dp(e)))
+        return f, e
+
+    def set_config(self, config):
+        self.config = config
+        self._p = config.to_c()
+        self._check(self.lib.tree_gpu_set_params(self.h, ctypes.byref(self._p)))

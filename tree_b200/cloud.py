@@ -61,3 +61,27 @@ def make_cloud(n_total: int, *, seed: int = 1234, te_k: float = 50.0,
     v_ion = _maxwell(rng, half, ti_k, m_i)
     return Cloud(np.ascontiguousarray(x_el), np.ascontiguousarray(v_el),
                  np.ascontiguousarray(x_ion), np.ascontiguousarray(v_ion), sig)
+
+
+def make_ensemble(ncloud: int = 64, *, seed: int = 5, n_range=(8192, 131072),
+                  n0_range=(1e14, 1e16), te_range=(10.0, 200.0), ti_k: float = 1e-3):
+    """Independent clouds: N log-uniform in n_range (even), peak density
+    log-uniform in n0_range, T_e uniform in te_range; each cloud as
+    make_cloud.  Returns (clouds, te per cloud, n0 per cloud)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    lo, hi = np.log(n_range[0]), np.log(n_range[1])
+    ns = (np.exp(rng.uniform(lo, hi, ncloud)) / 2).astype(np.int64) * 2
+    n0 = np.exp(rng.uniform(np.log(n0_range[0]), np.log(n0_range[1]), ncloud))
+    te = rng.uniform(te_range[0], te_range[1], ncloud)
+    clouds = [make_cloud(int(ns[c]), seed=seed * 1000 + c, te_k=float(te[c]), ti_k=ti_k,
+                         n0_per_m3=float(n0[c])) for c in range(ncloud)]
+    return clouds, te, n0
+
+
+def pack_ensemble(clouds):
+    """Cloud-major arrays (x, v) and per-cloud (n_el, n_ion) for Ensemble."""
+    x = np.vstack([np.vstack([c.x_el, c.x_ion]) for c in clouds])
+    v = np.vstack([np.vstack([c.v_el, c.v_ion]) for c in clouds])
+    n_el = np.array([len(c.x_el) for c in clouds], np.int64)
+    n_ion = np.array([len(c.x_ion) for c in clouds], np.int64)
+    return np.ascontiguousarray(x), np.ascontiguousarray(v), n_el, n_ion

@@ -113,6 +113,85 @@ __global__ void k_geom(const uint64_t* bb, int n, int n_el, Geom* g) {
   g[s] = G;
 }
 
+// Largest c with start[c] <= i (start[0] = 0, nseg entries searched).
+__device__ __forceinline__ int seg_of(const int32_t* __restrict__ start, int nseg,
+                                      int i) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&start[mid]) <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Per-cloud bounding boxes: one block per cloud, bb[(c*3+k)*2 + 0/1] = ord
+// of the min / max along axis k.
+__global__ void k_bbox_seg(const double* __restrict__ x,
+                           const int32_t* __restrict__ start, uint64_t* bb,
+                           int32_t* err) {
+  __shared__ uint64_t smin[3][256 / 32], smax[3][256 / 32];
+  const int c = blockIdx.x;
+  const int i0 = start[c], i1 = start[c + 1];
+  uint64_t mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0ull, 0ull, 0ull};
+  bool bad = false;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double v = x[3 * (int64_t)i + k];
+      if (!isfinite(v)) bad = true;
+      const uint64_t o = ord_from_double(v);
+      mn[k] = o < mn[k] ? o : mn[k];
+      mx[k] = o > mx[k] ? o : mx[k];
+    }
+  if (bad) set_error(err, kErrNonFinite);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const uint64_t a = shfl_min_u64(mn[k]), b = shfl_max_u64(mx[k]);
+    if (lane == 0) {
+      smin[k][w] = a;
+      smax[k][w] = b;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int k = threadIdx.x;
+    uint64_t a = ~0ull, b = 0ull;
+    for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) {
+      a = smin[k][ww] < a ? smin[k][ww] : a;
+      b = smax[k][ww] > b ? smax[k][ww] : b;
+    }
+    bb[(c * 3 + k) * 2] = a;
+    bb[(c * 3 + k) * 2 + 1] = b;
+  }
+}
+
+// Root box per cloud, as k_geom does per species.
+__global__ void k_geom_seg(const uint64_t* bb, const int32_t* __restrict__ start,
+                           int nseg, Geom* g) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nseg) return;
+  Geom G;
+  G.first = start[c];
+  G.n = start[c + 1] - start[c];
+  double smax = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    if (G.n > 0) {
+      const double lo = double_from_ord(bb[(c * 3 + k) * 2]);
+      const double hi = double_from_ord(bb[(c * 3 + k) * 2 + 1]);
+      G.c0[k] = (hi + lo) / 2.0;
+      G.lx0[k] = hi - lo;
+    } else {
+      G.c0[k] = 0.0;
+      G.lx0[k] = 0.0;
+    }
+    if (k == 0 || G.lx0[k] > smax) smax = G.lx0[k];
+  }
+  G.smax0 = smax;
+  g[c] = G;
+}
+
 // ---------------------------------------------------------------- keys ----
 // Replays Insert_Tree's descent (tree.f90:132-173 comparisons, 123-126 child
 // centres) for 42 levels.  The reference recursion has no depth limit; 42
@@ -125,13 +204,26 @@ __global__ void k_geom(const uint64_t* bb, int n, int n_el, Geom* g) {
 //     bit 0 = species, a 43rd one-bit level that separates an electron
 //     sitting exactly on an ion (the t = 0 state of the clouds).
 // In both, the digit of level l is (key >> (127 - 3l + lsb)) & 7.
+// An ensemble of clouds (combined layout) puts the cloud id in the top `top`
+// bits and keeps nlev = (126 - top) / 3 spatial levels right below it (any
+// spare bits sit between level nlev and the species bit); the digit of level
+// l is then (key >> (128 - top - 3l)) & 7, which is the general form
+// (top = 1 - lsb for the single-cloud layouts).
 __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
                        int lsb, int n_el_charge, const Geom* __restrict__ geom,
-                       key128* keys, uint32_t* vals) {
+                       Ensemble ens, key128* keys, uint32_t* vals) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int s = i >= n_el;
-  const Geom& G = geom[s];
+  int seg = s, top = 1 - lsb, nlev = kMaxLevel;
+  bool ion = i >= n_el_charge;
+  if (ens.nseg > 0) {
+    seg = seg_of(ens.start, ens.nseg, i);
+    ion = i >= __ldg(&ens.elec_end[seg]);
+    top = ens.top;
+    nlev = ens.nlev;
+  }
+  const Geom& G = geom[seg];
   double p[3], c[3], lx[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -140,7 +232,7 @@ __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
     lx[k] = G.lx0[k];
   }
   key128 key = 0;
-  for (int l = 0; l < kMaxLevel; ++l) {
+  for (int l = 0; l < nlev; ++l) {
     uint32_t b = 0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -151,8 +243,11 @@ __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
     }
     key = (key << 3) | (key128)b;
   }
-  if (lsb) key = (key << 2) | (key128)(i >= n_el_charge ? 1u : 0u);
-  else key = (key << 1) | ((key128)(s ? 1u : 0u) << 127);
+  // level 1 right below the top bits; the bits under level nlev are zero
+  // except, in the combined layout, the species in bit 0
+  key <<= (128 - top - 3 * nlev);
+  if (lsb) key |= (key128)(ion ? 1u : 0u);
+  if (top > 0) key |= (key128)(uint32_t)seg << (128 - top);
   keys[i] = key;
   vals[i] = (uint32_t)i;
 }
@@ -389,25 +484,25 @@ __device__ __forceinline__ int clz128(key128 x) {
 }
 
 // L[p] = number of leading levels that sorted keys p and p+1 share (same
-// species), else -1.  Identical keys mean the 42-level cap was hit.
+// species tree / same cloud: equal `top` bits), else -1.  Identical keys mean
+// the level cap was hit.
 __global__ void k_common_levels(const key128* __restrict__ keys, int n,
-                                int lsb, int8_t* L, int32_t* err) {
+                                int top, int nlev, int8_t* L, int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int8_t r = -1;
   if (p + 1 < n) {
     key128 a = keys[p], b = keys[p + 1];
     key128 x = a ^ b;
-    if (lsb || (x >> 127) == 0) {
+    if (top == 0 || (x >> (128 - top)) == 0) {
       if (x == 0) {
         set_error(err, kErrDepth);
-        r = kMaxLevel;
+        r = (int8_t)nlev;
       } else {
-        int lz = clz128(x);
-        // lsb = 0: lz >= 1 (species bit equal); lsb = 1: lz = 127 means only
-        // the species bit differs, i.e. all 42 spatial levels are shared
-        int lev = lsb ? lz / 3 : (lz - 1) / 3;
-        r = (int8_t)(lev < kMaxLevel ? lev : kMaxLevel);
+        // lz >= top (same tree); for the combined layouts lz = 127 means only
+        // the species bit differs, i.e. all nlev spatial levels are shared
+        int lev = (clz128(x) - top) / 3;
+        r = (int8_t)(lev < nlev ? lev : nlev);
       }
     }
   }
@@ -452,10 +547,10 @@ __device__ __forceinline__ int lower_prefix(const key128* __restrict__ keys,
   return lo_i;
 }
 
-// Shift that leaves the first d levels of a key (1 <= d <= 42); level 43 of
-// the combined layout is the whole key.
-__device__ __forceinline__ int shift_for_level(int d, int lsb) {
-  int s = 127 - 3 * d + lsb;
+// Shift that leaves the first d levels of a key (with the top bits; 1 <= d <=
+// nlev); level nlev + 1 of the combined layout is the whole key.
+__device__ __forceinline__ int shift_for_level(int d, int top) {
+  int s = 128 - top - 3 * d;
   return s > 0 ? s : 0;
 }
 
@@ -463,8 +558,8 @@ __device__ __forceinline__ int shift_for_level(int d, int lsb) {
 // was opened at an earlier particle (first particle of the level-d prefix).
 __device__ __forceinline__ int twig_index_before(
     const key128* __restrict__ keys, const int8_t* __restrict__ L,
-    const int32_t* __restrict__ off, int sb, int p, int d, int lsb) {
-  int sh = shift_for_level(d, lsb);
+    const int32_t* __restrict__ off, int sb, int p, int d, int top) {
+  int sh = shift_for_level(d, top);
   key128 pre = keys[p] >> sh;
   int q = lower_prefix(keys, sb, p + 1, sh, pre);
   int lo_q = q == 0 ? -1 : (int)L[q - 1];
@@ -481,13 +576,22 @@ __global__ void k_topology(const key128* __restrict__ keys,
                            double4* node_c, int32_t* node_skip,
                            int32_t* node_pt, int32_t* node_parent,
                            int32_t* node_nchild, int32_t* node_done,
-                           int8_t* node_level, MixedNodes mx, int32_t* err) {
+                           int8_t* node_level, MixedNodes mx, Ensemble ens,
+                           int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int lo, hi;
   lo_hi(L, p, lo, hi);
   int s = p >= n_el;
   int sb = s ? n_el : 0, se = s ? n : n_el;
+  int top = 1 - lsb, nlev = kMaxLevel;
+  if (ens.nseg > 0) {  // sorted order keeps every cloud's index range
+    s = seg_of(ens.start, ens.nseg, p);
+    sb = ens.start[s];
+    se = ens.start[s + 1];
+    top = ens.top;
+    nlev = ens.nlev;
+  }
   int tree_end = off[se];
   int base = off[p];
   key128 key = keys[p];
@@ -516,7 +620,7 @@ __global__ void k_topology(const key128* __restrict__ keys,
         sk = tree_end;
         q_end = se;
       } else {
-        int sh = shift_for_level(d, lsb);
+        int sh = shift_for_level(d, top);
         int q = upper_prefix(keys, p + 1, se, sh, key >> sh);
         sk = q < se ? off[q] : tree_end;
         q_end = q;
@@ -525,19 +629,19 @@ __global__ void k_topology(const key128* __restrict__ keys,
       // particle range and child table used by the mixed-precision walk
       mx.first[idx] = p;
       mx.count[idx] = q_end - p;
-      mx.digit[idx] = d == 0 ? (int8_t)0 : (int8_t)((key >> (127 - 3 * d + lsb)) & 7);
+      mx.digit[idx] = d == 0 ? (int8_t)0 : (int8_t)((key >> (128 - top - 3 * d)) & 7);
       int4* kk = reinterpret_cast<int4*>(mx.kids + 8 * (int64_t)idx);
       kk[0] = make_int4(-1, -1, -1, -1);
       kk[1] = make_int4(-1, -1, -1, -1);
       int par;
       if (d == 0) par = -1;
       else if (d > lo + 1) par = idx - 1;
-      else par = twig_index_before(keys, L, off, sb, p, d - 1, lsb);
+      else par = twig_index_before(keys, L, off, sb, p, d - 1, top);
       node_parent[idx] = par;
     }
     // descend one level along this particle's digits
-    if (d < kMaxLevel) {
-      int dig = (int)((key >> (124 - 3 * d + lsb)) & 7);
+    if (d < nlev) {
+      int dig = (int)((key >> (125 - top - 3 * d)) & 7);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         bool bit = (dig >> k) & 1;
@@ -560,10 +664,10 @@ __global__ void k_topology(const key128* __restrict__ keys,
   node_nchild[leaf] = 0;
   mx.first[leaf] = p;
   mx.count[leaf] = 1;
-  mx.digit[leaf] = depth <= kMaxLevel ? (int8_t)((key >> (127 - 3 * depth + lsb)) & 7)
-                                      : (int8_t)(lsb ? (int)(key & 1) : 0);
+  mx.digit[leaf] = depth <= nlev ? (int8_t)((key >> (128 - top - 3 * depth)) & 7)
+                                 : (int8_t)(lsb ? (int)(key & 1) : 0);
   node_parent[leaf] = ntw > 0 ? leaf - 1
-                              : twig_index_before(keys, L, off, sb, p, depth - 1, lsb);
+                              : twig_index_before(keys, L, off, sb, p, depth - 1, top);
 }
 
 // Counts children per twig (separate launch so the zeroing in k_topology is
@@ -579,6 +683,14 @@ __global__ void k_link_children(const int32_t* __restrict__ node_parent,
     atomicAdd(&node_nchild[par], 1);
     mx.kids[8 * (int64_t)par + mx.digit[i]] = i;  // siblings have distinct digits
   }
+}
+
+// Root node of every cloud: the first node its first sorted particle emits.
+__global__ void k_roots(const int32_t* __restrict__ off,
+                        const int32_t* __restrict__ start, int nseg,
+                        int32_t* roots) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nseg) roots[c] = off[start[c]];
 }
 
 __global__ void k_bounds(const int32_t* __restrict__ off, int n, int n_el,
@@ -740,7 +852,7 @@ __global__ void k_upward_net(const double* __restrict__ x,
                              const int32_t* __restrict__ node_nchild,
                              int32_t* node_done,
                              const int8_t* __restrict__ node_level,
-                             MixedNodes mx, int32_t* err) {
+                             MixedNodes mx, Ensemble ens, int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   if (*((volatile int32_t*)err) & kErrCapacity) return;
@@ -750,7 +862,9 @@ __global__ void k_upward_net(const double* __restrict__ x,
   int leaf = off[p] + ntw;
   if (leaf >= cap) return;
   uint32_t o = vals[p];
-  const bool ion = (int)o >= n_el_charge;
+  // sorting keeps each cloud's index range, so p and o share the cloud
+  const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, p) : 0;
+  const bool ion = (int)o >= (ens.nseg > 0 ? __ldg(&ens.elec_end[seg]) : n_el_charge);
   const double q = ion ? 1.0 : -1.0;
   const double px = x[3 * (int64_t)o], py = x[3 * (int64_t)o + 1],
                pz = x[3 * (int64_t)o + 2];
@@ -774,7 +888,7 @@ __global__ void k_upward_net(const double* __restrict__ x,
     mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
   }
   __threadfence();
-  const double smax0 = geom[0].smax0;
+  const double smax0 = geom[seg].smax0;
   int cur = node_parent[leaf];
   int guard = 0;
   while (cur >= 0) {
@@ -910,14 +1024,15 @@ __global__ void k_upward_net(const double* __restrict__ x,
 // bounding box stays compact.  Group order is not deterministic (atomic
 // append); the content of every group is.
 __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
-                         MixedNodes mx, int2* groups, int32_t* n_groups) {
+                         const int32_t* __restrict__ node_parent, MixedNodes mx,
+                         int2* groups, int32_t* n_groups) {
   int m = bounds[2] < cap ? bounds[2] : cap;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= m) return;
   const int cnt = mx.count[t];
-  if (t == 0 && cnt <= kGroupMax) {  // whole tree fits one group
+  if (node_parent[t] < 0 && cnt <= kGroupMax) {  // a whole tree fits one group
     int g = atomicAdd(n_groups, 1);
-    groups[g] = make_int2(mx.first[0], cnt);
+    groups[g] = make_int2(mx.first[t], cnt);
     return;
   }
   if (cnt <= kGroupMax || cnt == 1) return;
@@ -968,21 +1083,30 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   int launches = 1;
   int gb = (n + T - 1) / T;
   int gbb = gb < 4 * 148 ? gb : 4 * 148;
-  k_bbox<<<gbb, T, 0, st>>>(x, n, split, b.bbox, b.err);
-  k_geom<<<1, 32, 0, st>>>(b.bbox, n, split, b.geom);
+  // an ensemble of clouds only exists on the mixed path
+  const Ensemble ens = mode == 1 ? b.ens : Ensemble();
+  if (ens.nseg > 0) {
+    k_bbox_seg<<<ens.nseg, T, 0, st>>>(x, ens.start, b.bbox, b.err);
+    k_geom_seg<<<(ens.nseg + 31) / 32, 32, 0, st>>>(b.bbox, ens.start, ens.nseg, b.geom);
+  } else {
+    k_bbox<<<gbb, T, 0, st>>>(x, n, split, b.bbox, b.err);
+    k_geom<<<1, 32, 0, st>>>(b.bbox, n, split, b.geom);
+  }
   const int lsb = mode == 0 ? 0 : 1;
-  k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, b.keys, b.vals);
+  const int top = ens.nseg > 0 ? ens.top : 1 - lsb;
+  const int nlev = ens.nseg > 0 ? ens.nlev : kMaxLevel;
+  k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, ens, b.keys, b.vals);
   launches += 3;
   launches += radix_sort(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
                          b.sort_hist, b.scan_partial, st);
-  k_common_levels<<<gb, T, 0, st>>>(b.keys, n, lsb, b.L, b.err);
+  k_common_levels<<<gb, T, 0, st>>>(b.keys, n, top, nlev, b.L, b.err);
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);
   k_bounds<<<1, 32, 0, st>>>(b.off, n, split, b.cap, b.bounds, b.err);
   k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, split, lsb, b.geom,
                                b.cap, b.node_c, b.node_skip, b.node_pt,
                                b.node_parent, b.node_nchild, b.node_done,
-                               b.node_level, b.mx, b.err);
+                               b.node_level, b.mx, ens, b.err);
   int gcap = (b.cap + T - 1) / T;
   k_link_children<<<gcap, T, 0, st>>>(b.node_parent, b.bounds, b.cap,
                                       b.node_nchild, b.mx);
@@ -997,10 +1121,16 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   k_upward_net<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.geom, theta,
                                  b.cap, b.node_c, b.node_skip, b.node_parent,
                                  b.node_nchild, b.node_done, b.node_level, b.mx,
-                                 b.err);
+                                 ens, b.err);
   cudaMemsetAsync(b.mx.n_groups, 0, sizeof(int32_t), st);
-  k_groups<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.mx, b.mx.groups, b.mx.n_groups);
-  return launches + 2;
+  k_groups<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_parent, b.mx, b.mx.groups,
+                               b.mx.n_groups);
+  launches += 2;
+  if (ens.nseg > 0) {
+    k_roots<<<(ens.nseg + 31) / 32, 32, 0, st>>>(b.off, ens.start, ens.nseg, ens.roots);
+    launches += 1;
+  }
+  return launches;
 }
 
 }  // namespace tg

@@ -23,6 +23,20 @@ struct MixedNodes {
   int32_t* n_groups; // device count of groups
 };
 
+// Independent clouds in one combined forest (mixed path only).  Cloud c holds
+// particles [start[c], start[c+1]) of the index space, electrons first up to
+// elec_end[c]; its key carries c in the top `top` bits above nlev spatial
+// levels, so one sort groups the clouds and its tree is rooted at node
+// roots[c].  nseg = 0: a single cloud with the classic layout.
+struct Ensemble {
+  int nseg = 0;
+  int top = 0;
+  int nlev = kMaxLevel;
+  const int32_t* start = nullptr;     // device, nseg + 1
+  const int32_t* elec_end = nullptr;  // device, nseg
+  int32_t* roots = nullptr;           // device, nseg
+};
+
 struct BuildBuffers {
   // particle-indexed (n)
   key128* keys;
@@ -45,11 +59,12 @@ struct BuildBuffers {
   int32_t* node_done;
   int8_t* node_level;
   // small
-  uint64_t* bbox;       // 12
-  Geom* geom;           // 2
+  uint64_t* bbox;       // 6 per segment (>= 2 segments)
+  Geom* geom;           // per segment (>= 2)
   int32_t* bounds;      // 4: 0, M_e, M (clamped to cap), M (untruncated)
   int32_t* err;
   MixedNodes mx;
+  Ensemble ens;
 };
 
 int radix_blocks(int n);

@@ -28,6 +28,7 @@ namespace {
 constexpr double kHbar = 1.054571817e-34;  // J s
 constexpr double kAmu = 1.66053906660e-27;  // kg
 constexpr double kKbSi = 1.380649e-23;      // J/K
+constexpr int kMaxClouds = 256;             // cloud id in at most 8 key bits
 
 double kelbg_lambda_um(double mu_amu, double te) {
   return kHbar / std::sqrt(2.0 * mu_amu * kAmu * kKbSi * te) * 1e6;
@@ -98,6 +99,15 @@ struct tree_gpu_handle {
   int32_t* series_count = nullptr;
   int series_cap = 0;
   unsigned long long* rdf64 = nullptr;  // RDF sums of a run (2 x kRdfBins)
+  // ensemble of independent clouds (b.ens.nseg > 0)
+  std::vector<tree_gpu_params> cloud_prm;
+  std::vector<int64_t> cloud_ne, cloud_ni;
+  int32_t* ens_start = nullptr;     // device, nseg + 1
+  int32_t* ens_elec_end = nullptr;  // device, nseg
+  int32_t* ens_roots = nullptr;     // device, nseg
+  float4* cloud_pk = nullptr;       // device, 2 per cloud
+  uint8_t* ion_flag = nullptr;      // device, per particle (ensembles)
+  double* cloud_sums = nullptr;     // device, 6 per cloud
 };
 
 namespace {
@@ -214,7 +224,9 @@ void free_all(tree_gpu_handle* h) {
                   b.node_done, b.node_level, h->rdf, h->counters, h->partial,
                   h->diag, h->mlp_params, h->mlp_stats, h->mlp_packed,
                   h->smp_feats, h->smp_labels, h->smp_extra, h->smp_count,
-                  h->series, h->series_count, h->rdf64};
+                  h->series, h->series_count, h->rdf64, h->ens_start,
+                  h->ens_elec_end, h->ens_roots, h->cloud_pk, h->ion_flag,
+                  h->cloud_sums};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   tg::mixed_free(h->mb);
@@ -291,7 +303,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
       lm.rho_hi = h->mac_rho_hi;
     }
     tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp, h->tune,
-                   use_learned ? &lm : nullptr, h->f, h->epot_part,
+                   use_learned ? &lm : nullptr, h->b.ens, h->cloud_pk, h->f, h->epot_part,
                    with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
   }
   if (ev) record(h, ev->e[2]);
@@ -381,8 +393,8 @@ void enqueue_step_body(tree_gpu_handle* h, double dt, bool sample, bool last,
   const tree_gpu_params& p = h->prm;
   const int n = h->n, ne = (int)h->n_el;
   enqueue_force(h, rdf, ev);
-  tg::kick2(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, sample, !last,
-            h->partial, h->diag + 4, h->st);
+  tg::kick2(h->x, h->v, h->f, n, ne, h->ion_flag, dt, p.xm_el, p.xm_ion, sample,
+            !last, h->partial, h->diag + 4, h->st);
   h->timing.launches += n > 0 ? (sample ? 2 : 1) : 0;
   if (rdf) {
     tg::rdf_fold(h->rdf, h->rdf64, h->st);
@@ -482,7 +494,7 @@ int run_impl(tree_gpu_handle* h, double dt, int32_t nsteps, int32_t nsamp,
       for (StepGraph& g : b2) g.replays = 0;
   std::vector<char> own_ev((size_t)nsteps, 0);  // step s recorded events[1 + s]
   cudaEventRecord(et.e[0], h->st);
-  tg::kick_drift(h->x, h->v, h->f, n, ne, dt, p.xm_el, p.xm_ion, h->st);
+  tg::kick_drift(h->x, h->v, h->f, n, ne, h->ion_flag, dt, p.xm_el, p.xm_ion, h->st);
   h->timing.launches += n > 0 ? 1 : 0;
   for (int s = 0; s < nsteps; ++s) {
     const int64_t nl = h->nloop + s + 1;
@@ -588,6 +600,19 @@ int tree_gpu_set_params(tree_gpu_handle* h, const tree_gpu_params* params) {
   if (!h) return TREE_GPU_ERR_ARG;
   if (check_params(params) != TREE_GPU_OK)
     return fail(h, TREE_GPU_ERR_ARG, "invalid parameters");
+  if (h->b.ens.nseg > 0) {
+    // an ensemble keeps its clouds' physics; theta and the criterion change
+    if (params->precision != TREE_GPU_PREC_MIXED)
+      return fail(h, TREE_GPU_ERR_ARG, "ensembles run the mixed path only");
+    h->prm.theta = params->theta;
+    h->prm.mac = params->mac;
+    for (tree_gpu_params& c : h->cloud_prm) {
+      c.theta = params->theta;
+      c.mac = params->mac;
+    }
+    ++h->epoch;
+    return TREE_GPU_OK;
+  }
   h->prm = *params;
   set_lambdas(h);
   ++h->epoch;
@@ -597,6 +622,8 @@ int tree_gpu_set_params(tree_gpu_handle* h, const tree_gpu_params* params) {
 int tree_gpu_force(tree_gpu_handle* h, const double* x_el, const double* x_ion,
                    double* f_el, double* f_ion, double* epot_e, double* epot_i,
                    int64_t* rdf_ei, int64_t* rdf_ii) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h) return TREE_GPU_ERR_ARG;
   if ((h->n_el && (!x_el || !f_el)) || (h->n_ion && (!x_ion || !f_ion)))
     return fail(h, TREE_GPU_ERR_ARG, "null particle buffer");
@@ -644,6 +671,8 @@ int tree_gpu_force(tree_gpu_handle* h, const double* x_el, const double* x_ion,
 int tree_gpu_set_state(tree_gpu_handle* h, const double* x_el,
                        const double* v_el, const double* x_ion,
                        const double* v_ion) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h) return TREE_GPU_ERR_ARG;
   if ((h->n_el && (!x_el || !v_el)) || (h->n_ion && (!x_ion || !v_ion)))
     return fail(h, TREE_GPU_ERR_ARG, "null particle buffer");
@@ -670,6 +699,8 @@ int tree_gpu_load_state(tree_gpu_handle* h, const double* x_el,
                         const double* v_el, const double* f_el,
                         const double* x_ion, const double* v_ion,
                         const double* f_ion) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h) return TREE_GPU_ERR_ARG;
   if ((h->n_el && (!x_el || !v_el || !f_el)) ||
       (h->n_ion && (!x_ion || !v_ion || !f_ion)))
@@ -728,6 +759,8 @@ int tree_gpu_run(tree_gpu_handle* h, double dt, int32_t nsteps, int32_t nsamp,
   if (n_series) *n_series = 0;
   if (nsteps == 0) return TREE_GPU_OK;
   const bool rdf = rdf_ei || rdf_ii;
+  if (rdf && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "RDF counts are per cloud: not kept for ensembles");
   // sample steps of this call, and room for their records
   int64_t nsamples = 0;
   if (nsamp > 0) nsamples = (h->nloop + nsteps) / nsamp - h->nloop / nsamp;
@@ -796,6 +829,8 @@ int tree_gpu_get_nloop(tree_gpu_handle* h, int64_t* nloop) {
 int tree_gpu_get_state(tree_gpu_handle* h, double* x_el, double* v_el,
                        double* f_el, double* x_ion, double* v_ion,
                        double* f_ion) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h) return TREE_GPU_ERR_ARG;
   const size_t be = 3 * sizeof(double) * (size_t)h->n_el;
   const size_t bi = 3 * sizeof(double) * (size_t)h->n_ion;
@@ -816,6 +851,8 @@ int tree_gpu_get_state(tree_gpu_handle* h, double* x_el, double* v_el,
 
 int tree_gpu_direct(tree_gpu_handle* h, const int64_t* targets, int64_t nt,
                     double* f, double* epot) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h) return TREE_GPU_ERR_ARG;
   if (nt < 0 || nt > 0x7fffffff || (nt && (!targets || !f || !epot)))
     return fail(h, TREE_GPU_ERR_ARG, "bad target list");
@@ -857,6 +894,8 @@ int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
                        double* centre, double* moments, double* rcrit,
                        int32_t* level, int64_t* skip, int64_t* pt,
                        int64_t* n_nodes) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h || (species != 0 && species != 1)) return TREE_GPU_ERR_ARG;
   int32_t bnd[4];
   CK(cudaMemcpy(bnd, h->b.bounds, sizeof(bnd), cudaMemcpyDeviceToHost));
@@ -947,6 +986,199 @@ int tree_gpu_destroy(tree_gpu_handle* h) {
 
 const char* tree_gpu_version(void) { return TREE_GPU_VERSION_STR; }
 
+/* ---- ensembles of independent clouds ---- */
+
+int tree_gpu_ensemble_create(const tree_gpu_params* params, int32_t ncloud,
+                             const int64_t* n_el, const int64_t* n_ion,
+                             tree_gpu_handle** out) {
+  if (!out) return TREE_GPU_ERR_ARG;
+  *out = nullptr;
+  if (!params || !n_el || !n_ion || ncloud < 1 || ncloud > kMaxClouds)
+    return TREE_GPU_ERR_ARG;
+  int64_t total = 0, total_el = 0;
+  for (int c = 0; c < ncloud; ++c) {
+    if (check_params(&params[c]) != TREE_GPU_OK) return TREE_GPU_ERR_ARG;
+    const tree_gpu_params& a = params[c];
+    const tree_gpu_params& p0 = params[0];
+    // one walk, one integrator and one criterion for all clouds
+    if (a.precision != TREE_GPU_PREC_MIXED || a.physics != p0.physics ||
+        a.theta != p0.theta || a.mac != p0.mac || a.xm_el != p0.xm_el ||
+        a.xm_ion != p0.xm_ion)
+      return TREE_GPU_ERR_ARG;
+    if (n_el[c] < 0 || n_ion[c] < 0) return TREE_GPU_ERR_ARG;
+    total += n_el[c] + n_ion[c];
+    total_el += n_el[c];
+  }
+  if (total > (int64_t)0x7fffffff / 4) return TREE_GPU_ERR_ARG;
+  tree_gpu_handle* h = nullptr;
+  int rc = tree_gpu_create(&params[0], total_el, total - total_el, &h);
+  if (rc) return rc;
+  h->cloud_prm.assign(params, params + ncloud);
+  h->cloud_ne.assign(n_el, n_el + ncloud);
+  h->cloud_ni.assign(n_ion, n_ion + ncloud);
+  std::vector<int32_t> start(ncloud + 1), eend(ncloud);
+  std::vector<uint8_t> ion((size_t)std::max<int64_t>(total, 1), 0);
+  std::vector<float4> pk(2 * (size_t)ncloud);
+  int64_t o = 0;
+  for (int c = 0; c < ncloud; ++c) {
+    start[c] = (int32_t)o;
+    eend[c] = (int32_t)(o + n_el[c]);
+    for (int64_t i = o + n_el[c]; i < o + n_el[c] + n_ion[c]; ++i) ion[i] = 1;
+    o += n_el[c] + n_ion[c];
+    const tree_gpu_params& a = params[c];
+    double lam[3] = {1, 1, 1};
+    if (a.te > 0.0 && a.xm_el > 0.0 && a.xm_ion > 0.0) {
+      lam[0] = kelbg_lambda_um(a.xm_el / 2.0, a.te);
+      lam[1] = kelbg_lambda_um(a.xm_el * a.xm_ion / (a.xm_el + a.xm_ion), a.te);
+      lam[2] = kelbg_lambda_um(a.xm_ion / 2.0, a.te);
+    }
+    const float rs_inv = a.rs > 0.0 ? (float)(1.0 / a.rs) : 0.f;
+    pk[2 * c] = make_float4((float)(1.0 / (lam[0] * lam[0])), (float)(1.0 / (lam[1] * lam[1])),
+                            (float)(1.0 / (lam[2] * lam[2])), rs_inv);
+    pk[2 * c + 1] = make_float4((float)(1.0 / lam[0]), (float)(1.0 / lam[1]),
+                                (float)(1.0 / lam[2]), 0.f);
+  }
+  start[ncloud] = (int32_t)o;
+  do {
+    tg::BuildBuffers& b = h->b;
+    if ((rc = dalloc(h, &b.bbox, 6 * (size_t)std::max(2, ncloud)))) break;
+    if ((rc = dalloc(h, &b.geom, (size_t)std::max(2, ncloud)))) break;
+    if ((rc = dalloc(h, &h->ens_start, (size_t)ncloud + 1))) break;
+    if ((rc = dalloc(h, &h->ens_elec_end, (size_t)ncloud))) break;
+    if ((rc = dalloc(h, &h->ens_roots, (size_t)ncloud))) break;
+    if ((rc = dalloc(h, &h->cloud_pk, 2 * (size_t)ncloud))) break;
+    if ((rc = dalloc(h, &h->ion_flag, ion.size()))) break;
+    if ((rc = dalloc(h, &h->cloud_sums, 6 * (size_t)ncloud))) break;
+    cudaMemcpy(h->ens_start, start.data(), start.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->ens_elec_end, eend.data(), eend.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->cloud_pk, pk.data(), pk.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    if (cudaMemcpy(h->ion_flag, ion.data(), ion.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = fail(h, TREE_GPU_ERR_CUDA, "ensemble upload failed");
+      break;
+    }
+    int top = 1;
+    while ((1 << top) < ncloud) ++top;
+    b.ens.nseg = ncloud;
+    b.ens.top = top;
+    b.ens.nlev = (126 - top) / 3;
+    b.ens.start = h->ens_start;
+    b.ens.elec_end = h->ens_elec_end;
+    b.ens.roots = h->ens_roots;
+    ++h->epoch;
+  } while (0);
+  if (rc) {
+    tree_gpu_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_ensemble_load_state(tree_gpu_handle* h, const double* x,
+                                 const double* v, const double* f) {
+  if (!h || h->b.ens.nseg == 0) return TREE_GPU_ERR_ARG;
+  if (h->n && (!x || !v)) return fail(h, TREE_GPU_ERR_ARG, "null particle buffer");
+  const size_t bytes = 3 * sizeof(double) * (size_t)h->n;
+  if (bytes) {
+    CK(cudaMemcpyAsync(h->x, x, bytes, cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->v, v, bytes, cudaMemcpyHostToDevice, h->st));
+    if (f) CK(cudaMemcpyAsync(h->f, f, bytes, cudaMemcpyHostToDevice, h->st));
+  }
+  h->nloop = 0;
+  if (f) {
+    h->has_state = true;
+    h->has_fprev = true;
+    return TREE_GPU_OK;
+  }
+  h->has_fprev = false;  // initial forces with the fixed-theta test
+  int rc = force_device(h, false);
+  if (rc) return rc;
+  h->has_state = true;
+  h->has_fprev = true;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_ensemble_set_state(tree_gpu_handle* h, const double* x, const double* v) {
+  return tree_gpu_ensemble_load_state(h, x, v, nullptr);
+}
+
+int tree_gpu_ensemble_get_state(tree_gpu_handle* h, double* x, double* v, double* f) {
+  if (!h || h->b.ens.nseg == 0) return TREE_GPU_ERR_ARG;
+  const size_t bytes = 3 * sizeof(double) * (size_t)h->n;
+  if (bytes) {
+    if (x) CK(cudaMemcpyAsync(x, h->x, bytes, cudaMemcpyDeviceToHost, h->st));
+    if (v) CK(cudaMemcpyAsync(v, h->v, bytes, cudaMemcpyDeviceToHost, h->st));
+    if (f) CK(cudaMemcpyAsync(f, h->f, bytes, cudaMemcpyDeviceToHost, h->st));
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_ensemble_sums(tree_gpu_handle* h, double* out) {
+  if (!h || h->b.ens.nseg == 0 || !out) return TREE_GPU_ERR_ARG;
+  const int nc = h->b.ens.nseg;
+  tg::cloud_sums(h->x, h->v, h->epot_part, h->ens_start, h->ens_elec_end, nc,
+                 h->prm.xm_el, h->prm.xm_ion, h->cloud_sums, h->st);
+  h->timing.launches += 1;
+  CK(cudaMemcpyAsync(out, h->cloud_sums, 6 * sizeof(double) * nc,
+                     cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_ensemble_direct(tree_gpu_handle* h, int32_t cloud,
+                             const int64_t* targets, int64_t nt, double* f,
+                             double* epot) {
+  if (!h || h->b.ens.nseg == 0) return TREE_GPU_ERR_ARG;
+  if (cloud < 0 || cloud >= h->b.ens.nseg) return fail(h, TREE_GPU_ERR_ARG, "cloud index");
+  const int64_t ne = h->cloud_ne[cloud], nc = ne + h->cloud_ni[cloud];
+  int64_t off = 0;
+  for (int c = 0; c < cloud; ++c) off += h->cloud_ne[c] + h->cloud_ni[c];
+  if (nt < 0 || nt > 0x7fffffff || (nt && (!targets || !f || !epot)))
+    return fail(h, TREE_GPU_ERR_ARG, "bad target list");
+  if (nt == 0) return TREE_GPU_OK;
+  for (int64_t i = 0; i < nt; ++i)
+    if (targets[i] < 0 || targets[i] >= nc)
+      return fail(h, TREE_GPU_ERR_ARG, "target index out of range");
+  const tree_gpu_params& a = h->cloud_prm[cloud];
+  tg::WalkParams wp;
+  wp.physics = a.physics;
+  wp.theta = a.theta;
+  wp.rs = a.rs;
+  wp.lam_ee = kelbg_lambda_um(a.xm_el / 2.0, a.te);
+  wp.lam_ei = kelbg_lambda_um(a.xm_el * a.xm_ion / (a.xm_el + a.xm_ion), a.te);
+  wp.lam_ii = kelbg_lambda_um(a.xm_ion / 2.0, a.te);
+  wp.dx_ei = a.dx_ei;
+  wp.dx_ii = a.dx_ii;
+  int nch = tg::direct_chunks((int)nc, (int)nt);
+  int64_t* d_t = nullptr;
+  double4* d_part = nullptr;
+  double *d_f = nullptr, *d_e = nullptr;
+  int rc = TREE_GPU_OK;
+  do {
+    if (cudaMalloc(&d_t, nt * sizeof(int64_t)) != cudaSuccess ||
+        cudaMalloc(&d_part, (size_t)nch * nt * sizeof(double4)) != cudaSuccess ||
+        cudaMalloc(&d_f, 3 * nt * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&d_e, nt * sizeof(double)) != cudaSuccess) {
+      rc = fail(h, TREE_GPU_ERR_CUDA, "direct-sum scratch allocation failed");
+      break;
+    }
+    cudaMemcpyAsync(d_t, targets, nt * sizeof(int64_t), cudaMemcpyHostToDevice, h->st);
+    h->timing.launches += tg::direct_sum(h->x + 3 * off, (int)nc, (int)ne, d_t, (int)nt,
+                                         wp, nch, d_part, d_f, d_e, h->st);
+    cudaMemcpyAsync(f, d_f, 3 * nt * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    cudaMemcpyAsync(epot, d_e, nt * sizeof(double), cudaMemcpyDeviceToHost, h->st);
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) rc = fail(h, TREE_GPU_ERR_CUDA, cudaGetErrorString(e));
+  } while (0);
+  cudaFree(d_t);
+  cudaFree(d_part);
+  cudaFree(d_f);
+  cudaFree(d_e);
+  return rc;
+}
+
+
 }  // extern "C"
 
 // ------------------------------------------------------- learned MAC ----
@@ -968,6 +1200,8 @@ int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
                          double rho_lo, double rho_hi, int32_t max_count,
                          float keep, uint64_t seed, int64_t cap,
                          int64_t* n_total) {
+  if (h && h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: use the tree_gpu_ensemble_* calls");
   if (!h) return TREE_GPU_ERR_ARG;
   if (!(theta_lo > 0 && theta_hi >= theta_lo && rho_lo > 0 && rho_hi >= rho_lo) ||
       cap <= 0 || cap > (int64_t)0x7fffffff || max_count < 2 || !(keep > 0.f && keep <= 1.f))

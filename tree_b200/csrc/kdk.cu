@@ -39,12 +39,19 @@ __device__ __forceinline__ void block_sum4(double a[4], double* partial) {
   }
 }
 
+// Species of particle i: electrons [0, n_el) or, for an ensemble of clouds,
+// the per-particle flag.
+__device__ __forceinline__ bool is_ion(const uint8_t* __restrict__ ion, int i, int n_el) {
+  return ion ? ion[i] != 0 : i >= n_el;
+}
+
 __global__ void k_kick_drift(double* __restrict__ x, double* __restrict__ v,
                              const double* __restrict__ f, int n, int n_el,
-                             double dt, double xm_e, double xm_i) {
+                             const uint8_t* __restrict__ ion, double dt,
+                             double xm_e, double xm_i) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double xm = i < n_el ? xm_e : xm_i;
+  double xm = is_ion(ion, i, n_el) ? xm_i : xm_e;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     int64_t j = 3 * (int64_t)i + k;
@@ -59,12 +66,14 @@ __global__ void k_kick_drift(double* __restrict__ x, double* __restrict__ v,
 template <bool SAMPLE, bool DRIFT>
 __global__ void __launch_bounds__(kKdkThreads)
     k_kick2(double* __restrict__ x, double* __restrict__ v,
-            const double* __restrict__ f, int n, int n_el, double dt,
-            double xm_e, double xm_i, double* __restrict__ partial) {
+            const double* __restrict__ f, int n, int n_el,
+            const uint8_t* __restrict__ ion, double dt, double xm_e,
+            double xm_i, double* __restrict__ partial) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (i < n) {
-    double xm = i < n_el ? xm_e : xm_i;
+    const bool is = is_ion(ion, i, n_el);
+    double xm = is ? xm_i : xm_e;
     double xi[3], vi[3], fi[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -77,7 +86,7 @@ __global__ void __launch_bounds__(kKdkThreads)
     if (SAMPLE) {
       double mv2, rad;
       ke_terms(xi, vi, xm, mv2, rad);
-      int s = i >= n_el;
+      int s = is ? 1 : 0;
       acc[2 * s] = mv2;
       acc[2 * s + 1] = rad;
     }
@@ -128,25 +137,68 @@ __global__ void __launch_bounds__(kKdkThreads)
 int kdk_partials_needed(int n) { return (n + kKdkThreads - 1) / kKdkThreads; }
 
 void kick_drift(double* x, double* v, const double* f, int n, int n_el,
-                double dt, double xm_e, double xm_i, cudaStream_t st) {
+                const uint8_t* ion, double dt, double xm_e, double xm_i,
+                cudaStream_t st) {
   if (n == 0) return;
   int g = (n + kKdkThreads - 1) / kKdkThreads;
-  k_kick_drift<<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i);
+  k_kick_drift<<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, ion, dt, xm_e, xm_i);
 }
 
-void kick2(double* x, double* v, const double* f, int n, int n_el, double dt,
-           double xm_e, double xm_i, bool sample, bool drift, double* partial,
-           double* out4, cudaStream_t st) {
+void kick2(double* x, double* v, const double* f, int n, int n_el,
+           const uint8_t* ion, double dt, double xm_e, double xm_i, bool sample,
+           bool drift, double* partial, double* out4, cudaStream_t st) {
   if (n == 0) return;
   int g = (n + kKdkThreads - 1) / kKdkThreads;
   if (sample) {
-    if (drift) k_kick2<true, true><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
-    else k_kick2<true, false><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
+    if (drift) k_kick2<true, true><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, ion, dt, xm_e, xm_i, partial);
+    else k_kick2<true, false><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, ion, dt, xm_e, xm_i, partial);
     k_sum_partials4<<<1, kKdkThreads, 0, st>>>(partial, g, out4);
   } else {
-    if (drift) k_kick2<false, true><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
-    else k_kick2<false, false><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, dt, xm_e, xm_i, partial);
+    if (drift) k_kick2<false, true><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, ion, dt, xm_e, xm_i, partial);
+    else k_kick2<false, false><<<g, kKdkThreads, 0, st>>>(x, v, f, n, n_el, ion, dt, xm_e, xm_i, partial);
   }
+}
+
+// Per-cloud diagnostics of an ensemble, one block per cloud in fixed order:
+// out[6c..6c+5] = (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion).
+__global__ void __launch_bounds__(kKdkThreads)
+    k_cloud_sums(const double* __restrict__ x, const double* __restrict__ v,
+                 const double2* __restrict__ ep, const int32_t* __restrict__ start,
+                 const int32_t* __restrict__ elec_end, double xm_e, double xm_i,
+                 double* out) {
+  __shared__ double sh[kKdkThreads / 32][6];
+  const int c = blockIdx.x;
+  const int i0 = start[c], i1 = start[c + 1], ie = elec_end[c];
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const double2 e = ep[i];
+    a[0] += e.x;
+    a[1] += e.y;
+    const int s = i >= ie;
+    double mv2, rad;
+    ke_terms(x + 3 * (int64_t)i, v + 3 * (int64_t)i, s ? xm_i : xm_e, mv2, rad);
+    a[2 + s] += mv2;
+    a[4 + s] += rad;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    for (int o = 16; o > 0; o >>= 1) a[j] += __shfl_down_sync(0xffffffffu, a[j], o);
+    if (lane == 0) sh[w][j] = a[j];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int ww = 0; ww < kKdkThreads / 32; ++ww) s += sh[ww][threadIdx.x];
+    out[6 * c + threadIdx.x] = s;
+  }
+}
+
+void cloud_sums(const double* x, const double* v, const double2* ep,
+                const int32_t* start, const int32_t* elec_end, int nseg,
+                double xm_e, double xm_i, double* out, cudaStream_t st) {
+  if (nseg > 0)
+    k_cloud_sums<<<nseg, kKdkThreads, 0, st>>>(x, v, ep, start, elec_end, xm_e, xm_i, out);
 }
 
 void epot_sum(const double2* ep, int n, double* partial, double* out4,

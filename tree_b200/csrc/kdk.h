@@ -6,14 +6,20 @@
 namespace tg {
 
 int kdk_partials_needed(int n);
-// VVerletNotemp1 for all particles (electrons [0,n_el) use xm_e).
+// VVerletNotemp1 for all particles (electrons [0,n_el) use xm_e; with a
+// per-particle ion flag, as in an ensemble of clouds, the flag decides).
 void kick_drift(double* x, double* v, const double* f, int n, int n_el,
-                double dt, double xm_e, double xm_i, cudaStream_t st);
+                const uint8_t* ion, double dt, double xm_e, double xm_i,
+                cudaStream_t st);
 // VVerletNotemp2 (+ next VVerletNotemp1 when drift).  When sample, out4 gets
 // (mv2_el, rad_el, mv2_ion, rad_ion) of the state after the second kick.
-void kick2(double* x, double* v, const double* f, int n, int n_el, double dt,
-           double xm_e, double xm_i, bool sample, bool drift, double* partial,
-           double* out4, cudaStream_t st);
+void kick2(double* x, double* v, const double* f, int n, int n_el,
+           const uint8_t* ion, double dt, double xm_e, double xm_i, bool sample,
+           bool drift, double* partial, double* out4, cudaStream_t st);
+// Per-cloud (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion) of an ensemble.
+void cloud_sums(const double* x, const double* v, const double2* ep,
+                const int32_t* start, const int32_t* elec_end, int nseg,
+                double xm_e, double xm_i, double* out, cudaStream_t st);
 // out4 = (Epot_e, Epot_i, 0, 0)
 void epot_sum(const double2* ep, int n, double* partial, double* out4,
               cudaStream_t st);

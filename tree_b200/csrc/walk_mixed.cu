@@ -53,6 +53,9 @@ struct WarpSmem {
   // (Tyyz, Txzz, Tyzz, Txyz) -- S and T trace-free
   float4 cell[32 * kCellF4];
   float4 part[32 * 2];   // (hi xyz, sorted index bits), (lo xyz, charge)
+  // pair constants of the group's cloud: 1/lambda^2 (ee, ei, ii), 1/rs,
+  // 1/lambda (ee, ei, ii)
+  float pk[8];
 };
 
 struct MixedArgs {
@@ -92,6 +95,11 @@ struct MixedArgs {
   float eta_over_eps;
   float rho_lo, rho_hi;
   float lam_ei;
+  // ensemble of clouds (nseg > 0): cloud ranges, roots, pair constants
+  int nseg;
+  const int32_t* ens_start;
+  const int32_t* roots;
+  const float4* cloud_pk;  // 2 per cloud, the layout of WarpSmem::pk
 };
 
 struct Acc {
@@ -244,8 +252,9 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
   __syncwarp();
   const float tq = tsp ? 1.f : -1.f;  // target charge
   // pair constants of the target's own species and of the other species
-  const float il2_same = PHYS == 1 ? (tsp ? a.inv_lam2_ii : a.inv_lam2_ee) : 0.f;
-  const float il_same = PHYS == 1 ? (tsp ? a.inv_lam_ii : a.inv_lam_ee) : 0.f;
+  const float il2_same = PHYS == 1 ? (tsp ? sm.pk[2] : sm.pk[0]) : 0.f;
+  const float il_same = PHYS == 1 ? (tsp ? sm.pk[6] : sm.pk[4]) : 0.f;
+  const float il2_ei = sm.pk[1], il_ei = sm.pk[5], rs_inv = sm.pk[3];
   float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pq = 0.f;
   for (int k = 0; k < cnt; ++k) {
     const float4 P = sm.part[2 * k], Q = sm.part[2 * k + 1];
@@ -260,7 +269,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
     bool rare;
     float wc;  // weight of the plain Coulomb term
     if (PHYS == 1) {
-      const float il2 = same ? il2_same : a.inv_lam2_ei;
+      const float il2 = same ? il2_same : il2_ei;
       rare = !self && r2 * il2 < 40.f;  // exp(-x^2) still visible in FP32
       wc = (self || rare) ? 0.f : ssign;
     } else {
@@ -268,7 +277,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
         rare = false;
         wc = r2 > 0.01f ? ssign : 0.f;  // reference cutoff, also drops self
       } else {
-        rare = r2 * (a.rs_inv * a.rs_inv) < 400.f;  // exp(-r/rs) visible
+        rare = r2 * (rs_inv * rs_inv) < 400.f;  // exp(-r/rs) visible
         wc = rare ? 0.f : ssign;
       }
     }
@@ -281,7 +290,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
     if (rare) {
       float rfs = 0.f, ve;
       if (PHYS == 1) {
-        const float il = same ? il_same : a.inv_lam_ei;
+        const float il = same ? il_same : il_ei;
         const float sqrtpi = 1.77245385f;
         if (r2 > 0.f) {
           const float r = sqrtf(r2);
@@ -297,12 +306,12 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
         if (r2 > 0.f) {
           const float r = sqrtf(r2);
           const float ri = 1.f / r;
-          const float e = expf(-r * a.rs_inv);
-          const float g = ri - e * (ri + a.rs_inv);
+          const float e = expf(-r * rs_inv);
+          const float g = ri - e * (ri + rs_inv);
           rfs = ssign * g * ri * ri;
           ve = (1.f - e) * ri;
         } else {
-          ve = a.rs_inv;  // r -> 0 limit of (1 - exp(-r/rs))/r
+          ve = rs_inv;  // r -> 0 limit of (1 - exp(-r/rs))/r
         }
       }
       fx = fmaf(rfs, dx, fx);
@@ -410,7 +419,33 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
       hlen = (float)sqrt(hx * hx + hy * hy + hz * hz);
     }
     int ssize = 1;
-    if (lane == 0) stack[0] = 0;  // root
+    // the group's tree: its cloud's root and pair constants
+    int root = 0;
+    if (a.nseg > 0) {
+      int c = 0;
+      if (lane == 0) {
+        int lo = 0, hi = a.nseg - 1;  // largest c with start[c] <= p0
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (__ldg(&a.ens_start[mid]) <= p0) lo = mid;
+          else hi = mid - 1;
+        }
+        c = lo;
+      }
+      c = __shfl_sync(0xffffffffu, c, 0);
+      root = __ldg(&a.roots[c]);
+      if (lane < 8) sm.pk[lane] = __ldg(reinterpret_cast<const float*>(a.cloud_pk + 2 * c) + lane);
+    } else if (lane == 0) {
+      sm.pk[0] = a.inv_lam2_ee;
+      sm.pk[1] = a.inv_lam2_ei;
+      sm.pk[2] = a.inv_lam2_ii;
+      sm.pk[3] = a.rs_inv;
+      sm.pk[4] = a.inv_lam_ee;
+      sm.pk[5] = a.inv_lam_ei;
+      sm.pk[6] = a.inv_lam_ii;
+      sm.pk[7] = 0.f;
+    }
+    if (lane == 0) stack[0] = root;
     __syncwarp();
     int m2h = 0, m2t = 0, p2h = 0, p2t = 0;  // ring heads/tails (warp-uniform)
     long long n_m2p = 0, n_p2p = 0;
@@ -696,6 +731,7 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
 int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
                int n, int n_el, const TreeView& tv, const WalkParams& wp,
                const MixedTuning& tune, const LearnedMac* learned,
+               const Ensemble& ens, const float4* cloud_pk,
                double* f, double2* epot_part,
                uint32_t* rdf, unsigned long long* counters, int32_t* err,
                cudaStream_t st) {
@@ -751,6 +787,10 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.rho_lo = L ? learned->rho_lo : 0.f;
   a.rho_hi = L ? learned->rho_hi : 0.f;
   a.lam_ei = (float)wp.lam_ei;
+  a.nseg = ens.nseg;
+  a.ens_start = ens.start;
+  a.roots = ens.roots;
+  a.cloud_pk = cloud_pk;
   int bps = tune.blocks_per_sm < 1 ? 1 : (tune.blocks_per_sm > kMaxBlocksPerSm ? kMaxBlocksPerSm : tune.blocks_per_sm);
   int grid = (mb.grid_warps / (kMaxBlocksPerSm * kMxWarps)) * bps;
   const bool r = rdf != nullptr;

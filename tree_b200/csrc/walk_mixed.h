@@ -58,6 +58,7 @@ MixedNodes mixed_nodes(const MixedBuffers& mb);
 int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
                int n, int n_el, const TreeView& tv, const WalkParams& wp,
                const MixedTuning& tune, const LearnedMac* learned,
+               const Ensemble& ens, const float4* cloud_pk,
                double* f, double2* epot_part,
                uint32_t* rdf, unsigned long long* counters, int32_t* err,
                cudaStream_t st);
