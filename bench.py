@@ -61,6 +61,12 @@ def parse():
     ap.add_argument("--eta", type=float, default=HEADLINE["eta"])
     ap.add_argument("--order", type=int, default=HEADLINE["order"])
     ap.add_argument("--bucket", type=int, default=HEADLINE["bucket"])
+    ap.add_argument("--workload", choices=["cloud", "ensemble"], default="cloud",
+                    help="cloud: one N=1,048,576 cloud (headline); ensemble: 64 "
+                         "independent clouds of uneven N in one handle")
+    ap.add_argument("--clouds", type=int, default=64)
+    ap.add_argument("--tune", action="store_true",
+                    help="ensemble: autotune theta/eta/bucket/grid on the warm state")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the fixed-theta and plain-FP64 comparison arms")
     ap.add_argument("--ref-theta", type=float, default=0.5,
@@ -461,6 +467,146 @@ def run_ours(args, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------- ensemble ----
+def run_ensemble(args, rank, world, dist):
+    """Independent clouds of uneven N (log-uniform in [8192, 131072]), peak
+    densities log-uniform in [1e14, 1e16] m^-3, T_e uniform in [10, 200] K, in
+    one handle: one build, one persistent walk launch and one integrator launch
+    per step, replayed as CUDA graphs.  Compared with the same clouds stepped
+    one handle after another from the same state."""
+    import torch
+
+    from tree_b200 import api, cloud, learned_mac, tune, units
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    dt = units.dt_code(1e-11)
+    clouds, te, n0 = cloud.make_ensemble(args.clouds, seed=args.seed + rank)
+    x, v, n_el, n_ion = cloud.pack_ensemble(clouds)
+    n = len(x)
+    phys = api.PHYS_KELBG if args.physics == "kelbg" else api.PHYS_REF
+    mac = api.MAC_LEARNED if args.mac == "learned" else api.MAC_FIXED
+    cfgs = [api.Config(theta=args.theta, te=float(t), physics=phys,
+                       precision=api.PREC_MIXED, mac=mac) for t in te]
+    params, stats, _ = learned_mac.load_model()
+    stream = torch.cuda.Stream()
+    ens = api.Ensemble(cfgs, n_el, n_ion)
+    ens.set_stream(stream.cuda_stream)
+    ens.set_tuning(args.bucket, 4, args.order)
+    ens.mac_set_model(params, stats)
+    ens.mac_config(args.eta, 0.05, 0.9)
+    ens.set_state(x, v)
+    ens.step(dt, max(args.warmup, 3))
+    torch.cuda.synchronize()
+    tuned = None
+    if args.tune:
+        space = [tune.Candidate(t, e, b, 3, g) for t in (0.24, 0.26, 0.28, 0.30)
+                 for e in (1e-5, 3e-5) for b in (6, 8) for g in (3, 4)]
+        best, trials = tune.autotune(ens, dt, space=space, target=1e-4, audit=32768,
+                                     physics=phys, model=(params, stats))
+        if best is not None:
+            tuned = {**{k: getattr(best.cand, k) for k in ("theta", "eta", "bucket",
+                                                           "order", "blocks_per_sm")},
+                     "ms": best.ms, "rms": best.rms, "trials": len(trials)}
+    warm = ens.get_state()
+    if dist:
+        dist.barrier()
+    t_before = ens.timings()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step(dt, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t_after = ens.timings()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * world * args.steps / (ms / 1e3)
+    # per-cloud accuracy against each cloud's own FP64 direct sum
+    f = ens.get_state()["f"]
+    rms = []
+    for c in range(args.clouds):
+        a, b = int(ens.offsets[c]), int(ens.offsets[c + 1])
+        t = np.sort(np.random.default_rng(c).choice(b - a, min(4096, b - a), replace=False))
+        fd, _ = ens.direct(c, t)
+        err = np.linalg.norm(f[a:b][t] - fd, axis=1) / np.linalg.norm(fd, axis=1)
+        rms.append(float(np.sqrt(np.mean(err ** 2))))
+    # end to end: cloud-major state host -> device, one step, state back
+    pin = {k: torch.from_numpy(np.ascontiguousarray(warm[k])).pin_memory() for k in ("x", "v", "f")}
+    k2 = max(1, min(args.steps, 5))
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(k2):
+        ens.load_state(pin["x"].data_ptr(), pin["v"].data_ptr(), pin["f"].data_ptr())
+        ens.step(dt, 1)
+        ens.get_state_ptr(pin["x"].data_ptr(), pin["v"].data_ptr(), pin["f"].data_ptr())
+    a1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a0.elapsed_time(a1) / k2
+    # the same clouds, one handle after another, from the same warm state
+    sep_ms = None
+    if not args.no_compare:
+        tb = ens.timings()
+        sep_ms = 0.0
+        for c in range(args.clouds):
+            a, b = int(ens.offsets[c]), int(ens.offsets[c + 1])
+            ne = int(n_el[c])
+            sl = {k: warm[k][a:b] for k in ("x", "v", "f")}
+            cfg = api.Config(theta=ens.config.theta, te=float(te[c]), physics=phys,
+                             precision=api.PREC_MIXED, mac=ens.config.mac)
+            with api.TreeForce(ne, b - a - ne, cfg) as tc:
+                tc.set_stream(stream.cuda_stream)
+                tc.set_tuning(args.bucket, 4, args.order)
+                tc.mac_set_model(params, stats)
+                tc.mac_config(args.eta if tuned is None else tuned["eta"], 0.05, 0.9)
+                tc.load_state(sl["x"][:ne], sl["v"][:ne], sl["f"][:ne], sl["x"][ne:],
+                              sl["v"][ne:], sl["f"][ne:])
+                tc.step(dt, 1)
+                tc.load_state(sl["x"][:ne], sl["v"][:ne], sl["f"][:ne], sl["x"][ne:],
+                              sl["v"][ne:], sl["f"][ne:])
+                s0 = torch.cuda.Event(enable_timing=True)
+                s1 = torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                tc.step(dt, args.steps)
+                s1.record(stream)
+                torch.cuda.synchronize()
+                sep_ms += s0.elapsed_time(s1) / args.steps
+    ens.close()
+    if rank != 0:
+        return
+    walk_ms = (t_after.ms_walk - t_before.ms_walk) / args.steps
+    build_ms = (t_after.ms_build - t_before.ms_build) / args.steps
+    line = {
+        "metric": f"particle-steps/s, ensemble of {args.clouds} independent clouds in one handle",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (walk) + f64 (positions, Verlet, top cells)",
+        "data": "synthetic (seeded Gaussian UCP clouds, electrons start on ions)",
+        "config": {"workload": f"{args.clouds} clouds, N log-uniform in [8192, 131072] "
+                               f"(total {n}), n0 log-uniform in [1e14, 1e16] m^-3, "
+                               f"T_e uniform in [10, 200] K, T_i = 1 mK, dt = 1e-11 s",
+                   "n_particles": n, "theta": ens.config.theta, "mac": args.mac,
+                   "eta": args.eta if tuned is None else tuned["eta"], "tuned": tuned,
+                   "l2": "inputs larger than L2"},
+        "clocks": clk, "gpu_launches": t_after.launches - t_before.launches,
+        "phases_ms_per_step": {"build": build_ms, "walk": walk_ms},
+        "accuracy": {"targets_per_cloud": 4096, "rms_rel_err_max_cloud": max(rms),
+                     "rms_rel_err_median_cloud": float(np.median(rms))},
+        "e2e": {"value": n * world / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n},
+        "separate_handles_ms_per_step": sep_ms,
+        "one_launch_speedup": (sep_ms / (ms / args.steps)) if sep_ms else None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -478,6 +624,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "ensemble":
+            run_ensemble(args, rank, world, dist)
         else:
             run_ours(args, rank, world, dist)
     finally:

@@ -487,6 +487,10 @@ class Ensemble(TreeForce):
         self._check(self.lib.tree_gpu_ensemble_get_state(self.h, _dp(x), _dp(v), _dp(f)))
         return dict(x=x, v=v, f=f)
 
+    def get_state_ptr(self, x, v, f):
+        """get_state into raw host addresses (pinned buffers)."""
+        self._check(self.lib.tree_gpu_ensemble_get_state(self.h, _dp(x), _dp(v), _dp(f)))
+
     def sums(self):
         """Per-cloud (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion)."""
         out = np.zeros((self.ncloud, 6))

@@ -1,0 +1,107 @@
+"""Long-run measurements of the force path on one GPU.
+
+    python -m tree_b200.sweep precision [--n 1048576] [--steps 1000]
+    python -m tree_b200.sweep drift [--n 1048576] [--steps 1000]
+
+precision: the precision form -- seeded clouds at T_e in {10, 50, 200} K,
+    each run with the mixed-precision walk at opening angles {0.3, 0.5, 0.7}
+    for `steps` steps; at steps 1, 10, 100 and the last, the rms and max
+    relative force error against the FP64 O(N^2) direct sum on 16,384 seeded
+    targets, and the time per step.
+drift: the total energy 1/2 (mv2_el + mv2_ion) + Epot_e + Epot_i, sampled every
+    10 steps over `steps` steps from the same seeded cloud, for the
+    mixed-precision walk with the learned criterion (theta 0.30, eta 3e-5) and
+    for the plain FP64 fixed-theta path (theta 0.5); reports the largest
+    excursion |E - E_0| relative to the mean kinetic energy for both.
+
+One JSON line per run.  Inputs are seeded synthetic clouds (Gaussian at peak
+density 1e15 m^-3, electrons on their ions at t = 0, T_i = 1 mK, dt = 1e-11 s).
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import api, cloud, learned_mac, units
+
+
+def _audit(tf, idx):
+    st = tf.get_state()
+    fd, _ = tf.direct(idx)
+    f = np.vstack([st["f_el"], st["f_ion"]])[idx]
+    err = np.linalg.norm(f - fd, axis=1) / np.linalg.norm(fd, axis=1)
+    return float(np.sqrt(np.mean(err ** 2))), float(err.max())
+
+
+def precision(n, steps, seed, tes=(10.0, 50.0, 200.0), thetas=(0.3, 0.5, 0.7)):
+    dt = units.dt_code(1e-11)
+    rng = np.random.default_rng(seed + 17)
+    idx = np.sort(rng.choice(n, min(16384, n), replace=False))
+    marks = sorted({m for m in (1, 10, 100, steps) if m <= steps})
+    for te in tes:
+        c = cloud.make_cloud(n, seed=seed, te_k=te)
+        for th in thetas:
+            cfg = api.Config(theta=th, te=te, physics=api.PHYS_KELBG, precision=api.PREC_MIXED)
+            with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
+                tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
+                done, rows = 0, []
+                t0 = tf.timings()
+                wall = 0.0
+                for m in marks:
+                    w0 = time.perf_counter()
+                    tf.step(dt, m - done)
+                    wall += time.perf_counter() - w0
+                    done = m
+                    rms, mx = _audit(tf, idx)
+                    rows.append({"step": m, "rms": rms, "max": mx})
+                t1 = tf.timings()
+            print(json.dumps({"mode": "precision", "n": n, "te_k": te, "theta": th,
+                              "steps": steps, "audits": rows,
+                              "ms_per_step": (t1.ms_total - t0.ms_total) / steps}), flush=True)
+
+
+def drift(n, steps, seed, nsamp=10):
+    dt = units.dt_code(1e-11)
+    c = cloud.make_cloud(n, seed=seed)
+    params, stats, _ = learned_mac.load_model()
+    out = {}
+    arms = (("mixed_learned", api.Config(theta=0.30, physics=api.PHYS_KELBG,
+                                         precision=api.PREC_MIXED, mac=api.MAC_LEARNED)),
+            ("fp64_plain", api.Config(theta=0.5, physics=api.PHYS_KELBG,
+                                      precision=api.PREC_FP64)))
+    for name, cfg in arms:
+        with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
+            if cfg.precision == api.PREC_MIXED:
+                tf.set_tuning(8, 4, 3)
+                tf.mac_set_model(params, stats)
+                tf.mac_config(3e-5, 0.05, 0.9)
+            tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
+            t0 = tf.timings()
+            rec = tf.run(dt, steps, nsamp=nsamp)
+            t1 = tf.timings()
+        e = 0.5 * (rec["mv2_el"] + rec["mv2_ion"]) + rec["epot_e"] + rec["epot_i"]
+        ke = 0.5 * (rec["mv2_el"] + rec["mv2_ion"])
+        out[name] = {"excursion_over_mean_ke": float(np.max(np.abs(e - e[0])) / np.mean(ke)),
+                     "e_first": float(e[0]), "e_last": float(e[-1]),
+                     "ms_per_step": (t1.ms_total - t0.ms_total) / steps}
+    out["ratio"] = out["mixed_learned"]["excursion_over_mean_ke"] / out["fp64_plain"]["excursion_over_mean_ke"]
+    print(json.dumps({"mode": "drift", "n": n, "steps": steps, "nsamp": nsamp, **out}),
+          flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("mode", choices=["precision", "drift"])
+    ap.add_argument("--n", type=int, default=1048576)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=2024)
+    args = ap.parse_args()
+    if args.mode == "precision":
+        precision(args.n, args.steps, args.seed)
+    else:
+        drift(args.n, args.steps, args.seed)
+
+
+if __name__ == "__main__":
+    main()

@@ -76,19 +76,74 @@ def _apply(tf, cand, physics, te, model):
         tf.mac_config(cand.eta, 0.05, 0.9)
 
 
+class _Single:
+    """State, forces and the FP64 judge of a single-cloud handle."""
+
+    def __init__(self, tf, audit, seed):
+        self.tf = tf
+        n = tf.n_el + tf.n_ion
+        self.idx = np.sort(np.random.default_rng(seed).choice(n, min(audit, n),
+                                                              replace=False))
+        self.snap = tf.get_state()
+
+    def load(self):
+        s = self.snap
+        self.tf.load_state(s["x_el"], s["v_el"], s["f_el"], s["x_ion"], s["v_ion"],
+                           s["f_ion"])
+
+    def forces(self):
+        st = self.tf.get_state()
+        return np.vstack([st["f_el"], st["f_ion"]])[self.idx]
+
+    def judge(self):
+        return self.tf.direct(self.idx)[0]
+
+    def rms(self, f, fd):
+        err = np.linalg.norm(f - fd, axis=1) / np.linalg.norm(fd, axis=1)
+        return float(np.sqrt(np.mean(err ** 2)))
+
+
+class _Clouds:
+    """The same for an ensemble: audit targets spread over the clouds, each
+    judged by its own cloud-local direct sum."""
+
+    def __init__(self, ens, audit, seed):
+        self.ens = ens
+        rng = np.random.default_rng(seed)
+        per = max(1, audit // ens.ncloud)
+        self.sel = []
+        for c in range(ens.ncloud):
+            m = int(ens.offsets[c + 1] - ens.offsets[c])
+            self.sel.append(np.sort(rng.choice(m, min(per, m), replace=False)))
+        self.snap = ens.get_state()
+
+    def load(self):
+        self.ens.load_state(self.snap["x"], self.snap["v"], self.snap["f"])
+
+    def forces(self):
+        f = self.ens.get_state()["f"]
+        return np.vstack([f[self.ens.offsets[c]:][t] for c, t in enumerate(self.sel)])
+
+    def judge(self):
+        return np.vstack([self.ens.direct(c, t)[0] for c, t in enumerate(self.sel)])
+
+    def rms(self, f, fd):
+        """The worst cloud's rms: every cloud must meet the target."""
+        err = np.linalg.norm(f - fd, axis=1) / np.linalg.norm(fd, axis=1)
+        ends = np.cumsum([len(t) for t in self.sel])
+        return max(float(np.sqrt(np.mean(e ** 2))) for e in np.split(err, ends[:-1]))
+
+
 def autotune(tf, dt, space=None, target=1e-4, margin=0.9, audit=4096, seed=0,
              physics=api.PHYS_KELBG, te=50.0, model=None, verbose=False):
-    """Times every candidate of `space` on tf's current state and applies the
-    fastest one that meets the accuracy target.  Returns (best Trial or None,
-    all trials).  tf's state is restored before returning."""
+    """Times every candidate of `space` on tf's current state (a TreeForce or
+    an Ensemble, where the worst cloud must meet the target) and applies the
+    fastest one that meets the accuracy target.
+    Returns (best Trial or None, all trials).  tf's state is restored before
+    returning."""
     space = list(space or default_space(model is not None))
-    snap = tf.get_state()
-    n = tf.n_el + tf.n_ion
-    idx = np.sort(np.random.default_rng(seed).choice(n, min(audit, n), replace=False))
-
-    def load():
-        tf.load_state(snap["x_el"], snap["v_el"], snap["f_el"], snap["x_ion"],
-                      snap["v_ion"], snap["f_ion"])
+    io = _Clouds(tf, audit, seed) if isinstance(tf, api.Ensemble) else _Single(tf, audit, seed)
+    load = io.load
 
     fd = None
     trials = []
@@ -102,13 +157,10 @@ def autotune(tf, dt, space=None, target=1e-4, margin=0.9, audit=4096, seed=0,
         t0 = tf.timings()
         tf.step(dt, 1)
         t1 = tf.timings()
-        st = tf.get_state()
         if fd is None:
-            fd, _ = tf.direct(idx)
-        f = np.vstack([st["f_el"], st["f_ion"]])[idx]
-        err = np.linalg.norm(f - fd, axis=1) / np.linalg.norm(fd, axis=1)
+            fd = io.judge()
         tr = Trial(cand, (t1.ms_build - t0.ms_build) + (t1.ms_walk - t0.ms_walk),
-                   float(np.sqrt(np.mean(err ** 2))), t1.n_m2p, t1.n_p2p)
+                   io.rms(io.forces(), fd), t1.n_m2p, t1.n_p2p)
         trials.append(tr)
         if verbose:
             print(json.dumps({**dataclasses.asdict(cand), "ms": tr.ms, "rms": tr.rms}),
