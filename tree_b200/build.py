@@ -74,7 +74,25 @@ def build(verbose=False):
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_driver()
     return LIB
+
+
+DRIVER = os.path.join(HERE, "tree_run")
+
+
+def build_driver():
+    """The host driver tree_b200/tree_run (control.prm / input.xyz in,
+    ener / rdf / res files out), linked against the library next to it."""
+    cxx = shutil.which("g++") or "g++"
+    src = os.path.join(HERE, "host", "tree_run.cpp")
+    cmd = [cxx, "-O2", "-std=c++17", src, "-o", DRIVER + ".tmp", "-L" + HERE,
+           "-ltree_b200", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -77,10 +77,17 @@ def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
 
 
 def save_model(path, params, stats, report):
+    """npz with the parameters, statistics and training report, and beside it
+    the raw .bin (parameters then statistics, float32) the C++ driver reads."""
     os.makedirs(os.path.dirname(path), exist_ok=True)
     np.savez(path, params=np.asarray(params, np.float32),
              stats=np.asarray(stats, np.float32),
              report=np.frombuffer(json.dumps(report).encode(), np.uint8))
+    write_bin(os.path.splitext(path)[0] + ".bin", params, stats)
+
+
+def write_bin(path, params, stats):
+    np.concatenate([np.asarray(params, "<f4"), np.asarray(stats, "<f4")]).tofile(path)
 
 
 def load_model(path=DEFAULT_MODEL):
