@@ -265,64 +265,61 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const float ssign = Q.w;  // source charge: -1 e, +1 ion
     const bool same = ssign == tq;
-    const bool self = s == p_self;
-    bool rare;
-    float wc;  // weight of the plain Coulomb term
-    if (PHYS == 1) {
-      const float il2 = same ? il2_same : il2_ei;
-      rare = !self && r2 * il2 < 40.f;  // exp(-x^2) still visible in FP32
-      wc = (self || rare) ? 0.f : ssign;
+    // "special" pairs leave the plain Coulomb law: the target itself (r = 0),
+    // pairs inside the Kelbg core (exp(-x^2) still visible in FP32), and for
+    // the reference laws same-species pairs inside the r^2 <= 0.01 cutoff and
+    // e-i pairs where exp(-r/rs) is visible.  They are rare, so the common
+    // path carries no selects.
+    bool special;
+    if (PHYS == 1) special = r2 * (same ? il2_same : il2_ei) < 40.f;
+    else special = same ? !(r2 > 0.01f) : r2 * (rs_inv * rs_inv) < 400.f;
+    float fs, ph;
+    if (!special) {
+      const float rinv = rsqrtf(r2);
+      fs = ssign * rinv * rinv * rinv;
+      ph = ssign * rinv;
     } else {
-      if (same) {
-        rare = false;
-        wc = r2 > 0.01f ? ssign : 0.f;  // reference cutoff, also drops self
-      } else {
-        rare = r2 * (rs_inv * rs_inv) < 400.f;  // exp(-r/rs) visible
-        wc = rare ? 0.f : ssign;
-      }
-    }
-    const float rinv = rsqrtf(r2 > 0.f ? r2 : 1.f);
-    const float fs = wc * rinv * rinv * rinv;
-    fx = fmaf(fs, dx, fx);
-    fy = fmaf(fs, dy, fy);
-    fz = fmaf(fs, dz, fz);
-    float ph = wc * rinv;
-    if (rare) {
-      float rfs = 0.f, ve;
+      fs = 0.f;
+      ph = 0.f;
       if (PHYS == 1) {
-        const float il = same ? il_same : il_ei;
-        const float sqrtpi = 1.77245385f;
-        if (r2 > 0.f) {
-          const float r = sqrtf(r2);
-          const float ri = 1.f / r;
-          const float x2 = r2 * il * il;
-          const float g = -expm1f(-x2);
-          rfs = ssign * g * ri * ri * ri;
-          ve = g * ri + sqrtpi * erfcf(r * il) * il;
-        } else {
-          ve = sqrtpi * il;  // distinct particles on one point: V(0)
+        if (s != p_self) {
+          const float il = same ? il_same : il_ei;
+          const float sqrtpi = 1.77245385f;
+          float ve;
+          if (r2 > 0.f) {
+            const float r = sqrtf(r2);
+            const float ri = 1.f / r;
+            const float x2 = r2 * il * il;
+            const float g = -expm1f(-x2);
+            fs = ssign * g * ri * ri * ri;
+            ve = g * ri + sqrtpi * erfcf(r * il) * il;
+          } else {
+            ve = sqrtpi * il;  // distinct particles on one point: V(0)
+          }
+          ph = ssign * ve;
         }
-      } else {
+      } else if (!same) {
+        float ve;
         if (r2 > 0.f) {
           const float r = sqrtf(r2);
           const float ri = 1.f / r;
           const float e = expf(-r * rs_inv);
           const float g = ri - e * (ri + rs_inv);
-          rfs = ssign * g * ri * ri;
+          fs = ssign * g * ri * ri;
           ve = (1.f - e) * ri;
         } else {
           ve = rs_inv;  // r -> 0 limit of (1 - exp(-r/rs))/r
         }
-      }
-      fx = fmaf(rfs, dx, fx);
-      fy = fmaf(rfs, dy, fy);
-      fz = fmaf(rfs, dz, fz);
-      ph += ssign * ve;
+        ph = ssign * ve;
+      }  // same species inside the cutoff (and the target itself): nothing
     }
+    fx = fmaf(fs, dx, fx);
+    fy = fmaf(fs, dy, fy);
+    fz = fmaf(fs, dz, fz);
     pa += ph;
     pq = fmaf(ssign, ph, pq);
     if (RDF && act) {
-      bool counted = PHYS == 1 ? !self : (same ? r2 > 0.01f : true);
+      bool counted = PHYS == 1 ? s != p_self : (same ? r2 > 0.01f : true);
       if (counted && (!same || tsp == 1)) {
         // bin in FP64 from the hi/lo offsets so bin edges match the FP64 path
         const double ex = ((double)thx - (double)P.x) + ((double)tlx - (double)Q.x);
