@@ -499,8 +499,8 @@ def run_ensemble(args, rank, world, dist):
     torch.cuda.synchronize()
     tuned = None
     if args.tune:
-        space = [tune.Candidate(t, e, b, 3, g) for t in (0.24, 0.26, 0.28, 0.30)
-                 for e in (1e-5, 3e-5) for b in (6, 8) for g in (3, 4)]
+        space = [tune.Candidate(t, e, 8, 3, g) for t in (0.20, 0.22, 0.24, 0.26, 0.28, 0.30)
+                 for e in (0.0, 3e-6, 1e-5, 3e-5) for g in (3, 4)]
         best, trials = tune.autotune(ens, dt, space=space, target=1e-4, audit=32768,
                                      physics=phys, model=(params, stats))
         if best is not None:
@@ -598,7 +598,10 @@ def run_ensemble(args, rank, world, dist):
         "clocks": clk, "gpu_launches": t_after.launches - t_before.launches,
         "phases_ms_per_step": {"build": build_ms, "walk": walk_ms},
         "accuracy": {"targets_per_cloud": 4096, "rms_rel_err_max_cloud": max(rms),
-                     "rms_rel_err_median_cloud": float(np.median(rms))},
+                     "rms_rel_err_median_cloud": float(np.median(rms)),
+                     "per_cloud": [{"n": int(ens.offsets[c + 1] - ens.offsets[c]),
+                                    "te_k": round(float(te[c]), 2), "n0": float(n0[c]),
+                                    "rms": rms[c]} for c in range(args.clouds)]},
         "e2e": {"value": n * world / (e2e_ms / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n},
         "separate_handles_ms_per_step": sep_ms,

@@ -841,17 +841,13 @@ __constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
 // (S'xx, S'yy, S'zz, Sxy), (Syz, Szx, trace S, q_ion); mom3 per node
 // (3 x float4): (T'xxx, T'yyy, T'zzz, T'xxy), (T'xxz, T'xyy, T'yyz, T'xzz),
 // (T'yzz, Txyz, |T'|_F, 0); geom (s, dx, n, |S'|_F).
-__global__ void k_upward_net(const double* __restrict__ x,
+// Leaves of the combined tree (one per sorted particle) and the sorted
+// positions the walk reads.
+__global__ void k_net_leaves(const double* __restrict__ x,
                              const uint32_t* __restrict__ vals,
                              const int8_t* __restrict__ L,
                              const int32_t* __restrict__ off, int n,
-                             int n_el_charge, const Geom* __restrict__ geom,
-                             double theta, int cap, double4* node_c,
-                             const int32_t* __restrict__ node_skip,
-                             const int32_t* __restrict__ node_parent,
-                             const int32_t* __restrict__ node_nchild,
-                             int32_t* node_done,
-                             const int8_t* __restrict__ node_level,
+                             int n_el_charge, int cap, double4* node_c,
                              MixedNodes mx, Ensemble ens, int32_t* err) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
@@ -887,133 +883,178 @@ __global__ void k_upward_net(const double* __restrict__ x,
     mx.geom[leaf] = make_float4(0.f, 0.f, 1.f, 0.f);
     mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
   }
-  __threadfence();
-  const double smax0 = geom[seg].smax0;
-  int cur = node_parent[leaf];
-  int guard = 0;
-  while (cur >= 0) {
-    if (++guard > kMaxLevel + 2) {
+}
+
+// Net moments of twig `cur` from its children (all final): centroid, then
+// Q, D, S and T about it by the parallel-axis rules, in the children's
+// pre-order; writes the FP64 record and the trace-free FP32 copies.
+__device__ bool net_twig(int cur, double smax0, double theta, int cap,
+                         double4* node_c, const int32_t* __restrict__ node_skip,
+                         const int8_t* __restrict__ node_level, MixedNodes mx,
+                         int32_t* err) {
+  const double4 gc = ldcg_d4(&node_c[cur]);  // geometric centre (topology)
+  int end = node_skip[cur];
+  if (end > cap) end = cap;
+  // pass 1: count and centroid
+  double nsum = 0.0, X0 = 0.0, X1 = 0.0, X2 = 0.0;
+  int c = cur + 1;
+  while (c < end) {
+    const double4 cc = ldcg_d4(&node_c[c]);
+    const double nc = __ldcg(mx.m64 + kM64 * (int64_t)c).x;
+    nsum += nc;
+    X0 += nc * cc.x;
+    X1 += nc * cc.y;
+    X2 += nc * cc.z;
+    int nx = node_skip[c];
+    if (nx <= c) {
       set_error(err, kErrWalk);
+      return false;
+    }
+    c = nx;
+  }
+  X0 /= nsum;
+  X1 /= nsum;
+  X2 /= nsum;
+  // pass 2: moments about the centroid
+  double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
+  double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
+  double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  c = cur + 1;
+  while (c < end) {
+    const double4 cc = ldcg_d4(&node_c[c]);
+    const double2* cm = mx.m64 + kM64 * (int64_t)c;
+    const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
+                  a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
+    const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
+    const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
+    {  // third moment, parallel axis
+      const double d[3] = {ex, ey, ez};
+      const double Dc[3] = {dcx, dcy, dcz};
+      const double S2[3][3] = {{2 * a3.x, 2 * a4.y, 2 * a5.y},
+                               {2 * a4.y, 2 * a3.y, 2 * a5.x},
+                               {2 * a5.y, 2 * a5.x, 2 * a4.x}};
+      double Tc[10];
+#pragma unroll
+      for (int u = 0; u < 5; ++u) {
+        const double2 t2 = __ldcg(cm + 6 + u);
+        Tc[2 * u] = t2.x;
+        Tc[2 * u + 1] = t2.y;
+      }
+#pragma unroll
+      for (int u = 0; u < 10; ++u) {
+        const int i = kTI[u][0], j = kTI[u][1], k = kTI[u][2];
+        T[u] += Tc[u] + d[i] * S2[j][k] + d[j] * S2[i][k] + d[k] * S2[i][j] +
+                d[i] * d[j] * Dc[k] + d[i] * Dc[j] * d[k] + Dc[i] * d[j] * d[k] +
+                qc * d[i] * d[j] * d[k];
+      }
+    }
+    Q += qc;
+    qi += a2.y;
+    Dx += dcx + qc * ex;
+    Dy += dcy + qc * ey;
+    Dz += dcz + qc * ez;
+    Sxx += a3.x + dcx * ex + 0.5 * qc * ex * ex;
+    Syy += a3.y + dcy * ey + 0.5 * qc * ey * ey;
+    Szz += a4.x + dcz * ez + 0.5 * qc * ez * ez;
+    Sxy += a4.y + 0.5 * (dcx * ey + ex * dcy) + 0.5 * qc * ex * ey;
+    Syz += a5.x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez;
+    Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
+    c = node_skip[c];
+  }
+  const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
+  const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+  const int lev = node_level[cur];
+  double smax = smax0;
+  for (int l = 0; l < lev; ++l) smax = smax * 0.5;
+  node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
+  double2* m = mx.m64 + kM64 * (int64_t)cur;
+  m[0] = make_double2(nsum, Q);
+  m[1] = make_double2(Dx, Dy);
+  m[2] = make_double2(Dz, qi);
+  m[3] = make_double2(Sxx, Syy);
+  m[4] = make_double2(Szz, Sxy);
+  m[5] = make_double2(Syz, Szx);
+#pragma unroll
+  for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+  // trace-free parts (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz)
+  const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
+  double Tt[10];
+  Tt[0] = T[0] - 0.6 * Vx;
+  Tt[1] = T[1] - 0.6 * Vy;
+  Tt[2] = T[2] - 0.6 * Vz;
+  Tt[3] = T[3] - 0.2 * Vy;
+  Tt[4] = T[4] - 0.2 * Vz;
+  Tt[5] = T[5] - 0.2 * Vx;
+  Tt[6] = T[6] - 0.2 * Vz;
+  Tt[7] = T[7] - 0.2 * Vx;
+  Tt[8] = T[8] - 0.2 * Vy;
+  Tt[9] = T[9];
+  double tn = 0.0;
+#pragma unroll
+  for (int u = 0; u < 10; ++u) tn += kTMult[u] * Tt[u] * Tt[u];
+  const double trS = Sxx + Syy + Szz;
+  const double Sxxt = Sxx - trS / 3.0, Syyt = Syy - trS / 3.0, Szzt = Szz - trS / 3.0;
+  const double sn = sqrt(Sxxt * Sxxt + Syyt * Syyt + Szzt * Szzt +
+                         2.0 * (Sxy * Sxy + Syz * Syz + Szx * Szx));
+  float4* f3 = mx.mom3 + 3 * (int64_t)cur;
+  f3[0] = make_float4((float)Tt[0], (float)Tt[1], (float)Tt[2], (float)Tt[3]);
+  f3[1] = make_float4((float)Tt[4], (float)Tt[5], (float)Tt[6], (float)Tt[7]);
+  f3[2] = make_float4((float)Tt[8], (float)Tt[9], (float)sqrt(tn), 0.f);
+  float4* f = mx.mom + 3 * (int64_t)cur;
+  f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
+  f[1] = make_float4((float)Sxxt, (float)Syyt, (float)Szzt, (float)Sxy);
+  f[2] = make_float4((float)Syz, (float)Szx, (float)trS, (float)qi);
+  mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, (float)sn);
+  return true;
+}
+
+// Level-synchronous pass over the twigs: counted and listed by level, then
+// one launch per level from the deepest up, one thread per twig.  Every
+// child is final when its parent's level runs (a launch boundary orders
+// them), so no arrival counters or fences are needed and the critical path
+// is one round of loads per level.
+__global__ void k_level_count(const int32_t* __restrict__ node_pt,
+                              const int8_t* __restrict__ node_level,
+                              const int32_t* __restrict__ bounds, int cap,
+                              int32_t* lvl) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m && node_pt[i] < 0) atomicAdd(&lvl[node_level[i]], 1);
+}
+
+__global__ void k_level_offsets(int32_t* lvl) {
+  if (threadIdx.x != 0) return;
+  int run = 0;
+  for (int l = 0; l < kLevelSlots; ++l) {
+    lvl[kLevelSlots + l] = run;
+    lvl[2 * kLevelSlots + l] = 0;
+    run += lvl[l];
+  }
+}
+
+__global__ void k_level_scatter(const int32_t* __restrict__ node_pt,
+                                const int8_t* __restrict__ node_level,
+                                const int32_t* __restrict__ bounds, int cap,
+                                int32_t* lvl, int32_t* list) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m || node_pt[i] >= 0) return;
+  const int l = node_level[i];
+  list[lvl[kLevelSlots + l] + atomicAdd(&lvl[2 * kLevelSlots + l], 1)] = i;
+}
+
+__global__ void k_net_level(int level, const Geom* __restrict__ geom, double theta,
+                            int cap, double4* node_c,
+                            const int32_t* __restrict__ node_skip,
+                            const int8_t* __restrict__ node_level, MixedNodes mx,
+                            Ensemble ens, int32_t* err) {
+  if (*((volatile int32_t*)err) & kErrCapacity) return;
+  const int cnt = mx.lvl[level], base = mx.lvl[kLevelSlots + level];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+    const int cur = mx.lvl_list[base + k];
+    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[cur]) : 0;
+    if (!net_twig(cur, geom[seg].smax0, theta, cap, node_c, node_skip, node_level, mx, err))
       return;
-    }
-    int old = atomicAdd(&node_done[cur], 1);
-    if (old != node_nchild[cur] - 1) return;
-    __threadfence();
-    const double4 gc = ldcg_d4(&node_c[cur]);  // geometric centre (topology)
-    int end = node_skip[cur];
-    if (end > cap) end = cap;
-    // pass 1: count and centroid
-    double nsum = 0.0, X0 = 0.0, X1 = 0.0, X2 = 0.0;
-    int c = cur + 1;
-    while (c < end) {
-      const double4 cc = ldcg_d4(&node_c[c]);
-      const double nc = __ldcg(mx.m64 + kM64 * (int64_t)c).x;
-      nsum += nc;
-      X0 += nc * cc.x;
-      X1 += nc * cc.y;
-      X2 += nc * cc.z;
-      int nx = node_skip[c];
-      if (nx <= c) {
-        set_error(err, kErrWalk);
-        return;
-      }
-      c = nx;
-    }
-    X0 /= nsum;
-    X1 /= nsum;
-    X2 /= nsum;
-    // pass 2: moments about the centroid
-    double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
-    double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
-    double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    c = cur + 1;
-    while (c < end) {
-      const double4 cc = ldcg_d4(&node_c[c]);
-      const double2* cm = mx.m64 + kM64 * (int64_t)c;
-      const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
-                    a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
-      const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
-      const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
-      {  // third moment, parallel axis
-        const double d[3] = {ex, ey, ez};
-        const double Dc[3] = {dcx, dcy, dcz};
-        const double S2[3][3] = {{2 * a3.x, 2 * a4.y, 2 * a5.y},
-                                 {2 * a4.y, 2 * a3.y, 2 * a5.x},
-                                 {2 * a5.y, 2 * a5.x, 2 * a4.x}};
-        double Tc[10];
-#pragma unroll
-        for (int u = 0; u < 5; ++u) {
-          const double2 t2 = __ldcg(cm + 6 + u);
-          Tc[2 * u] = t2.x;
-          Tc[2 * u + 1] = t2.y;
-        }
-#pragma unroll
-        for (int u = 0; u < 10; ++u) {
-          const int i = kTI[u][0], j = kTI[u][1], k = kTI[u][2];
-          T[u] += Tc[u] + d[i] * S2[j][k] + d[j] * S2[i][k] + d[k] * S2[i][j] +
-                  d[i] * d[j] * Dc[k] + d[i] * Dc[j] * d[k] + Dc[i] * d[j] * d[k] +
-                  qc * d[i] * d[j] * d[k];
-        }
-      }
-      Q += qc;
-      qi += a2.y;
-      Dx += dcx + qc * ex;
-      Dy += dcy + qc * ey;
-      Dz += dcz + qc * ez;
-      Sxx += a3.x + dcx * ex + 0.5 * qc * ex * ex;
-      Syy += a3.y + dcy * ey + 0.5 * qc * ey * ey;
-      Szz += a4.x + dcz * ez + 0.5 * qc * ez * ez;
-      Sxy += a4.y + 0.5 * (dcx * ey + ex * dcy) + 0.5 * qc * ex * ey;
-      Syz += a5.x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez;
-      Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
-      c = node_skip[c];
-    }
-    const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
-    const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
-    const int lev = node_level[cur];
-    double smax = smax0;
-    for (int l = 0; l < lev; ++l) smax = smax * 0.5;
-    node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
-    double2* m = mx.m64 + kM64 * (int64_t)cur;
-    m[0] = make_double2(nsum, Q);
-    m[1] = make_double2(Dx, Dy);
-    m[2] = make_double2(Dz, qi);
-    m[3] = make_double2(Sxx, Syy);
-    m[4] = make_double2(Szz, Sxy);
-    m[5] = make_double2(Syz, Szx);
-#pragma unroll
-    for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
-    // trace-free parts (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz)
-    const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
-    double Tt[10];
-    Tt[0] = T[0] - 0.6 * Vx;
-    Tt[1] = T[1] - 0.6 * Vy;
-    Tt[2] = T[2] - 0.6 * Vz;
-    Tt[3] = T[3] - 0.2 * Vy;
-    Tt[4] = T[4] - 0.2 * Vz;
-    Tt[5] = T[5] - 0.2 * Vx;
-    Tt[6] = T[6] - 0.2 * Vz;
-    Tt[7] = T[7] - 0.2 * Vx;
-    Tt[8] = T[8] - 0.2 * Vy;
-    Tt[9] = T[9];
-    double tn = 0.0;
-#pragma unroll
-    for (int u = 0; u < 10; ++u) tn += kTMult[u] * Tt[u] * Tt[u];
-    const double trS = Sxx + Syy + Szz;
-    const double Sxxt = Sxx - trS / 3.0, Syyt = Syy - trS / 3.0, Szzt = Szz - trS / 3.0;
-    const double sn = sqrt(Sxxt * Sxxt + Syyt * Syyt + Szzt * Szzt +
-                           2.0 * (Sxy * Sxy + Syz * Syz + Szx * Szx));
-    float4* f3 = mx.mom3 + 3 * (int64_t)cur;
-    f3[0] = make_float4((float)Tt[0], (float)Tt[1], (float)Tt[2], (float)Tt[3]);
-    f3[1] = make_float4((float)Tt[4], (float)Tt[5], (float)Tt[6], (float)Tt[7]);
-    f3[2] = make_float4((float)Tt[8], (float)Tt[9], (float)sqrt(tn), 0.f);
-    float4* f = mx.mom + 3 * (int64_t)cur;
-    f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
-    f[1] = make_float4((float)Sxxt, (float)Syyt, (float)Szzt, (float)Sxy);
-    f[2] = make_float4((float)Syz, (float)Szx, (float)trS, (float)qi);
-    mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, (float)sn);
-    __threadfence();
-    cur = node_parent[cur];
   }
 }
 
@@ -1118,10 +1159,23 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
                                b.node_done, b.node_level, b.err);
     return launches + 1;
   }
-  k_upward_net<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.geom, theta,
-                                 b.cap, b.node_c, b.node_skip, b.node_parent,
-                                 b.node_nchild, b.node_done, b.node_level, b.mx,
-                                 ens, b.err);
+  k_net_leaves<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.cap, b.node_c,
+                                 b.mx, ens, b.err);
+  cudaMemsetAsync(b.mx.lvl, 0, sizeof(int32_t) * kLevelSlots, st);
+  k_level_count<<<gcap, T, 0, st>>>(b.node_pt, b.node_level, b.bounds, b.cap, b.mx.lvl);
+  k_level_offsets<<<1, 32, 0, st>>>(b.mx.lvl);
+  k_level_scatter<<<gcap, T, 0, st>>>(b.node_pt, b.node_level, b.bounds, b.cap,
+                                      b.mx.lvl, b.mx.lvl_list);
+  launches += 3;
+  {
+    int lgrid = (n + T - 1) / T;
+    if (lgrid > 4 * 148) lgrid = 4 * 148;
+    for (int level = kMaxLevel; level >= 0; --level) {
+      k_net_level<<<lgrid, T, 0, st>>>(level, b.geom, theta, b.cap, b.node_c,
+                                       b.node_skip, b.node_level, b.mx, ens, b.err);
+      ++launches;
+    }
+  }
   cudaMemsetAsync(b.mx.n_groups, 0, sizeof(int32_t), st);
   k_groups<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_parent, b.mx, b.mx.groups,
                                b.mx.n_groups);

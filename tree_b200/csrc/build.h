@@ -21,7 +21,11 @@ struct MixedNodes {
   double4* xs;       // per sorted particle: position, w = 1 for ions
   int2* groups;      // target groups (first sorted particle, count)
   int32_t* n_groups; // device count of groups
+  int32_t* lvl_list; // per node: twigs grouped by level (upward pass)
+  int32_t* lvl;      // kLevelSlots x 3: count, offset, cursor per level
 };
+
+constexpr int kLevelSlots = 64;  // > deepest twig level
 
 // Independent clouds in one combined forest (mixed path only).  Cloud c holds
 // particles [start[c], start[c+1]) of the index space, electrons first up to

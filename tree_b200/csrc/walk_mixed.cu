@@ -172,55 +172,59 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
   }
   __syncwarp();
   float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
-#pragma unroll 2
+#pragma unroll 1
   for (int k = 0; k < cnt; ++k) {
     const float4* cl = sm.cell + kCellF4 * k;
     const float4 A = cl[0], B = cl[1], C = cl[2], E = cl[3];
     const float dx = tx - A.x, dy = ty - A.y, dz = tz - A.z;
-    const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
     // accepted cells are farther than rcrit >= 0; the floor only guards a
     // zero-size cell against an FP32 distance of 0
-    const float r2 = fmaxf(xx + yy + zz, 1e-30f);
-    const float rinv = rsqrtf(r2);
-    const float rinv2 = rinv * rinv;
-    const float rinv3 = rinv * rinv2;
-    const float rinv5 = rinv3 * rinv2;
-    // S d with S = [[Sxx,Sxy,Szx],[Sxy,Syy,Syz],[Szx,Syz,Szz]]
-    const float Sx = fmaf(C.x, dx, fmaf(C.w, dy, E.y * dz));
-    const float Sy = fmaf(C.w, dx, fmaf(C.y, dy, E.x * dz));
-    const float Sz = fmaf(E.y, dx, fmaf(E.x, dy, C.z * dz));
-    const float u = fmaf(dx, Sx, fmaf(dy, Sy, dz * Sz));
-    const float Dd = fmaf(B.x, dx, fmaf(B.y, dy, B.z * dz));
-    const float ur2 = u * rinv2;
-    float g = fmaf(A.w, rinv3, rinv5 * fmaf(3.f, Dd, 15.f * ur2));
-    float ph = fmaf(A.w, rinv, rinv3 * fmaf(3.f, ur2, Dd));
-    const float c3 = -rinv3, c5 = -6.f * rinv5;
-    float gx = fmaf(c5, Sx, c3 * B.x);
-    float gy = fmaf(c5, Sy, c3 * B.y);
-    float gz = fmaf(c5, Sz, c3 * B.z);
+    const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+    // Normalised form: the moments are contracted with the unit vector
+    // n = d / r and scaled by powers of s = 1/r, so every intermediate is
+    // bounded by n (a/r)^k -- escaped electrons millions of um away would
+    // otherwise overflow T(d,d,d) ~ |T| r^3 while 1/r^7 underflows.
+    const float s = rsqrtf(r2), s2 = s * s;
+    const float nx = dx * s, ny = dy * s, nz = dz * s;
+    // S n with S = [[Sxx,Sxy,Szx],[Sxy,Syy,Syz],[Szx,Syz,Szz]]
+    const float Sx = fmaf(C.x, nx, fmaf(C.w, ny, E.y * nz));
+    const float Sy = fmaf(C.w, nx, fmaf(C.y, ny, E.x * nz));
+    const float Sz = fmaf(E.y, nx, fmaf(E.x, ny, C.z * nz));
+    const float u = fmaf(nx, Sx, fmaf(ny, Sy, nz * Sz));
+    const float Dn = fmaf(B.x, nx, fmaf(B.y, ny, B.z * nz));
+    // r^2 (-grad phi) = gp n - s D - 6 s^2 S n - 7.5 s^3 T(., n, n),
+    // gp = Q + 3 s D.n + 15 s^2 n.S.n + 17.5 s^3 T(n,n,n);
+    // r phi = Q + s D.n + 3 s^2 n.S.n + 2.5 s^3 T(n,n,n)
+    float gp = fmaf(s, fmaf(3.f, Dn, 15.f * s * u), A.w);
+    float php = fmaf(s, fmaf(3.f * s, u, Dn), A.w);
+    const float c5 = -6.f * s2;
+    float gx = fmaf(c5, Sx, -s * B.x);
+    float gy = fmaf(c5, Sy, -s * B.y);
+    float gz = fmaf(c5, Sz, -s * B.z);
     if (ORDER >= 3) {
       const float4 T1 = cl[4], T2 = cl[5];
       // T order: xxx = E.z, yyy = E.w, zzz = T1.x, xxy = T1.y, xxz = T1.z,
       // xyy = T1.w, yyz = T2.x, xzz = T2.y, yzz = T2.z, xyz = T2.w
-      const float x2 = dx + dx, y2 = dy + dy;
-      const float xy2 = x2 * dy, xz2 = x2 * dz, yz2 = y2 * dz;
+      const float xx = nx * nx, yy = ny * ny, zz = nz * nz;
+      const float x2 = nx + nx, y2 = ny + ny;
+      const float xy2 = x2 * ny, xz2 = x2 * nz, yz2 = y2 * nz;
       const float Tx = fmaf(E.z, xx, fmaf(T1.w, yy, fmaf(T2.y, zz, fmaf(T1.y, xy2, fmaf(T1.z, xz2, T2.w * yz2)))));
       const float Ty = fmaf(T1.y, xx, fmaf(E.w, yy, fmaf(T2.z, zz, fmaf(T1.w, xy2, fmaf(T2.w, xz2, T2.x * yz2)))));
       const float Tz = fmaf(T1.z, xx, fmaf(T2.x, yy, fmaf(T1.x, zz, fmaf(T2.w, xy2, fmaf(T2.y, xz2, T2.z * yz2)))));
-      const float T3 = fmaf(dx, Tx, fmaf(dy, Ty, dz * Tz));
-      const float rinv7 = rinv5 * rinv2;
-      g = fmaf(17.5f * rinv7, T3 * rinv2, g);
-      ph = fmaf(2.5f * rinv7, T3, ph);
-      const float c7 = -7.5f * rinv7;
+      const float T3 = fmaf(nx, Tx, fmaf(ny, Ty, nz * Tz));
+      const float s3 = s2 * s;
+      gp = fmaf(17.5f * s3, T3, gp);
+      php = fmaf(2.5f * s3, T3, php);
+      const float c7 = -7.5f * s3;
       gx = fmaf(c7, Tx, gx);
       gy = fmaf(c7, Ty, gy);
       gz = fmaf(c7, Tz, gz);
     }
-    fx += fmaf(g, dx, gx);
-    fy += fmaf(g, dy, gy);
-    fz += fmaf(g, dz, gz);
-    pa += ph;
-    pi = fmaf(B.w, rinv, pi);
+    fx = fmaf(s2, fmaf(gp, nx, gx), fx);
+    fy = fmaf(s2, fmaf(gp, ny, gy), fy);
+    fz = fmaf(s2, fmaf(gp, nz, gz), fz);
+    pa = fmaf(s, php, pa);
+    pi = fmaf(B.w, s, pi);
   }
   __syncwarp();
   kahan_add(acc.sx, acc.cx, fx);
@@ -684,6 +688,7 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.mom3, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.geom, (size_t)cap);
+  rc |= realloc_dev(&mb.lvl_list, (size_t)cap);
   return rc;
 }
 
@@ -698,12 +703,14 @@ int mixed_alloc_particles(MixedBuffers& mb, int n) {
   rc |= realloc_dev(&mb.groups, (size_t)n);
   rc |= realloc_dev(&mb.stack, (size_t)mb.grid_warps * kStackCap);
   rc |= realloc_dev(&mb.control, 4);
+  rc |= realloc_dev(&mb.lvl, 3 * (size_t)kLevelSlots);
   return rc;
 }
 
 void mixed_free(MixedBuffers& mb) {
   void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
-                  mb.mom3, mb.geom, mb.xs, mb.groups, mb.stack, mb.control};
+                  mb.mom3, mb.geom, mb.xs, mb.groups, mb.stack, mb.control,
+                  mb.lvl_list, mb.lvl};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   mb = MixedBuffers();
@@ -722,6 +729,8 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
   m.xs = mb.xs;
   m.groups = mb.groups;
   m.n_groups = mb.control + 2;
+  m.lvl_list = mb.lvl_list;
+  m.lvl = mb.lvl;
   return m;
 }
 

@@ -22,6 +22,8 @@ struct MixedBuffers {
   float4* geom = nullptr;
   double4* xs = nullptr;
   int2* groups = nullptr;
+  int32_t* lvl_list = nullptr; // per node: twigs by level (upward pass)
+  int32_t* lvl = nullptr;      // per level: count, offset, cursor
   int32_t* stack = nullptr;    // per resident warp: kStackCap node indices
   int32_t* control = nullptr;  // [0] group cursor, [1] max stack depth, [2] groups
   int grid_warps = 0;
