@@ -501,8 +501,11 @@ def run_ensemble(args, rank, world, dist):
     if args.tune:
         space = [tune.Candidate(t, e, 8, 3, g) for t in (0.20, 0.22, 0.24, 0.26, 0.28, 0.30)
                  for e in (0.0, 3e-6, 1e-5, 3e-5) for g in (3, 4)]
-        best, trials = tune.autotune(ens, dt, space=space, target=1e-4, audit=32768,
-                                     physics=phys, model=(params, stats))
+        # 1024 audited targets per cloud; margin 0.8 leaves room for the state
+        # to drift during the timed steps
+        best, trials = tune.autotune(ens, dt, space=space, target=1e-4, margin=0.8,
+                                     audit=1024 * args.clouds, physics=phys,
+                                     model=(params, stats))
         if best is not None:
             tuned = {**{k: getattr(best.cand, k) for k in ("theta", "eta", "bucket",
                                                            "order", "blocks_per_sm")},
@@ -563,8 +566,10 @@ def run_ensemble(args, rank, world, dist):
             with api.TreeForce(ne, b - a - ne, cfg) as tc:
                 tc.set_stream(stream.cuda_stream)
                 tc.set_tuning(args.bucket, 4, args.order)
-                tc.mac_set_model(params, stats)
-                tc.mac_config(args.eta if tuned is None else tuned["eta"], 0.05, 0.9)
+                eta_c = args.eta if tuned is None else tuned["eta"]
+                if eta_c > 0:
+                    tc.mac_set_model(params, stats)
+                    tc.mac_config(eta_c, 0.05, 0.9)
                 tc.load_state(sl["x"][:ne], sl["v"][:ne], sl["f"][:ne], sl["x"][ne:],
                               sl["v"][ne:], sl["f"][ne:])
                 tc.step(dt, 1)
@@ -592,7 +597,8 @@ def run_ensemble(args, rank, world, dist):
         "config": {"workload": f"{args.clouds} clouds, N log-uniform in [8192, 131072] "
                                f"(total {n}), n0 log-uniform in [1e14, 1e16] m^-3, "
                                f"T_e uniform in [10, 200] K, T_i = 1 mK, dt = 1e-11 s",
-                   "n_particles": n, "theta": ens.config.theta, "mac": args.mac,
+                   "n_particles": n, "theta": ens.config.theta,
+                   "mac": "learned" if ens.config.mac == api.MAC_LEARNED else "fixed",
                    "eta": args.eta if tuned is None else tuned["eta"], "tuned": tuned,
                    "l2": "inputs larger than L2"},
         "clocks": clk, "gpu_launches": t_after.launches - t_before.launches,
