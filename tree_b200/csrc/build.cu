@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kRsThreads)
 // 8-bit passes, so the result ends in the primary buffers.
 template <class K>
 int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
-               int32_t* hist, int32_t* partial, cudaStream_t st) {
+               int32_t* hist, int32_t* partial, cudaStream_t st, int first_byte) {
   if (n <= 1) return 0;
   int launches = 0;
   int nb = radix_blocks(n);
@@ -460,7 +460,7 @@ int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
   uint32_t* vin = vals;
   K* kout = keys_alt;
   uint32_t* vout = vals_alt;
-  for (int pass = 0; pass < (int)sizeof(K); ++pass) {
+  for (int pass = first_byte; pass < (int)sizeof(K); ++pass) {
     int shift = pass * 8;
     k_rs_hist<K><<<nb, kRsThreads, 0, st>>>(kin, n, shift, hist);
     launches += 2 + exclusive_scan(hist, hist, kRsBins * nb, partial, false, st);
@@ -473,9 +473,35 @@ int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
 }
 
 template int radix_sort<uint64_t>(uint64_t*, uint32_t*, uint64_t*, uint32_t*, int,
-                                  int32_t*, int32_t*, cudaStream_t);
+                                  int32_t*, int32_t*, cudaStream_t, int);
 template int radix_sort<key128>(key128*, uint32_t*, key128*, uint32_t*, int,
-                                int32_t*, int32_t*, cudaStream_t);
+                                int32_t*, int32_t*, cudaStream_t, int);
+
+// After a stable sort on the high 64 key bits, runs of equal high words
+// (particles closer than about 2^-21 of the root box: co-located e-i pairs,
+// tight pairs) are put in full-key order by one thread per run.  Runs are
+// short (typically 2), and equal full keys keep their stable order.
+__global__ void k_tie_fix(key128* keys, uint32_t* vals, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p + 1 >= n) return;
+  const uint64_t h = (uint64_t)(keys[p] >> 64);
+  if ((uint64_t)(keys[p + 1] >> 64) != h) return;
+  if (p > 0 && (uint64_t)(keys[p - 1] >> 64) == h) return;  // not the run start
+  int e = p + 1;
+  while (e < n && (uint64_t)(keys[e] >> 64) == h) ++e;
+  for (int i = p + 1; i < e; ++i) {  // insertion sort on the low word
+    const key128 k = keys[i];
+    const uint32_t v = vals[i];
+    int j = i - 1;
+    while (j >= p && keys[j] > k) {
+      keys[j + 1] = keys[j];
+      vals[j + 1] = vals[j];
+      --j;
+    }
+    keys[j + 1] = k;
+    vals[j + 1] = v;
+  }
+}
 
 // ------------------------------------------------------------ topology ----
 __device__ __forceinline__ int clz128(key128 x) {
@@ -1013,13 +1039,21 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
 // child is final when its parent's level runs (a launch boundary orders
 // them), so no arrival counters or fences are needed and the critical path
 // is one round of loads per level.
+// Counts per level go through a block-local histogram: ~43 global counters
+// hit by every twig would serialise on their atomics.
 __global__ void k_level_count(const int32_t* __restrict__ node_pt,
                               const int8_t* __restrict__ node_level,
                               const int32_t* __restrict__ bounds, int cap,
                               int32_t* lvl) {
+  __shared__ int32_t h[kLevelSlots];
+  for (int l = threadIdx.x; l < kLevelSlots; l += blockDim.x) h[l] = 0;
+  __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m && node_pt[i] < 0) atomicAdd(&lvl[node_level[i]], 1);
+  if (i < m && node_pt[i] < 0) atomicAdd(&h[node_level[i]], 1);
+  __syncthreads();
+  for (int l = threadIdx.x; l < kLevelSlots; l += blockDim.x)
+    if (h[l]) atomicAdd(&lvl[l], h[l]);
 }
 
 __global__ void k_level_offsets(int32_t* lvl) {
@@ -1032,15 +1066,25 @@ __global__ void k_level_offsets(int32_t* lvl) {
   }
 }
 
+// Places each twig in its level's list: a rank inside the block (shared
+// atomics), then one global reservation per level and block.
 __global__ void k_level_scatter(const int32_t* __restrict__ node_pt,
                                 const int8_t* __restrict__ node_level,
                                 const int32_t* __restrict__ bounds, int cap,
                                 int32_t* lvl, int32_t* list) {
+  __shared__ int32_t h[kLevelSlots], base[kLevelSlots];
+  for (int l = threadIdx.x; l < kLevelSlots; l += blockDim.x) h[l] = 0;
+  __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m || node_pt[i] >= 0) return;
-  const int l = node_level[i];
-  list[lvl[kLevelSlots + l] + atomicAdd(&lvl[2 * kLevelSlots + l], 1)] = i;
+  const bool twig = i < m && node_pt[i] < 0;
+  const int l = twig ? node_level[i] : 0;
+  const int rank = twig ? atomicAdd(&h[l], 1) : 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < kLevelSlots; k += blockDim.x)
+    base[k] = h[k] ? lvl[kLevelSlots + k] + atomicAdd(&lvl[2 * kLevelSlots + k], h[k]) : 0;
+  __syncthreads();
+  if (twig) list[base[l] + rank] = i;
 }
 
 __global__ void k_net_level(int level, const Geom* __restrict__ geom, double theta,
@@ -1138,8 +1182,11 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   const int nlev = ens.nseg > 0 ? ens.nlev : kMaxLevel;
   k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, ens, b.keys, b.vals);
   launches += 3;
+  // sort on the high 64 bits (8 passes), then order the rare ties fully
   launches += radix_sort(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
-                         b.sort_hist, b.scan_partial, st);
+                         b.sort_hist, b.scan_partial, st, 8);
+  k_tie_fix<<<gb, T, 0, st>>>(b.keys, b.vals, n);
+  ++launches;
   k_common_levels<<<gb, T, 0, st>>>(b.keys, n, top, nlev, b.L, b.err);
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);

@@ -77,9 +77,10 @@ int exclusive_scan(const int32_t* in, int32_t* out, int n, int32_t* partial,
                    bool write_total, cudaStream_t st);
 // Stable LSD radix sort of (keys, vals) by all bytes of the key (8 passes for
 // uint64_t keys, 16 for key128); the result ends in the primary buffers.
+// first_byte > 0 skips the low bytes (an even number of passes must remain).
 template <class K>
 int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
-               int32_t* hist, int32_t* partial, cudaStream_t st);
+               int32_t* hist, int32_t* partial, cudaStream_t st, int first_byte = 0);
 // Builds the trees for positions x (AoS, electrons first).  mode 0: one tree
 // per species with the reference's one-level moments (parity path); mode 1:
 // one combined tree with net-charge moments and target groups (mixed path).
