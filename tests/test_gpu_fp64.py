@@ -134,6 +134,33 @@ def test_ragged_and_degenerate_species(device_lib, oracle_lib, n_el, n_ion):
         _check_tree(d["tree"][1], ti, cfg.theta)
 
 
+def _stretched_cluster(n_el, n_ion, width, seed):
+    """A cluster `width` wide with one particle of each species ~1e3 away: the
+    root box is 1e8 cluster widths across, so hundreds of keys share their
+    high 64 bits (21 levels) and the build takes its full-key sort."""
+    rng = np.random.default_rng(seed)
+    xe = rng.standard_normal((n_el, 3)) * width
+    xi = rng.standard_normal((n_ion, 3)) * width + 0.3 * width
+    xe[0] = (1e3, -2e3, 5e2)
+    xi[0] = (-1e3, 1e3, 0.0)
+    return xe, xi
+
+
+def test_tight_cluster_in_a_stretched_box(device_lib, oracle_lib):
+    xe, xi = _stretched_cluster(600, 500, 1e-5, 11)
+    cfg = _cfg(theta=0.5)
+    d = _device_force(xe, xi, cfg)
+    r = oracle.force(xe, xi, _oracle_params(cfg))
+    f = np.vstack([d["f_el"], d["f_ion"]])
+    fr = np.vstack([r["f_el"], r["f_ion"]])
+    assert _force_err(f, fr).max() <= FTOL
+    np.testing.assert_array_equal(d["rdf_ei"], r["rdf_ei"])
+    te, _ = oracle.tree_dump(xe, -1)
+    ti, _ = oracle.tree_dump(xi, +1)
+    _check_tree(d["tree"][0], te, cfg.theta)
+    _check_tree(d["tree"][1], ti, cfg.theta)
+
+
 def test_rdf_accumulates_across_calls(device_lib):
     xe, xi = _displaced(2000, 9)
     with api.TreeForce(len(xe), len(xi), _cfg()) as tf:

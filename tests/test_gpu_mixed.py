@@ -104,6 +104,28 @@ def test_mixed_ragged_species(device_lib, n_el, n_ion):
         assert np.sqrt(np.mean(_rel(f, fd) ** 2)) < 1e-4
 
 
+def test_mixed_tight_cluster_in_a_stretched_box(device_lib):
+    """Hundreds of keys share their high 64 bits (a cluster 0.3 um wide in a
+    box 3e6 um wide), which takes the build's full-key sort: the forces meet
+    the accuracy bar and do not depend on the input order within a species."""
+    rng = np.random.default_rng(12)
+    xe = rng.standard_normal((300, 3)) * 0.3
+    xi = rng.standard_normal((300, 3)) * 0.3
+    xe[0] = (1e6, -2e6, 5e5)
+    xi[0] = (-1e6, 1e6, 0.0)
+    pe = np.concatenate([[0], 1 + rng.permutation(299)])
+    pi = np.concatenate([[0], 1 + rng.permutation(299)])
+    with api.TreeForce(300, 300, _mixed(0.5)) as tf:
+        f_el, f_ion, _, _ = tf.force(xe, xi)
+        fd, _ = tf.direct(np.arange(600))
+        g_el, g_ion, _, _ = tf.force(xe[pe], xi[pi])
+    f = np.vstack([f_el, f_ion])
+    assert np.all(np.isfinite(f))
+    assert np.sqrt(np.mean(_rel(f, fd) ** 2)) < 1e-4
+    np.testing.assert_array_equal(g_el, f_el[pe])
+    np.testing.assert_array_equal(g_ion, f_ion[pi])
+
+
 def test_mixed_step_energy_drift_close_to_fp64(device_lib):
     """50 steps of dt = 1e-11 s: the mixed path's relative energy drift stays
     within a small multiple of the FP64 path's."""

@@ -480,15 +480,25 @@ template int radix_sort<key128>(key128*, uint32_t*, key128*, uint32_t*, int,
 // After a stable sort on the high 64 key bits, runs of equal high words
 // (particles closer than about 2^-21 of the root box: co-located e-i pairs,
 // tight pairs) are put in full-key order by one thread per run.  Runs are
-// short (typically 2), and equal full keys keep their stable order.
-__global__ void k_tie_fix(key128* keys, uint32_t* vals, int n) {
+// short (typically 2), and equal full keys keep their stable order.  A run
+// longer than kTieSerial (a tight cluster in a box stretched by a far
+// outlier) is left alone and raises *long_run, which makes k_sort_block sort
+// the whole array by the full key; that sort is stable, so the result is the
+// same order either way.
+constexpr int kTieSerial = 64;
+
+__global__ void k_tie_fix(key128* keys, uint32_t* vals, int n, int32_t* long_run) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p + 1 >= n) return;
   const uint64_t h = (uint64_t)(keys[p] >> 64);
   if ((uint64_t)(keys[p + 1] >> 64) != h) return;
   if (p > 0 && (uint64_t)(keys[p - 1] >> 64) == h) return;  // not the run start
   int e = p + 1;
-  while (e < n && (uint64_t)(keys[e] >> 64) == h) ++e;
+  while (e < n && e - p <= kTieSerial && (uint64_t)(keys[e] >> 64) == h) ++e;
+  if (e - p > kTieSerial) {
+    *long_run = 1;
+    return;
+  }
   for (int i = p + 1; i < e; ++i) {  // insertion sort on the low word
     const key128 k = keys[i];
     const uint32_t v = vals[i];
@@ -500,6 +510,96 @@ __global__ void k_tie_fix(key128* keys, uint32_t* vals, int n) {
     }
     keys[j + 1] = k;
     vals[j + 1] = v;
+  }
+}
+
+// Stable LSD radix sort of all 16 key bytes by ONE block of kSbThreads, run
+// only when *gate != 0 (otherwise the launch returns at once): the rare
+// fallback of the high-word sort, slow (one SM streams the array 32 times)
+// but a single launch in the common case.  Same order rule as k_rs_scatter:
+// per tile, warp w owns items [w*kSbItems*32, (w+1)*kSbItems*32).
+constexpr int kSbThreads = 1024;
+constexpr int kSbWarps = kSbThreads / 32;
+constexpr int kSbItems = 4;
+constexpr int kSbTile = kSbThreads * kSbItems;
+
+__global__ void __launch_bounds__(kSbThreads)
+    k_sort_block(key128* keys, uint32_t* vals, key128* keys_alt, uint32_t* vals_alt,
+                 int n, const int32_t* gate) {
+  if (*gate == 0) return;
+  __shared__ int32_t whist[kSbWarps][kRsBins];
+  __shared__ int32_t base_s[kRsBins];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  key128* kin = keys;
+  uint32_t* vin = vals;
+  key128* kout = keys_alt;
+  uint32_t* vout = vals_alt;
+  for (int pass = 0; pass < 16; ++pass) {
+    const int shift = 8 * pass;
+    for (int b = threadIdx.x; b < kRsBins; b += blockDim.x) base_s[b] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      atomicAdd(&base_s[(int)((kin[i] >> shift) & 0xff)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0;
+      for (int b = 0; b < kRsBins; ++b) {
+        const int t = base_s[b];
+        base_s[b] = run;
+        run += t;
+      }
+    }
+    __syncthreads();
+    for (int64_t tile = 0; tile < n; tile += kSbTile) {
+      for (int b = threadIdx.x; b < kRsBins; b += blockDim.x)
+#pragma unroll
+        for (int ww = 0; ww < kSbWarps; ++ww) whist[ww][b] = 0;
+      __syncthreads();
+      const int64_t wbase = tile + (int64_t)w * (32 * kSbItems);
+      key128 k[kSbItems];
+      uint32_t v[kSbItems];
+      int32_t loc[kSbItems];
+#pragma unroll
+      for (int j = 0; j < kSbItems; ++j) {
+        const int64_t i = wbase + j * 32 + lane;
+        const bool ok = i < n;
+        k[j] = ok ? kin[i] : (key128)0;
+        v[j] = ok ? vin[i] : 0u;
+        const int d = ok ? (int)((k[j] >> shift) & 0xff) : kRsBins;  // sentinel bin
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int rank = __popc(peers & lt);
+        const int32_t before = ok ? whist[w][d] : 0;
+        __syncwarp();
+        if (ok && rank == 0) whist[w][d] = before + __popc(peers);
+        __syncwarp();
+        loc[j] = ok ? before + rank : -1;
+      }
+      __syncthreads();
+      // exclusive prefix over warps per digit; the tile's totals advance base_s
+      for (int b = threadIdx.x; b < kRsBins; b += blockDim.x) {
+        int32_t run = 0;
+#pragma unroll
+        for (int ww = 0; ww < kSbWarps; ++ww) {
+          const int32_t t = whist[ww][b];
+          whist[ww][b] = run + base_s[b];
+          run += t;
+        }
+        base_s[b] += run;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < kSbItems; ++j) {
+        if (loc[j] < 0) continue;
+        const int d = (int)((k[j] >> shift) & 0xff);
+        const int64_t pos = (int64_t)whist[w][d] + loc[j];
+        kout[pos] = k[j];
+        vout[pos] = v[j];
+      }
+      __syncthreads();
+    }
+    key128* tk = kin; kin = kout; kout = tk;
+    uint32_t* tv = vin; vin = vout; vout = tv;
   }
 }
 
@@ -1105,11 +1205,64 @@ __global__ void k_net_level(int level, const Geom* __restrict__ geom, double the
 // ------------------------------------------------------------ groups ----
 // Target groups of the mixed walk: maximal cells holding at most kGroupMax
 // particles, with consecutive small siblings packed together up to kGroupMax.
-// Every group is a contiguous sorted range inside one parent cell, so its
-// bounding box stays compact.  Group order is not deterministic (atomic
-// append); the content of every group is.
+// Every group is a contiguous sorted range inside one parent cell.  Packing
+// is limited to parents at most kGroupSlack + 1 levels above the cloud's
+// typical group level (the particle-weighted median level of its maximal
+// cells): the sparse octants of a large parent -- escaped electrons around a
+// dense core -- would otherwise share one group whose bounding box spans the
+// parent and contains the core, and that one warp opens the whole tree.
+// Group order is not deterministic (atomic append); the content of every
+// group is.
+constexpr int kGroupSlack = 3;
+
+// Particle-weighted histogram of the levels of the maximal cells holding at
+// most kGroupMax particles, per cloud: glvl[seg * kLevelSlots + level].
+__global__ void k_group_levels(const int32_t* __restrict__ bounds, int cap,
+                               const int32_t* __restrict__ node_parent,
+                               const int8_t* __restrict__ node_level, MixedNodes mx,
+                               Ensemble ens, int32_t* glvl) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = -1, w = 0;
+  if (t < m) {
+    const int cnt = mx.count[t];
+    const int par = node_parent[t];
+    if (cnt <= kGroupMax && (par < 0 || mx.count[par] > kGroupMax)) {
+      const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[t]) : 0;
+      slot = seg * kLevelSlots + node_level[t];
+      w = cnt;
+    }
+  }
+  // one atomic per distinct slot per warp (all lanes reach this point)
+  const unsigned peers = __match_any_sync(0xffffffffu, slot);
+  const int sum = __reduce_add_sync(peers, w);
+  if (slot >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&glvl[slot], sum);
+}
+
+// Per cloud: the lowest level at which siblings may be packed, stored in the
+// last slot of the cloud's histogram row (levels stay below kLevelSlots - 1).
+__global__ void k_group_cut(int32_t* glvl, int nseg) {
+  const int seg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (seg >= nseg) return;
+  int32_t* h = glvl + (int64_t)seg * kLevelSlots;
+  int64_t tot = 0;
+  for (int l = 0; l < kLevelSlots - 1; ++l) tot += h[l];
+  int64_t run = 0;
+  int med = 0;
+  for (int l = 0; l < kLevelSlots - 1; ++l) {
+    run += h[l];
+    if (2 * run >= tot) {
+      med = l;
+      break;
+    }
+  }
+  h[kLevelSlots - 1] = med > kGroupSlack ? med - kGroupSlack : 0;
+}
+
 __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
-                         const int32_t* __restrict__ node_parent, MixedNodes mx,
+                         const int32_t* __restrict__ node_parent,
+                         const int8_t* __restrict__ node_level, MixedNodes mx,
+                         Ensemble ens, const int32_t* __restrict__ glvl,
                          int2* groups, int32_t* n_groups) {
   int m = bounds[2] < cap ? bounds[2] : cap;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1121,6 +1274,8 @@ __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
     return;
   }
   if (cnt <= kGroupMax || cnt == 1) return;
+  const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[t]) : 0;
+  const bool pack = node_level[t] + 1 >= glvl[seg * kLevelSlots + kLevelSlots - 1];
   const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)t);
   const int4 k0 = kk[0], k1 = kk[1];
   const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
@@ -1130,21 +1285,18 @@ __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
     const int c = kv[j];
     if (c < 0) continue;
     const int cc = mx.count[c];
-    if (cc > kGroupMax) {  // recursed into by its own thread: closes the run
+    // a large child is recursed into by its own thread; below a large
+    // parent every small child is a group of its own: both close the run
+    if (cc > kGroupMax || (!pack && run_cnt > 0) ||
+        (run_cnt > 0 && run_cnt + cc > kGroupMax)) {
       if (run_cnt > 0) {
         int g = atomicAdd(n_groups, 1);
         groups[g] = make_int2(run_first, run_cnt);
       }
       run_first = -1;
       run_cnt = 0;
-      continue;
     }
-    if (run_cnt > 0 && run_cnt + cc > kGroupMax) {
-      int g = atomicAdd(n_groups, 1);
-      groups[g] = make_int2(run_first, run_cnt);
-      run_first = -1;
-      run_cnt = 0;
-    }
+    if (cc > kGroupMax) continue;
     if (run_cnt == 0) run_first = mx.first[c];
     run_cnt += cc;
   }
@@ -1182,11 +1334,15 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   const int nlev = ens.nseg > 0 ? ens.nlev : kMaxLevel;
   k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, ens, b.keys, b.vals);
   launches += 3;
-  // sort on the high 64 bits (8 passes), then order the rare ties fully
+  // sort on the high 64 bits (8 passes), then order the rare ties fully;
+  // a long tie run switches on the one-block full sort (which exits otherwise)
   launches += radix_sort(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
                          b.sort_hist, b.scan_partial, st, 8);
-  k_tie_fix<<<gb, T, 0, st>>>(b.keys, b.vals, n);
-  ++launches;
+  cudaMemsetAsync(b.bounds + 4, 0, sizeof(int32_t), st);
+  k_tie_fix<<<gb, T, 0, st>>>(b.keys, b.vals, n, b.bounds + 4);
+  k_sort_block<<<1, kSbThreads, 0, st>>>(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
+                                         b.bounds + 4);
+  launches += 2;
   k_common_levels<<<gb, T, 0, st>>>(b.keys, n, top, nlev, b.L, b.err);
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);
@@ -1223,10 +1379,18 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
       ++launches;
     }
   }
+  // the level lists of the upward pass are free again: a single cloud keeps
+  // its group-level histogram there, an ensemble has one row per cloud
+  const int nsg = ens.nseg > 0 ? ens.nseg : 1;
+  int32_t* glvl = ens.nseg > 0 ? ens.glvl : b.mx.lvl;
+  cudaMemsetAsync(glvl, 0, sizeof(int32_t) * kLevelSlots * (size_t)nsg, st);
+  k_group_levels<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_parent, b.node_level, b.mx,
+                                     ens, glvl);
+  k_group_cut<<<(nsg + 127) / 128, 128, 0, st>>>(glvl, nsg);
   cudaMemsetAsync(b.mx.n_groups, 0, sizeof(int32_t), st);
-  k_groups<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_parent, b.mx, b.mx.groups,
-                               b.mx.n_groups);
-  launches += 2;
+  k_groups<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_parent, b.node_level, b.mx, ens,
+                               glvl, b.mx.groups, b.mx.n_groups);
+  launches += 5;
   if (ens.nseg > 0) {
     k_roots<<<(ens.nseg + 31) / 32, 32, 0, st>>>(b.off, ens.start, ens.nseg, ens.roots);
     launches += 1;

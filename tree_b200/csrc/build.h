@@ -39,6 +39,7 @@ struct Ensemble {
   const int32_t* start = nullptr;     // device, nseg + 1
   const int32_t* elec_end = nullptr;  // device, nseg
   int32_t* roots = nullptr;           // device, nseg
+  int32_t* glvl = nullptr;            // device, nseg x kLevelSlots (target groups)
 };
 
 struct BuildBuffers {
@@ -65,7 +66,7 @@ struct BuildBuffers {
   // small
   uint64_t* bbox;       // 6 per segment (>= 2 segments)
   Geom* geom;           // per segment (>= 2)
-  int32_t* bounds;      // 4: 0, M_e, M (clamped to cap), M (untruncated)
+  int32_t* bounds;      // 5: 0, M_e, M (clamped to cap), M (untruncated), long-tie flag
   int32_t* err;
   MixedNodes mx;
   Ensemble ens;

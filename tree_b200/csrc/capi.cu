@@ -105,6 +105,7 @@ struct tree_gpu_handle {
   int32_t* ens_start = nullptr;     // device, nseg + 1
   int32_t* ens_elec_end = nullptr;  // device, nseg
   int32_t* ens_roots = nullptr;     // device, nseg
+  int32_t* ens_glvl = nullptr;      // device, nseg x kLevelSlots
   float4* cloud_pk = nullptr;       // device, 2 per cloud
   uint8_t* ion_flag = nullptr;      // device, per particle (ensembles)
   double* cloud_sums = nullptr;     // device, 6 per cloud
@@ -200,7 +201,7 @@ int alloc_all(tree_gpu_handle* h) {
   if ((rc = dalloc(h, &b.scan_partial, (size_t)sp + 1))) return rc;
   if ((rc = dalloc(h, &b.bbox, 12))) return rc;
   if ((rc = dalloc(h, &b.geom, 2))) return rc;
-  if ((rc = dalloc(h, &b.bounds, 4))) return rc;
+  if ((rc = dalloc(h, &b.bounds, 5))) return rc;
   if ((rc = dalloc(h, &b.err, 1))) return rc;
   if ((rc = dalloc(h, &h->rdf, 2 * (size_t)tg::kRdfBins))) return rc;
   if ((rc = dalloc(h, &h->counters, 4))) return rc;
@@ -225,8 +226,8 @@ void free_all(tree_gpu_handle* h) {
                   h->diag, h->mlp_params, h->mlp_stats, h->mlp_packed,
                   h->smp_feats, h->smp_labels, h->smp_extra, h->smp_count,
                   h->series, h->series_count, h->rdf64, h->ens_start,
-                  h->ens_elec_end, h->ens_roots, h->cloud_pk, h->ion_flag,
-                  h->cloud_sums};
+                  h->ens_elec_end, h->ens_roots, h->ens_glvl, h->cloud_pk,
+                  h->ion_flag, h->cloud_sums};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   tg::mixed_free(h->mb);
@@ -1046,6 +1047,7 @@ int tree_gpu_ensemble_create(const tree_gpu_params* params, int32_t ncloud,
     if ((rc = dalloc(h, &h->ens_start, (size_t)ncloud + 1))) break;
     if ((rc = dalloc(h, &h->ens_elec_end, (size_t)ncloud))) break;
     if ((rc = dalloc(h, &h->ens_roots, (size_t)ncloud))) break;
+    if ((rc = dalloc(h, &h->ens_glvl, (size_t)ncloud * tg::kLevelSlots))) break;
     if ((rc = dalloc(h, &h->cloud_pk, 2 * (size_t)ncloud))) break;
     if ((rc = dalloc(h, &h->ion_flag, ion.size()))) break;
     if ((rc = dalloc(h, &h->cloud_sums, 6 * (size_t)ncloud))) break;
@@ -1064,6 +1066,7 @@ int tree_gpu_ensemble_create(const tree_gpu_params* params, int32_t ncloud,
     b.ens.start = h->ens_start;
     b.ens.elec_end = h->ens_elec_end;
     b.ens.roots = h->ens_roots;
+    b.ens.glvl = h->ens_glvl;
     ++h->epoch;
   } while (0);
   if (rc) {
