@@ -499,6 +499,9 @@ def run_ensemble(args, rank, world, dist):
     torch.cuda.synchronize()
     tuned = None
     if args.tune:
+        # the force error grows while the electrons leave their ions (about
+        # ten steps of 1e-11 s): tune on a state past that transient
+        ens.step(dt, 10)
         space = [tune.Candidate(t, e, 8, 3, g) for t in (0.20, 0.22, 0.24, 0.26, 0.28, 0.30)
                  for e in (0.0, 3e-6, 1e-5, 3e-5) for g in (3, 4)]
         # 1024 audited targets per cloud; margin 0.8 leaves room for the state
