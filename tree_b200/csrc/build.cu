@@ -1279,7 +1279,21 @@ __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
   const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)t);
   const int4 k0 = kk[0], k1 = kk[1];
   const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+  // runs of consecutive small children are cut into balanced contiguous
+  // chunks of at most kGroupMax (a chunk may straddle two children, but it
+  // stays inside this cell)
   int run_first = -1, run_cnt = 0;
+  auto close_run = [&]() {
+    if (run_cnt <= 0) return;
+    const int k = (run_cnt + kGroupMax - 1) / kGroupMax;
+    const int g = atomicAdd(n_groups, k);
+    for (int i = 0; i < k; ++i) {
+      const int lo = (int)((int64_t)i * run_cnt / k), hi = (int)((int64_t)(i + 1) * run_cnt / k);
+      groups[g + i] = make_int2(run_first + lo, hi - lo);
+    }
+    run_first = -1;
+    run_cnt = 0;
+  };
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const int c = kv[j];
@@ -1287,23 +1301,12 @@ __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
     const int cc = mx.count[c];
     // a large child is recursed into by its own thread; below a large
     // parent every small child is a group of its own: both close the run
-    if (cc > kGroupMax || (!pack && run_cnt > 0) ||
-        (run_cnt > 0 && run_cnt + cc > kGroupMax)) {
-      if (run_cnt > 0) {
-        int g = atomicAdd(n_groups, 1);
-        groups[g] = make_int2(run_first, run_cnt);
-      }
-      run_first = -1;
-      run_cnt = 0;
-    }
+    if (cc > kGroupMax || !pack) close_run();
     if (cc > kGroupMax) continue;
     if (run_cnt == 0) run_first = mx.first[c];
     run_cnt += cc;
   }
-  if (run_cnt > 0) {
-    int g = atomicAdd(n_groups, 1);
-    groups[g] = make_int2(run_first, run_cnt);
-  }
+  close_run();
 }
 
 // ------------------------------------------------------------- driver ----

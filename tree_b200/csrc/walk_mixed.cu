@@ -41,6 +41,7 @@ constexpr int kMinBlocksPerSm = 3;  // 80 registers: 24 resident warps per SM
 
 constexpr int kCandRing = 64;     // power of two, > 31 + 32
 constexpr int kCellF4 = 6;        // float4 per staged far-field cell
+constexpr int kPartF4 = 5;        // float4 per staged source pair (4 used + pad)
 
 struct WarpSmem {
   int m2p[kM2pRing];
@@ -52,7 +53,11 @@ struct WarpSmem {
   // (Sxx, Syy, Szz, Sxy), (Syz, Szx, Txxx, Tyyy), (Tzzz, Txxy, Txxz, Txyy),
   // (Tyyz, Txzz, Tyzz, Txyz) -- S and T trace-free
   float4 cell[32 * kCellF4];
-  float4 part[32 * 2];   // (hi xyz, sorted index bits), (lo xyz, charge)
+  // staged sources in pairs, kPartF4 float4 per pair: sources 2b and 2b+1
+  // side by side, (nhx nhx' nhy nhy') (nhz nhz' idx idx') (nlx nlx' nly nly')
+  // (nlz nlz' q q'): negated hi / lo offsets from the group centre, sorted
+  // index bits, charge
+  float4 part[16 * kPartF4];
   // pair constants of the group's cloud: 1/lambda^2 (ee, ei, ii), 1/rs,
   // 1/lambda (ee, ei, ii)
   float pk[8];
@@ -235,6 +240,96 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
 }
 
 // ---------------------------------------------------------------- P2P ----
+// RDF count of one pair (bins in FP64 from the hi/lo offsets, so bin edges
+// match the FP64 path).  (ngx, ngy, ngz) / (nlx, nly, nlz): the source's
+// negated hi / lo offsets from the group centre.
+template <int PHYS>
+__device__ __forceinline__ void rdf_count(const MixedArgs& a, float r2, float ssign, int s,
+                                          float ngx, float ngy, float ngz, float nlx,
+                                          float nly, float nlz, float thx, float thy,
+                                          float thz, float tlx, float tly, float tlz,
+                                          int p_self, int tsp) {
+  const bool same = ssign == (tsp ? 1.f : -1.f);
+  const bool counted = PHYS == 1 ? s != p_self : (same ? r2 > 0.01f : true);
+  if (ssign != 0.f && counted && (!same || tsp == 1)) {
+    const double ex = ((double)thx + (double)ngx) + ((double)tlx + (double)nlx);
+    const double ey = ((double)thy + (double)ngy) + ((double)tly + (double)nly);
+    const double ez = ((double)thz + (double)ngz) + ((double)tlz + (double)nlz);
+    const double t = sqrt(ex * ex + ey * ey + ez * ez) * (same ? a.dx_ii_inv : a.dx_ei_inv);
+    if (t < (double)kRdfBins) {
+      int id = (int)t;
+      if (id >= 0 && id < kRdfBins) atomicAdd(&a.rdf[(same ? kRdfBins : 0) + id], 1u);
+    }
+  }
+}
+
+// One source against this lane's target with every case of the pair laws:
+// "special" pairs leave the plain Coulomb law -- the target itself (r = 0),
+// pairs inside the Kelbg core (exp(-x^2) still visible in FP32), and for the
+// reference laws same-species pairs inside the r^2 <= 0.01 cutoff and e-i
+// pairs where exp(-r/rs) is visible.
+template <int PHYS>
+__device__ __forceinline__ void p2p_one(const WarpSmem& sm, float r2, float dx, float dy,
+                                        float dz, float ssign, int s, int p_self, int tsp,
+                                        float& fx, float& fy, float& fz, float& pa,
+                                        float& pq) {
+  const bool same = ssign == (tsp ? 1.f : -1.f);
+  const float il2_same = PHYS == 1 ? (tsp ? sm.pk[2] : sm.pk[0]) : 0.f;
+  const float il_same = PHYS == 1 ? (tsp ? sm.pk[6] : sm.pk[4]) : 0.f;
+  const float il2_ei = sm.pk[1], il_ei = sm.pk[5], rs_inv = sm.pk[3];
+  bool special;
+  if (PHYS == 1) special = r2 * (same ? il2_same : il2_ei) < 40.f;
+  else special = same ? !(r2 > 0.01f) : r2 * (rs_inv * rs_inv) < 400.f;
+  float fs, ph;
+  if (!special) {
+    const float rinv = rsqrtf(r2);
+    fs = ssign * rinv * rinv * rinv;
+    ph = ssign * rinv;
+  } else {
+    fs = 0.f;
+    ph = 0.f;
+    if (PHYS == 1) {
+      if (s != p_self) {
+        const float il = same ? il_same : il_ei;
+        const float sqrtpi = 1.77245385f;
+        float ve;
+        if (r2 > 0.f) {
+          const float r = sqrtf(r2);
+          const float ri = 1.f / r;
+          const float x2 = r2 * il * il;
+          const float g = -expm1f(-x2);
+          fs = ssign * g * ri * ri * ri;
+          ve = g * ri + sqrtpi * erfcf(r * il) * il;
+        } else {
+          ve = sqrtpi * il;  // distinct particles on one point: V(0)
+        }
+        ph = ssign * ve;
+      }
+    } else if (!same) {
+      float ve;
+      if (r2 > 0.f) {
+        const float r = sqrtf(r2);
+        const float ri = 1.f / r;
+        const float e = expf(-r * rs_inv);
+        const float g = ri - e * (ri + rs_inv);
+        fs = ssign * g * ri * ri;
+        ve = (1.f - e) * ri;
+      } else {
+        ve = rs_inv;  // r -> 0 limit of (1 - exp(-r/rs))/r
+      }
+      ph = ssign * ve;
+    }  // same species inside the cutoff (and the target itself): nothing
+  }
+  fx = fmaf(fs, dx, fx);
+  fy = fmaf(fs, dy, fy);
+  fz = fmaf(fs, dz, fz);
+  pa += ph;
+  pq = fmaf(ssign, ph, pq);
+}
+
+// Pair interactions of up to 32 staged sources with this lane's target, two
+// sources per packed FP32 (f32x2) instruction.  The common pair is plain
+// Coulomb; a pair with a special member goes through p2p_one.
 template <int PHYS, bool RDF>
 __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
                                          const MixedArgs& a, double Gx,
@@ -243,106 +338,91 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
                                          float tly, float tlz, int p_self,
                                          int tsp, bool act, int lane,
                                          Acc& acc) {
-  if (lane < cnt) {
-    int s = sm.p2p[(head + lane) & (kP2pRing - 1)];
-    double4 xs = a.xs[s];
-    double rx = xs.x - Gx, ry = xs.y - Gy, rz = xs.z - Gz;
-    float hx = (float)rx, hy = (float)ry, hz = (float)rz;
-    sm.part[2 * lane] = make_float4(hx, hy, hz, __int_as_float(s));
-    sm.part[2 * lane + 1] =
-        make_float4((float)(rx - (double)hx), (float)(ry - (double)hy),
-                    (float)(rz - (double)hz), xs.w > 0.5 ? 1.f : -1.f);
-  }
-  __syncwarp();
-  const float tq = tsp ? 1.f : -1.f;  // target charge
-  // pair constants of the target's own species and of the other species
-  const float il2_same = PHYS == 1 ? (tsp ? sm.pk[2] : sm.pk[0]) : 0.f;
-  const float il_same = PHYS == 1 ? (tsp ? sm.pk[6] : sm.pk[4]) : 0.f;
-  const float il2_ei = sm.pk[1], il_ei = sm.pk[5], rs_inv = sm.pk[3];
-  float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pq = 0.f;
-  for (int k = 0; k < cnt; ++k) {
-    const float4 P = sm.part[2 * k], Q = sm.part[2 * k + 1];
-    const int s = __float_as_int(P.w);
-    const float dx = (thx - P.x) + (tlx - Q.x);
-    const float dy = (thy - P.y) + (tly - Q.y);
-    const float dz = (thz - P.z) + (tlz - Q.z);
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const float ssign = Q.w;  // source charge: -1 e, +1 ion
-    const bool same = ssign == tq;
-    // "special" pairs leave the plain Coulomb law: the target itself (r = 0),
-    // pairs inside the Kelbg core (exp(-x^2) still visible in FP32), and for
-    // the reference laws same-species pairs inside the r^2 <= 0.01 cutoff and
-    // e-i pairs where exp(-r/rs) is visible.  They are rare, so the common
-    // path carries no selects.
-    bool special;
-    if (PHYS == 1) special = r2 * (same ? il2_same : il2_ei) < 40.f;
-    else special = same ? !(r2 > 0.01f) : r2 * (rs_inv * rs_inv) < 400.f;
-    float fs, ph;
-    if (!special) {
-      const float rinv = rsqrtf(r2);
-      fs = ssign * rinv * rinv * rinv;
-      ph = ssign * rinv;
+  {
+    // this lane's source (or, past cnt, a chargeless dummy 10^6 um away)
+    float v[8];
+    if (lane < cnt) {
+      const int s = sm.p2p[(head + lane) & (kP2pRing - 1)];
+      const double4 xs = a.xs[s];
+      const double rx = Gx - xs.x, ry = Gy - xs.y, rz = Gz - xs.z;
+      const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
+      v[0] = hx; v[1] = hy; v[2] = hz; v[3] = __int_as_float(s);
+      v[4] = (float)(rx - (double)hx); v[5] = (float)(ry - (double)hy);
+      v[6] = (float)(rz - (double)hz); v[7] = xs.w > 0.5 ? 1.f : -1.f;
     } else {
-      fs = 0.f;
-      ph = 0.f;
-      if (PHYS == 1) {
-        if (s != p_self) {
-          const float il = same ? il_same : il_ei;
-          const float sqrtpi = 1.77245385f;
-          float ve;
-          if (r2 > 0.f) {
-            const float r = sqrtf(r2);
-            const float ri = 1.f / r;
-            const float x2 = r2 * il * il;
-            const float g = -expm1f(-x2);
-            fs = ssign * g * ri * ri * ri;
-            ve = g * ri + sqrtpi * erfcf(r * il) * il;
-          } else {
-            ve = sqrtpi * il;  // distinct particles on one point: V(0)
-          }
-          ph = ssign * ve;
-        }
-      } else if (!same) {
-        float ve;
-        if (r2 > 0.f) {
-          const float r = sqrtf(r2);
-          const float ri = 1.f / r;
-          const float e = expf(-r * rs_inv);
-          const float g = ri - e * (ri + rs_inv);
-          fs = ssign * g * ri * ri;
-          ve = (1.f - e) * ri;
-        } else {
-          ve = rs_inv;  // r -> 0 limit of (1 - exp(-r/rs))/r
-        }
-        ph = ssign * ve;
-      }  // same species inside the cutoff (and the target itself): nothing
+      v[0] = v[1] = v[2] = 1.0e6f;
+      v[3] = __int_as_float(-1);
+      v[4] = v[5] = v[6] = v[7] = 0.f;
     }
-    fx = fmaf(fs, dx, fx);
-    fy = fmaf(fs, dy, fy);
-    fz = fmaf(fs, dz, fz);
-    pa += ph;
-    pq = fmaf(ssign, ph, pq);
-    if (RDF && act) {
-      bool counted = PHYS == 1 ? s != p_self : (same ? r2 > 0.01f : true);
-      if (counted && (!same || tsp == 1)) {
-        // bin in FP64 from the hi/lo offsets so bin edges match the FP64 path
-        const double ex = ((double)thx - (double)P.x) + ((double)tlx - (double)Q.x);
-        const double ey = ((double)thy - (double)P.y) + ((double)tly - (double)Q.y);
-        const double ez = ((double)thz - (double)P.z) + ((double)tlz - (double)Q.z);
-        const double t = sqrt(ex * ex + ey * ey + ez * ez) * (same ? a.dx_ii_inv : a.dx_ei_inv);
-        if (t < (double)kRdfBins) {
-          int id = (int)t;
-          if (id >= 0 && id < kRdfBins) atomicAdd(&a.rdf[(same ? kRdfBins : 0) + id], 1u);
-        }
-      }
+    const bool odd = lane & 1;
+    float2* pb = reinterpret_cast<float2*>(sm.part + kPartF4 * (lane >> 1)) + (odd ? 1 : 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float lo = v[2 * j], hi = v[2 * j + 1];
+      const float o_lo = __shfl_xor_sync(0xffffffffu, lo, 1);
+      const float o_hi = __shfl_xor_sync(0xffffffffu, hi, 1);
+      pb[2 * j] = odd ? make_float2(o_hi, hi) : make_float2(lo, o_lo);
     }
   }
   __syncwarp();
-  kahan_add(acc.sx, acc.cx, fx);
-  kahan_add(acc.sy, acc.cy, fy);
-  kahan_add(acc.sz, acc.cz, fz);
-  acc.phi_all += (double)pa;
-  acc.phi_ion += 0.5 * ((double)pa + (double)pq);  // ion sources: (all + charge-weighted) / 2
+  // the source charge that makes a pair "same species" for this target, and
+  // the FP32 screening constants of the common-path test
+  const float tq = tsp ? 1.f : -1.f;
+  const float il2_to_e = PHYS == 1 ? (tsp ? sm.pk[1] : sm.pk[0]) : 0.f;  // electron source
+  const float il2_to_i = PHYS == 1 ? (tsp ? sm.pk[2] : sm.pk[1]) : 0.f;  // ion source
+  const float rs2 = sm.pk[3] * sm.pk[3];
+  const float2 thx2 = make_float2(thx, thx), thy2 = make_float2(thy, thy), thz2 = make_float2(thz, thz);
+  const float2 tlx2 = make_float2(tlx, tlx), tly2 = make_float2(tly, tly), tlz2 = make_float2(tlz, tlz);
+  float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx, pa = fx, pq = fx;
+  const int npair = (cnt + 1) >> 1;
+  for (int b = 0; b < npair; ++b) {
+    const float4* blk = sm.part + kPartF4 * b;
+    const float4 q0 = blk[0], q1 = blk[1], q2 = blk[2], q3 = blk[3];
+    const float2 q = make_float2(q3.z, q3.w);  // source charges: -1 e, +1 ion
+    const float2 dx = __fadd2_rn(__fadd2_rn(thx2, make_float2(q0.x, q0.y)),
+                                 __fadd2_rn(tlx2, make_float2(q2.x, q2.y)));
+    const float2 dy = __fadd2_rn(__fadd2_rn(thy2, make_float2(q0.z, q0.w)),
+                                 __fadd2_rn(tly2, make_float2(q2.z, q2.w)));
+    const float2 dz = __fadd2_rn(__fadd2_rn(thz2, make_float2(q1.x, q1.y)),
+                                 __fadd2_rn(tlz2, make_float2(q3.x, q3.y)));
+    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    bool sp0, sp1;
+    if (PHYS == 1) {
+      sp0 = r2.x * (q.x < 0.f ? il2_to_e : il2_to_i) < 40.f;
+      sp1 = r2.y * (q.y < 0.f ? il2_to_e : il2_to_i) < 40.f;
+    } else {
+      sp0 = q.x == tq ? !(r2.x > 0.01f) : r2.x * rs2 < 400.f;
+      sp1 = q.y == tq ? !(r2.y > 0.01f) : r2.y * rs2 < 400.f;
+    }
+    if (!(sp0 || sp1)) {
+      const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 ph = __fmul2_rn(q, rinv);
+      const float2 fs = __fmul2_rn(ph, __fmul2_rn(rinv, rinv));
+      fx = __ffma2_rn(fs, dx, fx);
+      fy = __ffma2_rn(fs, dy, fy);
+      fz = __ffma2_rn(fs, dz, fz);
+      pa = __fadd2_rn(pa, ph);
+      pq = __ffma2_rn(q, ph, pq);
+    } else {
+      p2p_one<PHYS>(sm, r2.x, dx.x, dy.x, dz.x, q.x, __float_as_int(q1.z), p_self, tsp,
+                    fx.x, fy.x, fz.x, pa.x, pq.x);
+      p2p_one<PHYS>(sm, r2.y, dx.y, dy.y, dz.y, q.y, __float_as_int(q1.w), p_self, tsp,
+                    fx.y, fy.y, fz.y, pa.y, pq.y);
+    }
+    if (RDF && act) {
+      rdf_count<PHYS>(a, r2.x, q.x, __float_as_int(q1.z), q0.x, q0.z, q1.x, q2.x, q2.z,
+                      q3.x, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
+      rdf_count<PHYS>(a, r2.y, q.y, __float_as_int(q1.w), q0.y, q0.w, q1.y, q2.y, q2.w,
+                      q3.y, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
+    }
+  }
+  __syncwarp();
+  kahan_add(acc.sx, acc.cx, fx.x + fx.y);
+  kahan_add(acc.sy, acc.cy, fy.x + fy.y);
+  kahan_add(acc.sz, acc.cz, fz.x + fz.y);
+  const double pad = (double)pa.x + (double)pa.y, pqd = (double)pq.x + (double)pq.y;
+  acc.phi_all += pad;
+  acc.phi_ion += 0.5 * (pad + pqd);  // ion sources: (all + charge-weighted) / 2
 }
 
 // --------------------------------------------------------------- walk ----
