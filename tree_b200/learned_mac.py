@@ -1,8 +1,8 @@
 """Trains the learned multipole acceptance criterion on the GPU.
 
-    python -m tree_b200.learned_mac [--n 65536] [--out tree_b200/data/mac_model.npz]
+    python -m tree_b200.learned_mac [--n 262144] [--out tree_b200/data/mac_model.npz]
 
-Training data is generated by the method itself: seeded clouds of N = 65,536
+Training data is generated by the method itself: seeded clouds of N = 262,144
 particles at electron temperatures across [10, 200] K are evolved a few steps
 with the fixed-theta mixed walk, and at each state `tree_gpu_mac_collect`
 walks the combined tree with opening angles drawn from [0.2, 0.9], recording
@@ -26,7 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(HERE, "data", "mac_model.npz")
 
 
-def collect_and_train(n=65536, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
+def collect_and_train(n=262144, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
                       steps_list=(2, 6, 20), theta=(0.2, 0.9), rho=(0.2, 0.9),
                       max_count=16384, keep=0.1, cap=12_000_000, epochs=10,
                       batch=8192, lr=2e-3, tau=0.99, seed=11, verbose=True):
@@ -98,7 +98,7 @@ def load_model(path=DEFAULT_MODEL):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--n", type=int, default=65536)
+    ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--out", default=DEFAULT_MODEL)
     ap.add_argument("--dump-samples", default="")
