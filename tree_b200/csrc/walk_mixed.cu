@@ -182,9 +182,9 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     const float4* cl = sm.cell + kCellF4 * k;
     const float4 A = cl[0], B = cl[1], C = cl[2], E = cl[3];
     const float dx = tx - A.x, dy = ty - A.y, dz = tz - A.z;
-    // accepted cells are farther than rcrit >= 0; the floor only guards a
+    // accepted cells are farther than rcrit >= 0; the 1e-30 only guards a
     // zero-size cell against an FP32 distance of 0
-    const float r2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), 1e-30f);
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, 1e-30f)));
     // Normalised form: the moments are contracted with the unit vector
     // n = d / r and scaled by powers of s = 1/r, so every intermediate is
     // bounded by n (a/r)^k -- escaped electrons millions of um away would
@@ -200,8 +200,9 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     // r^2 (-grad phi) = gp n - s D - 6 s^2 S n - 7.5 s^3 T(., n, n),
     // gp = Q + 3 s D.n + 15 s^2 n.S.n + 17.5 s^3 T(n,n,n);
     // r phi = Q + s D.n + 3 s^2 n.S.n + 2.5 s^3 T(n,n,n)
-    float gp = fmaf(s, fmaf(3.f, Dn, 15.f * s * u), A.w);
-    float php = fmaf(s, fmaf(3.f * s, u, Dn), A.w);
+    const float su = s * u;
+    float gp = fmaf(s, fmaf(15.f, su, 3.f * Dn), A.w);
+    float php = fmaf(s, fmaf(3.f, su, Dn), A.w);
     const float c5 = -6.f * s2;
     float gx = fmaf(c5, Sx, -s * B.x);
     float gy = fmaf(c5, Sy, -s * B.y);
@@ -209,17 +210,21 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     if (ORDER >= 3) {
       const float4 T1 = cl[4], T2 = cl[5];
       // T order: xxx = E.z, yyy = E.w, zzz = T1.x, xxy = T1.y, xxz = T1.z,
-      // xyy = T1.w, yyz = T2.x, xzz = T2.y, yzz = T2.z, xyz = T2.w
-      const float xx = nx * nx, yy = ny * ny, zz = nz * nz;
+      // xyy = T1.w, yyz = T2.x, xzz = T2.y, yzz = T2.z, xyz = T2.w.  T is
+      // trace-free (T_iik = 0), so T_kzz = -T_kxx - T_kyy and each component
+      // of T(., n, n) takes five terms with a = nx^2 - nz^2, b = ny^2 - nz^2
+      const float zz = nz * nz;
+      const float a2 = fmaf(nx, nx, -zz), b2 = fmaf(ny, ny, -zz);
       const float x2 = nx + nx, y2 = ny + ny;
       const float xy2 = x2 * ny, xz2 = x2 * nz, yz2 = y2 * nz;
-      const float Tx = fmaf(E.z, xx, fmaf(T1.w, yy, fmaf(T2.y, zz, fmaf(T1.y, xy2, fmaf(T1.z, xz2, T2.w * yz2)))));
-      const float Ty = fmaf(T1.y, xx, fmaf(E.w, yy, fmaf(T2.z, zz, fmaf(T1.w, xy2, fmaf(T2.w, xz2, T2.x * yz2)))));
-      const float Tz = fmaf(T1.z, xx, fmaf(T2.x, yy, fmaf(T1.x, zz, fmaf(T2.w, xy2, fmaf(T2.y, xz2, T2.z * yz2)))));
+      const float Tx = fmaf(E.z, a2, fmaf(T1.w, b2, fmaf(T1.y, xy2, fmaf(T1.z, xz2, T2.w * yz2))));
+      const float Ty = fmaf(T1.y, a2, fmaf(E.w, b2, fmaf(T1.w, xy2, fmaf(T2.w, xz2, T2.x * yz2))));
+      const float Tz = fmaf(T1.z, a2, fmaf(T2.x, b2, fmaf(T2.w, xy2, fmaf(T2.y, xz2, T2.z * yz2))));
       const float T3 = fmaf(nx, Tx, fmaf(ny, Ty, nz * Tz));
       const float s3 = s2 * s;
-      gp = fmaf(17.5f * s3, T3, gp);
-      php = fmaf(2.5f * s3, T3, php);
+      const float s3T3 = s3 * T3;
+      gp = fmaf(17.5f, s3T3, gp);
+      php = fmaf(2.5f, s3T3, php);
       const float c7 = -7.5f * s3;
       gx = fmaf(c7, Tx, gx);
       gy = fmaf(c7, Ty, gy);
