@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=1048576)
+    # --particles: the same, for launchers (torchrun) that claim --n* options
+    ap.add_argument("--n", "--particles", dest="n", type=int, default=1048576)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--mac", choices=["fixed", "learned"], default="learned")
     ap.add_argument("--physics", choices=["kelbg", "ref"], default="kelbg")
@@ -209,6 +210,24 @@ def auto_stride(n):
     return max(1, int(round(n / 16384)))
 
 
+# ------------------------------------------------------------- replicas ----
+def max_over_ranks(value, dist):
+    """The largest `value` over all ranks (the value itself without a process
+    group): every rank reports the slowest replica's time."""
+    if not dist:
+        return value
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(n_per_rank, world, steps, ms):
+    """Particle-steps/s of all replicas together over a time of ms."""
+    return n_per_rank * world * steps / (ms / 1e3)
+
+
 # ----------------------------------------------------------- reference arm ----
 def run_reference(args, rank, world):
     if rank != 0:
@@ -302,13 +321,9 @@ def run_ours(args, rank, world, dist):
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     t_after = tf.timings()
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * world * args.steps / (ms / 1e3)
+    value = whole_job_rate(n, world, args.steps, ms)
     walk_ms = (t_after.ms_walk - t_before.ms_walk) / args.steps
     build_ms = (t_after.ms_build - t_before.ms_build) / args.steps
     launches = t_after.launches - t_before.launches
@@ -343,12 +358,8 @@ def run_ours(args, rank, world, dist):
                              ptr["x_ion"], ptr["v_ion"], ptr["f_ion"])
         a1.record(stream)
         torch.cuda.synchronize()
-        ems = a0.elapsed_time(a1)
-        if dist:
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": n * world * k2 / (ems / 1e3), "unit": UNIT,
+        ems = max_over_ranks(a0.elapsed_time(a1), dist)
+        e2e = {"value": whole_job_rate(n, world, k2, ems), "unit": UNIT,
                "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n,
                "steps": k2,
                "path": "tree_gpu_load_state(x,v,f pinned host) + tree_gpu_step(1) "
@@ -412,7 +423,7 @@ def run_ours(args, rank, world, dist):
                 b1.record(stream)
                 torch.cuda.synchronize()
                 ta = tc.timings()
-                cms = b0.elapsed_time(b1) / args.steps
+                cms = max_over_ranks(b0.elapsed_time(b1), dist) / args.steps
                 acc_c = audit(tc, audit_idx)
                 compare[name] = {"theta": acfg.theta, "ms_per_step": cms,
                                  "walk_ms": (ta.ms_walk - tb.ms_walk) / args.steps,
@@ -526,13 +537,9 @@ def run_ensemble(args, rank, world, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     t_after = ens.timings()
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * world * args.steps / (ms / 1e3)
+    value = whole_job_rate(n, world, args.steps, ms)
     # per-cloud accuracy against each cloud's own FP64 direct sum
     f = ens.get_state()["f"]
     rms = []
@@ -554,7 +561,7 @@ def run_ensemble(args, rank, world, dist):
         ens.get_state_ptr(pin["x"].data_ptr(), pin["v"].data_ptr(), pin["f"].data_ptr())
     a1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = a0.elapsed_time(a1) / k2
+    e2e_ms = max_over_ranks(a0.elapsed_time(a1), dist) / k2
     # the same clouds, one handle after another, from the same warm state
     sep_ms = None
     if not args.no_compare:
@@ -584,7 +591,7 @@ def run_ensemble(args, rank, world, dist):
                 tc.step(dt, args.steps)
                 s1.record(stream)
                 torch.cuda.synchronize()
-                sep_ms += s0.elapsed_time(s1) / args.steps
+                sep_ms += max_over_ranks(s0.elapsed_time(s1), dist) / args.steps
     ens.close()
     if rank != 0:
         return
@@ -611,7 +618,7 @@ def run_ensemble(args, rank, world, dist):
                      "per_cloud": [{"n": int(ens.offsets[c + 1] - ens.offsets[c]),
                                     "te_k": round(float(te[c]), 2), "n0": float(n0[c]),
                                     "rms": rms[c]} for c in range(args.clouds)]},
-        "e2e": {"value": n * world / (e2e_ms / 1e3), "unit": UNIT,
+        "e2e": {"value": whole_job_rate(n, world, 1, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n},
         "separate_handles_ms_per_step": sep_ms,
         "one_launch_speedup": (sep_ms / (ms / args.steps)) if sep_ms else None,
@@ -629,8 +636,10 @@ def main():
 
         import torch
         import torch.distributed as tdist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        # the reference arm runs on the host cores: gloo, no device
         backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         dist = tdist
     try:
