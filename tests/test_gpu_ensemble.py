@@ -78,6 +78,41 @@ def test_ensemble_equals_clouds_run_alone(device_lib, learned):
         assert sums[k, 3] == pytest.approx(d.mv2_ion, rel=1e-12)
 
 
+def test_ensemble_tiny_ragged_and_empty_clouds(device_lib):
+    """Clouds of 2 and 31 particles (one target group each), 33 (a chunked
+    root), one species only, and an empty cloud: every non-empty cloud still
+    matches its own run alone bit for bit; the empty one contributes nothing."""
+    sizes = [(1, 1), (16, 15), (17, 16), (300, 0), (0, 300), (0, 0), (200, 180)]
+    rng = np.random.default_rng(77)
+    xs, vs = [], []
+    for ne, ni in sizes:
+        xs.append(rng.standard_normal((ne + ni, 3)) * 20.0)
+        vs.append(rng.standard_normal((ne + ni, 3)) * 1e-3)
+    n_el = np.array([ne for ne, _ in sizes], np.int64)
+    n_ion = np.array([ni for _, ni in sizes], np.int64)
+    x, v = np.vstack(xs), np.vstack(vs)
+    tes = [20.0 + 10 * k for k in range(len(sizes))]
+    with api.Ensemble([_cfg(t) for t in tes], n_el, n_ion) as ens:
+        ens.set_state(x, v)
+        ens.step(DT, 2)
+        st = ens.get_state()
+        sums = ens.sums()
+    for k, (ne, ni) in enumerate(sizes):
+        a, b = ens.offsets[k], ens.offsets[k + 1]
+        assert b - a == ne + ni
+        if ne + ni == 0:
+            assert np.all(sums[k] == 0)
+            continue
+        with api.TreeForce(ne, ni, _cfg(tes[k])) as tf:
+            tf.set_state(xs[k][:ne], vs[k][:ne], xs[k][ne:], vs[k][ne:])
+            tf.step(DT, 2)
+            sa = tf.get_state()
+        np.testing.assert_array_equal(st["x"][a:b], np.vstack([sa["x_el"], sa["x_ion"]]),
+                                      err_msg=f"x, cloud {k}")
+        np.testing.assert_array_equal(st["f"][a:b], np.vstack([sa["f_el"], sa["f_ion"]]),
+                                      err_msg=f"f, cloud {k}")
+
+
 def test_ensemble_accuracy_per_cloud(device_lib):
     """Every cloud meets the accuracy of the mixed path against its own FP64
     direct sum (cloud-local audit)."""
