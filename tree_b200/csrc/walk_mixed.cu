@@ -1,9 +1,10 @@
 // walk_mixed.cu -- warp-group Barnes-Hut walk in mixed precision.
 //
 // The mixed path walks ONE combined tree of both species (net-charge moments
-// about each cell's particle centroid, built by k_upward_net).  One warp owns a
-// target group -- a compact cell of at most 32 particles of either species,
-// built by k_groups -- and builds ONE interaction list for it:
+// about each cell's particle centroid, built level by level by k_net_level).
+// One warp owns a target group -- a contiguous sorted range of at most 32
+// particles of either species inside one cell, built by k_groups -- and
+// builds ONE interaction list for it:
 //   * group MAC: a cell is accepted when rcrit = s/theta + dx (the reference
 //     criterion, tree.f90:736-743) is below the distance from the cell's charge
 //     centre to the group's bounding box, so every target of the group would
@@ -13,7 +14,8 @@
 //     particle (P2P) entries, other twigs push their children on a per-warp
 //     stack;
 //   * every 32 entries the warp stages them in shared memory and each lane
-//     evaluates them for its own target in FP32.
+//     evaluates them for its own target in FP32 (particle pairs two at a time
+//     on the packed f32x2 pipeline).
 // Precision: positions, the group centre and the MAC stay FP64.  Cells are
 // evaluated in FP32 relative to the group centre; particle pairs use a
 // two-float (hi + lo) split of the FP64 offsets, so a pair separation keeps
