@@ -100,10 +100,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--epochs", type=int, default=10)
+    ap.add_argument("--keep", type=float, default=0.1,
+                    help="sampling probability of a tested cell in the acceptance band")
     ap.add_argument("--out", default=DEFAULT_MODEL)
     ap.add_argument("--dump-samples", default="")
     args = ap.parse_args()
-    params, stats, report, (f, y, e) = collect_and_train(n=args.n, epochs=args.epochs)
+    params, stats, report, (f, y, e) = collect_and_train(n=args.n, epochs=args.epochs, keep=args.keep)
     save_model(args.out, params, stats, report)
     if args.dump_samples:
         idx = np.random.default_rng(0).choice(len(y), min(len(y), 150_000), replace=False)

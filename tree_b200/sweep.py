@@ -2,6 +2,7 @@
 
     python -m tree_b200.sweep precision [--n 1048576] [--steps 1000]
     python -m tree_b200.sweep drift [--n 1048576] [--steps 1000]
+    python -m tree_b200.sweep learned [--n 4194304] [--steps 500]
 
 precision: the precision form -- seeded clouds at T_e in {10, 50, 200} K,
     each run with the mixed-precision walk at opening angles {0.3, 0.5, 0.7}
@@ -13,6 +14,13 @@ drift: the total energy 1/2 (mv2_el + mv2_ion) + Epot_e + Epot_i, sampled every
     mixed-precision walk with the learned criterion (theta 0.30, eta 3e-5) and
     for the plain FP64 fixed-theta path (theta 0.5); reports the largest
     excursion |E - E_0| relative to the mean kinetic energy for both.
+learned: the learned-MAC form -- the mixed walk with the learned criterion
+    (theta 0.30, eta 3e-5) for `steps` steps from a seeded cloud at T_e = 50 K;
+    at steps 1, 10, 100 and the last, the rms and max relative force error on
+    16,384 seeded targets; the time per step, against a fixed-theta mixed walk
+    (theta 0.30) and the plain FP64 fixed-theta path (theta 0.5) timed over a
+    few steps from the final state (after one untimed step each), beside the
+    learned walk timed over the same steps from the same state.
 
 One JSON line per run.  Inputs are seeded synthetic clouds (Gaussian at peak
 density 1e15 m^-3, electrons on their ions at t = 0, T_i = 1 mK, dt = 1e-11 s).
@@ -90,17 +98,75 @@ def drift(n, steps, seed, nsamp=10):
           flush=True)
 
 
+def learned(n, steps, seed, nplain=3):
+    dt = units.dt_code(1e-11)
+    c = cloud.make_cloud(n, seed=seed)
+    rng = np.random.default_rng(seed + 17)
+    idx = np.sort(rng.choice(n, min(16384, n), replace=False))
+    params, stats, _ = learned_mac.load_model()
+    marks = sorted({m for m in (1, 10, 100, steps) if m <= steps})
+    cfg = api.Config(theta=0.30, physics=api.PHYS_KELBG, precision=api.PREC_MIXED,
+                     mac=api.MAC_LEARNED)
+    out = {"mode": "learned", "n": n, "steps": steps}
+    with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
+        tf.set_tuning(8, 4, 3)
+        tf.mac_set_model(params, stats)
+        tf.mac_config(3e-5, 0.05, 0.9)
+        tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
+        done, rows, ms = 0, [], 0.0
+        for m in marks:
+            t0 = tf.timings()
+            tf.step(dt, m - done)
+            t1 = tf.timings()
+            ms += t1.ms_total - t0.ms_total
+            done = m
+            rms, mx = _audit(tf, idx)
+            rows.append({"step": m, "rms": rms, "max": mx, "n_m2p": t1.n_m2p,
+                         "n_p2p": t1.n_p2p, "n_net": t1.n_mac_net})
+        st = tf.get_state()
+        # the same few steps as the comparison arms, from the same state
+        t0 = tf.timings()
+        tf.step(dt, nplain)
+        t1 = tf.timings()
+        out["learned"] = {"theta": 0.30, "eta": 3e-5, "audits": rows,
+                          "ms_per_step": ms / steps,
+                          "ms_per_step_from_final_state": (t1.ms_total - t0.ms_total) / nplain}
+    # comparison arms from the final state: a few steps each, then an audit
+    arms = (("mixed_fixed_theta0.30", api.Config(theta=0.30, physics=api.PHYS_KELBG,
+                                                  precision=api.PREC_MIXED)),
+            ("fp64_plain_theta0.5", api.Config(theta=0.5, physics=api.PHYS_KELBG,
+                                               precision=api.PREC_FP64)))
+    for name, acfg in arms:
+        with api.TreeForce(len(c.x_el), len(c.x_ion), acfg) as tf:
+            if acfg.precision == api.PREC_MIXED:
+                tf.set_tuning(8, 4, 3)
+            tf.load_state(st["x_el"], st["v_el"], st["f_el"], st["x_ion"], st["v_ion"], st["f_ion"])
+            tf.step(dt, 1)  # graph capture and node-array growth, untimed
+            t0 = tf.timings()
+            tf.step(dt, nplain)
+            t1 = tf.timings()
+            rms, mx = _audit(tf, idx)
+            out[name] = {"ms_per_step": (t1.ms_total - t0.ms_total) / nplain,
+                         "steps": nplain, "rms": rms, "max": mx}
+    lf = out["learned"]["ms_per_step_from_final_state"]
+    out["learned_over_fp64_plain"] = out["fp64_plain_theta0.5"]["ms_per_step"] / lf
+    out["learned_over_fixed"] = out["mixed_fixed_theta0.30"]["ms_per_step"] / lf
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("mode", choices=["precision", "drift"])
-    ap.add_argument("--n", type=int, default=1048576)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("mode", choices=["precision", "drift", "learned"])
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--seed", type=int, default=2024)
     args = ap.parse_args()
     if args.mode == "precision":
-        precision(args.n, args.steps, args.seed)
+        precision(args.n or 1048576, args.steps or 1000, args.seed)
+    elif args.mode == "drift":
+        drift(args.n or 1048576, args.steps or 1000, args.seed)
     else:
-        drift(args.n, args.steps, args.seed)
+        learned(args.n or 4194304, args.steps or 500, args.seed)
 
 
 if __name__ == "__main__":
