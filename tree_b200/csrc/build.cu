@@ -680,14 +680,42 @@ __device__ __forceinline__ int shift_for_level(int d, int top) {
   return s > 0 ? s : 0;
 }
 
+// Ends of the level-d cell of particle p inside its segment [sb, se): keys q
+// and q+1 share fewer than d levels exactly where the level-d prefix
+// changes, so a short scan of the common-level array L finds the end of a
+// small cell (most of them); the keys beyond the scanned window are
+// binary-searched.  Both give the same index.
+constexpr int kRangeScan = 32;
+
+// first q in (p, se) outside the cell, or se
+__device__ __forceinline__ int range_end(const key128* __restrict__ keys,
+                                         const int8_t* __restrict__ L, int p, int se,
+                                         int d, int sh, key128 pre) {
+  const int lim = p + kRangeScan < se ? p + kRangeScan : se;
+  for (int q = p + 1; q < lim; ++q)
+    if (L[q - 1] < d) return q;
+  return upper_prefix(keys, lim, se, sh, pre);
+}
+
+// first q in [sb, p] inside the cell (level 0: the segment's root cell)
+__device__ __forceinline__ int range_start(const key128* __restrict__ keys,
+                                           const int8_t* __restrict__ L, int sb, int p,
+                                           int d, int sh, key128 pre) {
+  if (d == 0) return sb;
+  const int lim = p - kRangeScan > sb ? p - kRangeScan : sb;
+  for (int j = p - 1; j >= lim; --j)
+    if (L[j] < d) return j + 1;
+  return lower_prefix(keys, sb, lim + 1, sh, pre);
+}
+
 // Index of the twig at level d that contains sorted particle p, given that it
 // was opened at an earlier particle (first particle of the level-d prefix).
 __device__ __forceinline__ int twig_index_before(
     const key128* __restrict__ keys, const int8_t* __restrict__ L,
     const int32_t* __restrict__ off, int sb, int p, int d, int top) {
-  int sh = shift_for_level(d, top);
-  key128 pre = keys[p] >> sh;
-  int q = lower_prefix(keys, sb, p + 1, sh, pre);
+  const int sh = d > 0 ? shift_for_level(d, top) : 0;
+  const key128 pre = d > 0 ? keys[p] >> sh : (key128)0;
+  int q = range_start(keys, L, sb, p, d, sh, pre);
   int lo_q = q == 0 ? -1 : (int)L[q - 1];
   return off[q] + (d - lo_q - 1);
 }
@@ -747,7 +775,7 @@ __global__ void k_topology(const key128* __restrict__ keys,
         q_end = se;
       } else {
         int sh = shift_for_level(d, top);
-        int q = upper_prefix(keys, p + 1, se, sh, key >> sh);
+        int q = range_end(keys, L, p, se, d, sh, key >> sh);
         sk = q < se ? off[q] : tree_end;
         q_end = q;
       }
