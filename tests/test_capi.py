@@ -70,3 +70,55 @@ def test_fortran_module_declares_every_function():
     mod = open(os.path.join(ROOT, "include", "tree_gpu_mod.f90")).read()
     declared = set(re.findall(r"FUNCTION\s+(tree_gpu_\w+)\s*\(", mod))
     assert set(declared_functions()) == declared
+
+
+def _ensemble_create(lib, cfgs, n_el, n_ion):
+    arr = (api.Params * max(1, len(cfgs)))(*[c.to_c() for c in cfgs])
+    ne = (ctypes.c_int64 * max(1, len(n_el)))(*n_el)
+    ni = (ctypes.c_int64 * max(1, len(n_ion)))(*n_ion)
+    h = ctypes.c_void_p()
+    rc = lib.tree_gpu_ensemble_create(arr, len(cfgs), ne, ni, ctypes.byref(h))
+    return rc, h
+
+
+def _mixed(**kw):
+    return api.Config(precision=api.PREC_MIXED, physics=api.PHYS_KELBG, **kw)
+
+
+@pytest.mark.parametrize("case", ["no_clouds", "too_many", "fp64_cloud", "mixed_theta",
+                                  "negative_size"])
+def test_ensemble_create_rejects_bad_arguments_before_cuda(device_lib, case):
+    """One walk, one criterion and one integrator serve every cloud, so the
+    clouds must agree on precision (mixed), physics, theta, MAC and masses;
+    sizes are checked before any device memory is touched."""
+    cfgs, ne, ni = [_mixed(te=20.0), _mixed(te=80.0)], [10, 12], [10, 12]
+    if case == "no_clouds":
+        cfgs, ne, ni = [], [], []
+    elif case == "too_many":
+        cfgs, ne, ni = [_mixed()] * 257, [2] * 257, [2] * 257
+    elif case == "fp64_cloud":
+        cfgs[1] = api.Config(precision=api.PREC_FP64, physics=api.PHYS_KELBG)
+    elif case == "mixed_theta":
+        cfgs[1] = _mixed(theta=0.7)
+    elif case == "negative_size":
+        ne[1] = -1
+    rc, h = _ensemble_create(device_lib, cfgs, ne, ni)
+    assert rc == -1 and not h.value
+
+
+def test_direct_static_checks_arguments_before_cuda(device_lib):
+    """The allocation-free audit rejects a target list above its fixed
+    scratch size (capacity error) and bad parameters, and returns at once for
+    an empty list -- all before any CUDA call."""
+    p = _mixed(te=50.0).to_c()
+    f = device_lib.tree_gpu_direct_static
+    cap = int(re.search(r"#define TREE_GPU_DIRECT_STATIC_MAX_TARGETS (\d+)",
+                        open(HEADER).read()).group(1))
+    assert f(None, 4, 4, ctypes.byref(p), None, cap + 1, None, None, None) == -4
+    assert f(None, 4, 4, ctypes.byref(p), None, -1, None, None, None) == -1
+    assert f(None, -4, 4, ctypes.byref(p), None, 1, None, None, None) == -1
+    assert f(None, 4, 4, None, None, 1, None, None, None) == -1
+    assert f(None, 4, 4, ctypes.byref(p), None, 0, None, None, None) == 0
+    bad = _mixed(te=50.0).to_c()
+    bad.physics = 7
+    assert f(None, 4, 4, ctypes.byref(bad), None, 1, None, None, None) == -1
