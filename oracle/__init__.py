@@ -13,6 +13,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_NATIVE_PATH = os.path.join(_HERE, "liboracle_native.so")
 NBINS = 10001
 
 PHYS_REF = 0
@@ -27,6 +28,12 @@ class OracleParams(ctypes.Structure):
                 ("nthreads", ctypes.c_int32)]
 
 
+class Ref8Stats(ctypes.Structure):
+    _fields_ = [("n_el", ctypes.c_int64 * 8), ("n_ion", ctypes.c_int64 * 8),
+                ("ghost_nodes_e", ctypes.c_int64), ("ghost_nodes_i", ctypes.c_int64),
+                ("n_m2p_ghost", ctypes.c_int64), ("n_p2p_ghost", ctypes.c_int64)]
+
+
 class OracleStats(ctypes.Structure):
     _fields_ = [("n_m2p", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
                 ("max_depth_e", ctypes.c_int32), ("max_depth_i", ctypes.c_int32),
@@ -39,6 +46,7 @@ NODE_DTYPE = np.dtype([("xx", "<f8", 3), ("ox", "<f8", 3), ("lx", "<f8", 3),
                        ("level", "<i4"), ("ileaf", "<i4"), ("skip", "<i8")])
 
 _lib = None
+_flags = "-O3 -march=x86-64-v3 -ffp-contract=off -fopenmp"
 
 
 def build():
@@ -46,12 +54,37 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
+def use_native():
+    """Rebuilds the oracle with -march=native on this host (make -B, so a copy
+    built on another host is never used) and routes every later call to it.
+    Only for the timed CPU baseline; once a library is loaded it stays.
+    Returns the compiler flags of the library in use."""
+    global _flags
+    if _lib is not None:
+        return _flags
+    try:
+        subprocess.run(["make", "-s", "-B", "-C", _HERE, "native"], check=True,
+                       capture_output=True, timeout=300)
+        _load(_NATIVE_PATH)
+        _flags = "-O3 -march=native -ffp-contract=off -fopenmp"
+    except (subprocess.SubprocessError, OSError):
+        lib()
+        _flags += " (native build failed)"
+    return _flags
+
+
 def lib():
-    global _lib
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
+        _load(_LIB_PATH)
+    return _lib
+
+
+def _load(path):
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(path)
         dp = ctypes.POINTER(ctypes.c_double)
         lp = ctypes.POINTER(ctypes.c_int64)
         L.oracle_force.argtypes = [ctypes.c_int64, ctypes.c_int64, dp, dp,
@@ -60,6 +93,8 @@ def lib():
         L.oracle_force.restype = ctypes.c_int
         L.oracle_force_strided.argtypes = L.oracle_force.argtypes + [ctypes.c_int64]
         L.oracle_force_strided.restype = ctypes.c_int
+        L.oracle_force_ref8.argtypes = L.oracle_force.argtypes + [ctypes.POINTER(Ref8Stats)]
+        L.oracle_force_ref8.restype = ctypes.c_int
         L.oracle_tree_dump.argtypes = [ctypes.c_int64, dp, ctypes.c_int32,
                                        ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.POINTER(ctypes.c_int32)]
@@ -124,6 +159,36 @@ def force(x_el, x_ion, params, rdf=True, stride=1):
                            max_depth_e=st.max_depth_e,
                            max_depth_i=st.max_depth_i,
                            t_build=st.t_build, t_walk=st.t_walk))
+
+
+def force_ref8(x_el, x_ion, params, rdf=True):
+    """Force in the reference's 8-rank form (REF8): one domain per coordinate
+    octant, local trees walked locally, pruned ghost trees of the other seven
+    ranks walked with their unexpanded twigs as bare monopoles
+    (main.f90:506-701, tree.f90:1167-2330).  Same returns as force(), plus
+    "ref8": particles per rank, ghost-tree nodes and ghost interactions."""
+    x_el, x_ion = _c3(x_el), _c3(x_ion)
+    f_el = np.zeros_like(x_el)
+    f_ion = np.zeros_like(x_ion)
+    ep = np.zeros(2)
+    rei = np.zeros(NBINS, np.int64)
+    rii = np.zeros(NBINS, np.int64)
+    st = OracleStats()
+    s8 = Ref8Stats()
+    rc = lib().oracle_force_ref8(len(x_el), len(x_ion), _dp(x_el), _dp(x_ion),
+                                 ctypes.byref(params), _dp(f_el), _dp(f_ion), _dp(ep),
+                                 _lp(rei) if rdf else None, _lp(rii) if rdf else None,
+                                 ctypes.byref(st), ctypes.byref(s8))
+    if rc != 0:
+        raise RuntimeError(f"oracle_force_ref8 failed with status {rc}")
+    return dict(f_el=f_el, f_ion=f_ion, epot_e=ep[0], epot_i=ep[1],
+                rdf_ei=rei, rdf_ii=rii,
+                stats=dict(n_m2p=st.n_m2p, n_p2p=st.n_p2p,
+                           max_depth_e=st.max_depth_e, max_depth_i=st.max_depth_i,
+                           t_build=st.t_build, t_walk=st.t_walk),
+                ref8=dict(n_el=list(s8.n_el), n_ion=list(s8.n_ion),
+                          ghost_nodes_e=s8.ghost_nodes_e, ghost_nodes_i=s8.ghost_nodes_i,
+                          n_m2p_ghost=s8.n_m2p_ghost, n_p2p_ghost=s8.n_p2p_ghost))
 
 
 def tree_dump(x, sign):

@@ -681,3 +681,319 @@ void oracle_ke(int64_t n, const double* x, const double* v, double xm,
 int oracle_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+// ===================================================================== REF8 ==
+// The 8-rank form of Force (main.f90:506-701) run in one process.  The
+// reference runs on exactly 8 MPI ranks (mpienv.f90:19), one per coordinate
+// octant (id_FINDER, main.f90:840-862).  Each rank builds its own two species
+// trees over its own particles (BuildLocalTree) and walks them for its own
+// targets (LocalCoulombSum).  It then serialises each tree once per other
+// rank, pruned against the plane, line or point that its octant shares with
+// that rank's (CopyTree1..7, tree.f90:1204-1777, case from CriterionFind,
+// main.f90:865-925): a twig is expanded when MAXVAL(lx)/theta + dx exceeds
+// the distance from its charge centre to that contact set.  The receiver
+// rebuilds the serialised tree (RebuildGhostTree, tree.f90:1781-1853), where
+// every node sent without children -- a leaf, or a twig that was not expanded
+// -- becomes a leaf, and walks it (Ghost_Tree_ee/ie/ei/ii, tree.f90:1888-2330):
+// ghost twigs take the reference MAC and far field; ghost leaves are point
+// charges qeff with the leaf laws and no MAC, no r^2 > 0.01 cutoff.  Per
+// target the contributions arrive in the reference's order: own trees (ee or
+// ie, then ei or ii), the seven electron ghost trees from ranks r-1 .. r-7,
+// then the seven ion ghost trees in the same order.
+//
+// Particles are assigned to octants by their current positions (as right
+// after a migration, data.f90:196-389).  A rank without particles of a species
+// sends and walks no tree of that species (the reference would take MINVAL of
+// an empty array).  The deviations of the single-domain form (r = 0 e-i
+// guard, root qeff, RDF race, depth cap) apply unchanged.
+
+namespace {
+
+// id_FINDER: rank = 4(k-1) + 2(j-1) + (i-1), the low index for a negative
+// coordinate.
+inline int octant_of(const double* x) {
+  const int i = x[0] < 0.0 ? 0 : 1;
+  const int j = x[1] < 0.0 ? 0 : 1;
+  const int k = x[2] < 0.0 ? 0 : 1;
+  return 4 * k + 2 * j + i;
+}
+
+// CriterionFind: the contact case of octants a and b -- 1 y-z face, 2 x-z
+// face, 3 x-y face, 4 x-axis line, 5 y-axis line, 6 z-axis line, 7 the origin.
+int contact_case(int a, int b) {
+  const bool sx = (a & 1) == (b & 1);
+  const bool sy = ((a >> 1) & 1) == ((b >> 1) & 1);
+  const bool sz = ((a >> 2) & 1) == ((b >> 2) & 1);
+  if (sx) {
+    if (sy) return 3;
+    return sz ? 2 : 4;
+  }
+  if (sy) return sz ? 1 : 5;
+  return sz ? 6 : 7;
+}
+
+// Distance of a charge centre from the contact set of case c (the planes,
+// lines and point through the origin), in the reference's arithmetic.
+double contact_distance(int c, const double* xx) {
+  const double x = 0.0, y = 0.0, z = 0.0;
+  switch (c) {
+    case 1: return std::fabs(xx[0] - x);
+    case 2: return std::fabs(xx[1] - y);
+    case 3: return std::fabs(xx[2] - z);
+    case 4: return std::sqrt((xx[1] - y) * (xx[1] - y) + (xx[2] - z) * (xx[2] - z));
+    case 5: return std::sqrt((xx[0] - x) * (xx[0] - x) + (xx[2] - z) * (xx[2] - z));
+    case 6: return std::sqrt((xx[0] - x) * (xx[0] - x) + (xx[1] - y) * (xx[1] - y));
+    default:
+      return std::sqrt((xx[0] - x) * (xx[0] - x) + (xx[1] - y) * (xx[1] - y) +
+                       (xx[2] - z) * (xx[2] - z));
+  }
+}
+
+// CopyTree<c> of P followed by RebuildGhostTree: the ghost tree as the
+// receiver holds it.  Every node carries qeff, the charge centre, MAXVAL(lx)
+// (in all three lx slots, so the walk's MAXVAL returns it), dx and the
+// moments (zero for leaves); children keep their order and fill Child1.. in
+// turn; a node without children becomes a leaf of the sign of qeff.
+BT* copy_ghost(const BT* P, int c, double theta, int64_t& nodes) {
+  BT* G = new BT();
+  nodes++;
+  double s = P->lx[0];
+  if (P->lx[1] > s) s = P->lx[1];
+  if (P->lx[2] > s) s = P->lx[2];
+  G->qeff = P->qeff;
+  G->level = P->level;
+  for (int k = 0; k < 3; ++k) {
+    G->xx[k] = P->xx[k];
+    G->ox[k] = P->ox[k];
+    G->lx[k] = s;
+  }
+  int nk = 0;
+  if (P->ileaf == 0) {
+    G->dx = P->dx;
+    for (int k = 0; k < 3; ++k) {
+      G->D[k] = P->D[k];
+      G->Q[k] = P->Q[k];
+      G->QQ[k] = P->QQ[k];
+    }
+    if ((s / theta + G->dx) > contact_distance(c, G->xx)) {
+      for (int ch = 0; ch < 8; ++ch)
+        if (P->child[ch]) G->child[nk++] = copy_ghost(P->child[ch], c, theta, nodes);
+    }
+  }
+  G->ileaf = nk > 0 ? 0 : (G->qeff > 0.0 ? 1 : -1);
+  G->pt = -1;
+  return G;
+}
+
+// One target against one ghost tree (Ghost_Tree_ee/ie/ei/ii).
+void ghost_search(const BT* P, const double* xt, int tsign, int ssign,
+                  const Params& p, Acc& a, int64_t* rdf) {
+  double xr[3];
+  double r2 = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    xr[k] = xt[k] - P->xx[k];
+    r2 = r2 + xr[k] * xr[k];
+  }
+  if (P->ileaf == 0) {
+    const double s = P->lx[0];
+    const double r = std::sqrt(r2);
+    if ((s / p.theta + P->dx) < r) {  // tree.f90:1910
+      const double ff = (tsign < 0) ? -1.0 * kEps : kEps;
+      m2p(P, xr, r2, r, ff, a);
+    } else {
+      for (int c = 0; c < 8; ++c)
+        if (P->child[c]) ghost_search(P->child[c], xt, tsign, ssign, p, a, rdf);
+    }
+    return;
+  }
+  // ghost leaf: a point charge qeff (one particle, or a whole unexpanded twig)
+  a.n_p2p++;
+  const bool same = tsign == ssign;
+  const double r = std::sqrt(r2);
+  if (p.physics == 1) {
+    const double lam = same ? (tsign < 0 ? p.lam_ee : p.lam_ii) : p.lam_ei;
+    kelbg_pair(xr, r2, (double)tsign * P->qeff, lam, a);
+    if (!same) rdf_add(rdf, r, p.dx_ei);
+    else if (tsign > 0 && r2 > 0.0) rdf_add(rdf, r, p.dx_ii);
+    return;
+  }
+  // ff = -eps*qeff (electron target) or +eps*qeff (ion target), tree.f90:1975,
+  // 2072, 2210, 2315
+  const double ff = (tsign < 0 ? -1.0 : 1.0) * kEps * P->qeff;
+  if (same) {
+    // Ghost_Tree_ee tree.f90:1966-1981 / Ghost_Tree_ii 2306-2326
+    a.epot = a.epot + 0.5 * ff / r;
+    for (int k = 0; k < 3; ++k) a.f[k] = a.f[k] + ff * xr[k] / r / r2;
+    if (tsign > 0) rdf_add(rdf, r, p.dx_ii);
+    return;
+  }
+  // Ghost_Tree_ie tree.f90:2064-2084 / Ghost_Tree_ei 2202-2222
+  if (r2 == 0.0) {
+    a.epot = a.epot + 0.5 * ff * (1.0 / p.rs);  // deviation 1
+  } else {
+    const double e = std::exp(-r / p.rs);
+    a.epot = a.epot + 0.5 * ff * (1. - e) / r;
+    for (int k = 0; k < 3; ++k)
+      a.f[k] = a.f[k] + ff * xr[k] * (1.0 / r - e * (1.0 / r + 1.0 / p.rs)) / r2;
+  }
+  rdf_add(rdf, r, p.dx_ei);
+}
+
+}  // namespace
+
+extern "C" {
+
+typedef struct oracle_ref8_stats {
+  int64_t n_el[8], n_ion[8];       // particles per rank
+  int64_t ghost_nodes_e, ghost_nodes_i;  // nodes of all 56 ghost trees per species
+  int64_t n_m2p_ghost, n_p2p_ghost;      // interactions with ghost trees
+} oracle_ref8_stats;
+
+// Force in the 8-rank form (see above).  Arguments and outputs as
+// oracle_force; st8 (may be NULL) receives the decomposition's figures.
+int oracle_force_ref8(int64_t n_el, int64_t n_ion, const double* x_el,
+                      const double* x_ion, const oracle_params* prm,
+                      double* f_el, double* f_ion, double* epot,
+                      int64_t* rdf_ei, int64_t* rdf_ii, oracle_stats* st,
+                      oracle_ref8_stats* st8) {
+  if (n_el < 0 || n_ion < 0 || !prm || prm->theta <= 0.0) return ORACLE_ERR_ARG;
+  Params p{prm->theta, prm->rs, prm->dx_ei, prm->dx_ii,
+           prm->lam_ee, prm->lam_ei, prm->lam_ii, prm->physics};
+  const int nth = prm->nthreads > 0 ? prm->nthreads : omp_get_max_threads();
+  const double t0 = now_s();
+  // ranks by octant, particles in input order (Init, main.f90:306-316)
+  std::vector<int64_t> ie[8], ii[8];
+  std::vector<double> xe[8], xi[8];
+  for (int64_t i = 0; i < n_el; ++i) ie[octant_of(x_el + 3 * i)].push_back(i);
+  for (int64_t i = 0; i < n_ion; ++i) ii[octant_of(x_ion + 3 * i)].push_back(i);
+  Tree Te[8], Ti[8];
+  int rc = 0;
+  for (int r = 0; r < 8 && rc == 0; ++r) {
+    for (int64_t g : ie[r]) xe[r].insert(xe[r].end(), x_el + 3 * g, x_el + 3 * g + 3);
+    for (int64_t g : ii[r]) xi[r].insert(xi[r].end(), x_ion + 3 * g, x_ion + 3 * g + 3);
+    if (!ie[r].empty()) rc = build_tree(Te[r], (int64_t)ie[r].size(), xe[r].data(), -1);
+    if (rc == 0 && !ii[r].empty())
+      rc = build_tree(Ti[r], (int64_t)ii[r].size(), xi[r].data(), +1);
+  }
+  // ghost trees: rank s sends to DEST(i) = (s + i) mod 8 (mpienv.f90:58-65)
+  BT* Ge[8][8] = {};
+  BT* Gi[8][8] = {};
+  int64_t gn_e = 0, gn_i = 0;
+  if (rc == 0)
+    for (int s = 0; s < 8; ++s)
+      for (int i = 1; i < 8; ++i) {
+        const int r = (s + i) % 8;
+        const int c = contact_case(r, s);
+        if (Te[s].root) Ge[s][r] = copy_ghost(Te[s].root, c, p.theta, gn_e);
+        if (Ti[s].root) Gi[s][r] = copy_ghost(Ti[s].root, c, p.theta, gn_i);
+      }
+  const double t1 = now_s();
+  int64_t nm2p = 0, np2p = 0, gm2p = 0, gp2p = 0;
+  double ep_e = 0.0, ep_i = 0.0;
+  std::vector<int64_t> hei((size_t)(kNdist + 1) * nth, 0),
+      hii((size_t)(kNdist + 1) * nth, 0);
+  if (rc == 0) {
+#pragma omp parallel num_threads(nth) reduction(+ : nm2p, np2p, gm2p, gp2p, ep_e, ep_i)
+    {
+      const int tid = omp_get_thread_num();
+      int64_t* my_ei = hei.data() + (size_t)(kNdist + 1) * tid;
+      int64_t* my_ii = hii.data() + (size_t)(kNdist + 1) * tid;
+      for (int r = 0; r < 8; ++r) {
+        const int64_t ne = (int64_t)ie[r].size(), ni = (int64_t)ii[r].size();
+#pragma omp for schedule(static)
+        for (int64_t k = 0; k < ne; ++k) {
+          Acc a{{0.0, 0.0, 0.0}, 0.0, 0, 0};
+          const double* xt = xe[r].data() + 3 * k;
+          if (Te[r].root) search(Te[r].root, xt, -1, -1, k, p, a, nullptr);
+          const double e_ee = a.epot;
+          a.epot = 0.0;
+          if (Ti[r].root) search(Ti[r].root, xt, -1, +1, -1, p, a, my_ei);
+          const double e_loc = e_ee + a.epot;
+          a.epot = 0.0;
+          const int64_t lm = a.n_m2p, lp = a.n_p2p;
+          for (int i = 1; i < 8; ++i)
+            if (BT* G = Ge[(r - i + 8) % 8][r]) ghost_search(G, xt, -1, -1, p, a, nullptr);
+          for (int i = 1; i < 8; ++i)
+            if (BT* G = Gi[(r - i + 8) % 8][r]) ghost_search(G, xt, -1, +1, p, a, my_ei);
+          const int64_t g = ie[r][k];
+          for (int d = 0; d < 3; ++d) f_el[3 * g + d] = a.f[d];
+          ep_e += e_loc + a.epot;
+          nm2p += a.n_m2p;
+          np2p += a.n_p2p;
+          gm2p += a.n_m2p - lm;
+          gp2p += a.n_p2p - lp;
+        }
+#pragma omp for schedule(static)
+        for (int64_t k = 0; k < ni; ++k) {
+          Acc a{{0.0, 0.0, 0.0}, 0.0, 0, 0};
+          const double* xt = xi[r].data() + 3 * k;
+          if (Te[r].root) search(Te[r].root, xt, +1, -1, -1, p, a, my_ei);
+          const double e_ie = a.epot;
+          a.epot = 0.0;
+          if (Ti[r].root) search(Ti[r].root, xt, +1, +1, k, p, a, my_ii);
+          double e_ii = a.epot;
+          a.epot = 0.0;
+          const int64_t lm = a.n_m2p, lp = a.n_p2p;
+          for (int i = 1; i < 8; ++i)
+            if (BT* G = Ge[(r - i + 8) % 8][r]) ghost_search(G, xt, +1, -1, p, a, my_ei);
+          const double e_gie = a.epot;
+          a.epot = 0.0;
+          for (int i = 1; i < 8; ++i)
+            if (BT* G = Gi[(r - i + 8) % 8][r]) ghost_search(G, xt, +1, +1, p, a, my_ii);
+          e_ii += a.epot;
+          const int64_t g = ii[r][k];
+          for (int d = 0; d < 3; ++d) f_ion[3 * g + d] = a.f[d];
+          ep_e += e_ie + e_gie;
+          ep_i += e_ii;
+          nm2p += a.n_m2p;
+          np2p += a.n_p2p;
+          gm2p += a.n_m2p - lm;
+          gp2p += a.n_p2p - lp;
+        }
+      }
+    }
+    for (int t = 0; t < nth; ++t)
+      for (int b = 0; b <= kNdist; ++b) {
+        if (rdf_ei) rdf_ei[b] += hei[(size_t)(kNdist + 1) * t + b];
+        if (rdf_ii) rdf_ii[b] += hii[(size_t)(kNdist + 1) * t + b];
+      }
+  }
+  const double t2 = now_s();
+  if (rc == 0 && epot) {
+    epot[0] = ep_e;
+    epot[1] = ep_i;
+  }
+  if (st) {
+    st->n_m2p = nm2p;
+    st->n_p2p = np2p;
+    st->max_depth_e = 0;
+    st->max_depth_i = 0;
+    for (int r = 0; r < 8; ++r) {
+      if (Te[r].max_depth > st->max_depth_e) st->max_depth_e = Te[r].max_depth;
+      if (Ti[r].max_depth > st->max_depth_i) st->max_depth_i = Ti[r].max_depth;
+    }
+    st->t_build = t1 - t0;
+    st->t_walk = t2 - t1;
+  }
+  if (st8) {
+    for (int r = 0; r < 8; ++r) {
+      st8->n_el[r] = (int64_t)ie[r].size();
+      st8->n_ion[r] = (int64_t)ii[r].size();
+    }
+    st8->ghost_nodes_e = gn_e;
+    st8->ghost_nodes_i = gn_i;
+    st8->n_m2p_ghost = gm2p;
+    st8->n_p2p_ghost = gp2p;
+  }
+  for (int s = 0; s < 8; ++s) {
+    for (int r = 0; r < 8; ++r) {
+      dealloc(Ge[s][r]);
+      dealloc(Gi[s][r]);
+    }
+    dealloc(Te[s].root);
+    dealloc(Ti[s].root);
+  }
+  return rc;
+}
+
+}  // extern "C"
