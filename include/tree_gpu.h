@@ -28,7 +28,7 @@ extern "C" {
 #define TREE_GPU_OK 0
 #define TREE_GPU_ERR_ARG -1        /* bad argument / size */
 #define TREE_GPU_ERR_DEPTH -2      /* two same-species particles share the
-                                      deepest (21-level) cell; the reference
+                                      deepest (42-level) cell; the reference
                                       recurses forever here (tree.f90:128-273) */
 #define TREE_GPU_ERR_NONFINITE -3  /* NaN/Inf position */
 #define TREE_GPU_ERR_CAPACITY -4   /* internal node capacity exceeded */
@@ -196,15 +196,22 @@ int tree_gpu_direct(tree_gpu_handle* h, const int64_t* targets, int64_t nt,
  *   d_f, d_epot  outputs: 3*nt forces and nt values of 0.5*sum V
  *   stream    cudaStream_t to run on (NULL: the default stream)
  * Its scratch is a file-scope static device array of 8 MiB that every GPU
- * loading this library keeps until the process exits.  nt may be at most
- * TREE_GPU_DIRECT_STATIC_MAX_TARGETS (larger lists return
+ * loading this library keeps until the process exits.  The array is committed
+ * on a device when the library's direct-sum module is first loaded there:
+ * with CUDA's default lazy module loading that is the first call of
+ * tree_gpu_direct or tree_gpu_direct_static on that device (a caller whose
+ * memory manager takes all free memory should make one such call, or set
+ * CUDA_MODULE_LOADING=EAGER, before it does); later calls commit nothing.
+ * nt may be at most TREE_GPU_DIRECT_STATIC_MAX_TARGETS (larger lists return
  * TREE_GPU_ERR_CAPACITY and do no work); an index outside [0, n) returns
  * TREE_GPU_ERR_ARG (it is replaced by 0 on the device, so nothing is read out
  * of bounds).  The first call on each device looks up the scratch address
  * (cudaGetSymbolAddress), so make that first call before any stream capture.
  * All calls share the one array and its contents persist between calls:
- * calls that overlap on the GPU (other streams or threads) race on it.  The
- * call returns after `stream` has finished the work. */
+ * calls that overlap on the GPU (other streams or threads) race on it.  Each
+ * launch's status is checked on its own, so an error left by the caller's
+ * earlier work is neither reported nor cleared.  The call copies a 4-byte
+ * error word to the host and synchronises `stream` before it returns. */
 #define TREE_GPU_DIRECT_STATIC_MAX_TARGETS 65536
 int tree_gpu_direct_static(const double* d_x, int64_t n_el, int64_t n_ion,
                            const tree_gpu_params* params,

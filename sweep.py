@@ -1,8 +1,8 @@
 """Long-run measurements of the force path on one GPU.
 
-    python -m tree_b200.sweep precision [--n 1048576] [--steps 1000]
-    python -m tree_b200.sweep drift [--n 1048576] [--steps 1000]
-    python -m tree_b200.sweep learned [--n 4194304] [--steps 500]
+    python sweep.py precision [--n 1048576] [--steps 1000]
+    python sweep.py drift [--n 1048576] [--steps 1000]
+    python sweep.py learned [--n 4194304] [--steps 500]
 
 precision: the precision form -- seeded clouds at T_e in {10, 50, 200} K,
     each run with the mixed-precision walk at opening angles {0.3, 0.5, 0.7}
@@ -27,11 +27,14 @@ density 1e15 m^-3, electrons on their ions at t = 0, T_i = 1 mK, dt = 1e-11 s).
 """
 import argparse
 import json
+import os
+import sys
 import time
 
 import numpy as np
 
-from . import api, cloud, learned_mac, units
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from tree_b200 import api, cloud, learned_mac, units  # noqa: E402
 
 
 def _audit(tf, idx):

@@ -45,21 +45,36 @@ def test_static_direct_matches_allocating_direct(device_lib, physics):
     stream = torch.cuda.Stream()
     with api.TreeForce(n_el, n_ion, cfg) as tf:
         tf.force(x_el, x_ion)  # puts the same positions on the device
-        for call, nt in enumerate((5000, 1234)):  # two calls in a row
+        # two calls in a row, every buffer made before the first
+        calls = []
+        for nt in (5000, 1234):
             t = np.sort(rng.choice(n_el + n_ion, nt, replace=False)).astype(np.int64)
             f_ref, e_ref = tf.direct(t)
-            t_dev = torch.from_numpy(t).cuda()
-            f_dev = torch.full((3 * nt,), float("nan"), dtype=torch.float64, device="cuda")
-            e_dev = torch.full((nt,), float("nan"), dtype=torch.float64, device="cuda")
+            calls.append(dict(nt=nt, f_ref=f_ref, e_ref=e_ref,
+                              t_dev=torch.from_numpy(t).cuda(),
+                              f_dev=torch.full((3 * nt,), float("nan"), dtype=torch.float64,
+                                               device="cuda"),
+                              e_dev=torch.full((nt,), float("nan"), dtype=torch.float64,
+                                               device="cuda")))
+        torch.cuda.synchronize()
+        free = []
+        for k, c in enumerate(calls):
+            free.append(torch.cuda.mem_get_info()[0])
+            rc = _static_call(device_lib, x_dev, n_el, n_ion, params, c["t_dev"], c["nt"],
+                              c["f_dev"], c["e_dev"], stream.cuda_stream)
+            assert rc == 0, f"call {k}: status {rc}"
             torch.cuda.synchronize()
-            rc = _static_call(device_lib, x_dev, n_el, n_ion, params, t_dev, nt,
-                              f_dev, e_dev, stream.cuda_stream)
-            assert rc == 0, f"call {call}: status {rc}"
-            f = f_dev.cpu().numpy().reshape(-1, 3)
-            e = e_dev.cpu().numpy()
-            assert np.all(np.isfinite(f)) and np.all(np.isfinite(e))
-            assert _rel_err(f, f_ref).max() <= TOL
-            np.testing.assert_allclose(e, e_ref, rtol=TOL, atol=TOL * np.abs(e_ref).max())
+        free.append(torch.cuda.mem_get_info()[0])
+        # the first call may load the module that holds the static array; the
+        # second takes no device memory at all
+        assert free[2] == free[1], f"free device memory changed by {free[1] - free[2]} bytes"
+        for k, c in enumerate(calls):
+            f = c["f_dev"].cpu().numpy().reshape(-1, 3)
+            e = c["e_dev"].cpu().numpy()
+            assert np.all(np.isfinite(f)) and np.all(np.isfinite(e)), f"call {k}"
+            assert _rel_err(f, c["f_ref"]).max() <= TOL, f"call {k}"
+            np.testing.assert_allclose(e, c["e_ref"], rtol=TOL,
+                                       atol=TOL * np.abs(c["e_ref"]).max())
 
 
 def test_static_direct_rejects_oversize_and_bad_indices(device_lib):

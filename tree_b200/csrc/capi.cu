@@ -327,7 +327,7 @@ int check_device_status(tree_gpu_handle* h, bool* grow) {
     return fail(h, TREE_GPU_ERR_NONFINITE, "non-finite particle position");
   if (err & tg::kErrDepth)
     return fail(h, TREE_GPU_ERR_DEPTH,
-                "two same-species particles share a 21-level cell");
+                "two same-species particles share a 42-level cell");
   if (err & tg::kErrCapacity) {
     *grow = true;
     return TREE_GPU_OK;

@@ -164,6 +164,33 @@ double kelbg_lambda_um_static(double mu_amu, double te) {
   return 1.054571817e-34 / sqrt(2.0 * mu_amu * 1.66053906660e-27 * 1.380649e-23 * te) * 1e6;
 }
 
+// The launches of the allocation-free call, each returning its own status.
+cudaError_t launch_sanitize(const int64_t* in, int nt, int64_t n, int64_t* out,
+                            int32_t* flag, cudaStream_t st) {
+  void* args[] = {(void*)&in, (void*)&nt, (void*)&n, (void*)&out, (void*)&flag};
+  return cudaLaunchKernel((const void*)k_sanitize_targets, dim3((nt + 255) / 256),
+                          dim3(256), args, 0, st);
+}
+
+cudaError_t launch_direct(const double* x, int n, int n_el, const int64_t* targets,
+                          int nt, tg::WalkParams wp, int nchunks, double4* partial,
+                          double* f, double* epot, cudaStream_t st) {
+  // the grid of tg::direct_sum: tiles of kDirT targets x source chunks
+  int chunk = (n + nchunks - 1) / nchunks;
+  chunk = (chunk + tg::kDirT - 1) / tg::kDirT * tg::kDirT;
+  const int nch = (n + chunk - 1) / chunk;
+  const dim3 grid((nt + tg::kDirT - 1) / tg::kDirT, nch);
+  void* a1[] = {(void*)&x, (void*)&n, (void*)&n_el, (void*)&targets, (void*)&nt,
+                (void*)&chunk, (void*)&wp, (void*)&partial};
+  const void* kfn = wp.physics == 0 ? (const void*)tg::k_direct<0> : (const void*)tg::k_direct<1>;
+  cudaError_t e = cudaLaunchKernel(kfn, grid, dim3(tg::kDirT), a1, 0, st);
+  if (e != cudaSuccess) return e;
+  int nchv = nch;
+  void* a2[] = {(void*)&partial, (void*)&nt, (void*)&nchv, (void*)&f, (void*)&epot};
+  return cudaLaunchKernel((const void*)tg::k_direct_reduce, dim3((nt + 255) / 256),
+                          dim3(256), a2, 0, st);
+}
+
 }  // namespace
 
 extern "C" int tree_gpu_direct_static(const double* d_x, int64_t n_el,
@@ -210,10 +237,13 @@ extern "C" int tree_gpu_direct_static(const double* d_x, int64_t n_el,
   cudaStream_t st = (cudaStream_t)stream;
   // the error word keeps the previous call's value: clear it first
   if (cudaMemsetAsync(flag, 0, sizeof(int32_t), st) != cudaSuccess) return TREE_GPU_ERR_CUDA;
-  k_sanitize_targets<<<(int)((nt + 255) / 256), 256, 0, st>>>(d_targets, (int)nt, n, targets, flag);
-  tg::direct_sum(d_x, (int)n, (int)n_el, targets, (int)nt, wp, nch, partial,
-                 d_f, d_epot, st);
-  if (cudaGetLastError() != cudaSuccess) return TREE_GPU_ERR_CUDA;
+  // Each launch reports its own status (cudaLaunchKernel), so an error left
+  // behind by the caller's earlier work is neither reported as this call's
+  // nor cleared.
+  if (launch_sanitize(d_targets, (int)nt, n, targets, flag, st) != cudaSuccess ||
+      launch_direct(d_x, (int)n, (int)n_el, targets, (int)nt, wp, nch, partial, d_f,
+                    d_epot, st) != cudaSuccess)
+    return TREE_GPU_ERR_CUDA;
   int32_t hflag = 0;
   if (cudaMemcpyAsync(&hflag, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
