@@ -1,18 +1,24 @@
 #!/usr/bin/env python
 """Benchmark of the TREE force path: particle-steps/s at N = 1,048,576.
 
-One step = VVerletNotemp1 -> Force (octree build + upward pass + tree walk)
--> VVerletNotemp2, the loop body of main.f90:123-131 of hpjeonGIT/TREE, on a
-seeded synthetic ultracold-plasma cloud (isotropic Gaussian of ions at peak
-density 1e15 m^-3 with each electron starting on its ion, T_e = 50 K,
-T_i = 1 mK, dt = 1e-11 s).  The inputs (positions, velocities, trees) are far
-larger than the 126 MB L2 and every step rebuilds the trees from scratch.
+One step = VVerletNotemp1 -> Force (octree build + upward pass + tree walk,
+with the e-i / i-i RDF pair counts of every step) -> VVerletNotemp2, the loop
+body of main.f90:123-131 of hpjeonGIT/TREE, with the TEMPORAL kinetic sums on
+every step with Nloop % nsamp == 0 (vverlet.f90:81-106); the timed loop is
+one tree_gpu_run call.  Workload: a seeded synthetic ultracold-plasma cloud
+(isotropic Gaussian of ions at peak density 1e15 m^-3 with each electron
+starting on its ion, T_e = 50 K, T_i = 1 mK, dt = 1e-11 s, erf-Kelbg pair
+laws).  The inputs (positions, velocities, trees) are far larger than the
+126 MB L2 and every step rebuilds the trees from scratch.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 `--impl reference` times the CPU restatement of the reference algorithm
-(pointer octree, serial insertion, recursive OpenMP walks in FP64 with the
-reference pair laws) on the host cores, on a bounded sample of each step.
+(pointer octree, serial insertion, recursive OpenMP walks in FP64) on all host
+cores, on the same workload configuration (opening angle, pair laws, RDF
+every step): whole steps from the t = 0 cloud after the untimed initial force
+(Vinit), until K steps or the time budget --ref-budget, whichever comes
+first; the line reports the steps it actually timed.
 With N > 1 GPUs every rank runs an independent replica of the workload (the
 path has no exchange step); value = all particles x steps / max rank time.
 """
@@ -31,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s at N=1,048,576 (force path: build + upward + walk + KDK)"
 UNIT = "particle-steps/s"
+DT_S = 1e-11
 
 # Algorithmic flops per interaction, counted from the kernels' formulas
 # (FMA = 2; divisions, square roots and exponentials count as one flop each).
@@ -39,12 +46,17 @@ FLOPS_P2P_REF = 30     # leaf laws of tree.f90 / erf-Kelbg with the x^2>40 short
 FLOPS_M2P_MIXED = {2: 50, 3: 100}  # FP32 trace-free far field to quadrupole / octupole
 FLOPS_P2P_MIXED = 24   # FP32 erf-Kelbg pair with hi/lo offsets
 FLOPS_MLP = 2 * (16 * 64 + 64 * 64 + 64)  # one learned-MAC evaluation (BF16 mma + FP32)
+RDF_BYTES = 2 * 10001 * 8  # the two 64-bit RDF histograms read back per call
+SAMPLE_BYTES = 48          # one TEMPORAL record
 
 # Headline configuration: mixed precision, learned MAC on top of theta = 0.30,
 # octupole far field; chosen so the rms relative force error against the FP64
 # direct sum stays below 1e-4 at this workload (measured by the accuracy audit
 # below, which every run reports).
 HEADLINE = dict(theta=0.30, eta=3e-5, order=3, bucket=8)
+# Ensemble of 64 clouds: the autotuner's pick on that workload (learned MAC at
+# theta = 0.26, eta = 3e-5), fixed here so that the bench does no tuning.
+ENSEMBLE_TUNED = dict(theta=0.26, eta=3e-5, bucket=8, order=3, blocks_per_sm=4)
 
 
 def parse():
@@ -62,6 +74,10 @@ def parse():
     ap.add_argument("--eta", type=float, default=HEADLINE["eta"])
     ap.add_argument("--order", type=int, default=HEADLINE["order"])
     ap.add_argument("--bucket", type=int, default=HEADLINE["bucket"])
+    ap.add_argument("--nsamp", type=int, default=10,
+                    help="TEMPORAL cadence of the timed loop (Nloop %% nsamp == 0)")
+    ap.add_argument("--no-rdf", action="store_true",
+                    help="time the loop without the per-step RDF pair counts")
     ap.add_argument("--workload", choices=["cloud", "ensemble"], default="cloud",
                     help="cloud: one N=1,048,576 cloud (headline); ensemble: 64 "
                          "independent clouds of uneven N in one handle")
@@ -70,8 +86,16 @@ def parse():
                     help="ensemble: autotune theta/eta/bucket/grid on the warm state")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the fixed-theta and plain-FP64 comparison arms")
-    ap.add_argument("--ref-theta", type=float, default=0.5,
-                    help="opening angle of the reference CPU path (its own setting)")
+    ap.add_argument("--fp64-thetas", default="0.35,0.25",
+                    help="extra opening angles of the plain FP64 path (2 steps each) "
+                         "for the equal-accuracy comparison")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the ensemble sub-record of the cloud workload")
+    ap.add_argument("--ref-budget", type=float, default=100.0,
+                    help="reference arm: stop timing whole steps after this many seconds")
+    ap.add_argument("--ref-also-theta05", action="store_true",
+                    help="reference arm: also time one whole Force call at the "
+                         "reference's own theta = 0.5 with its own pair laws")
     ap.add_argument("--te", type=float, default=50.0)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--audit", type=int, default=16384,
@@ -142,6 +166,20 @@ def make_workload(n, seed, te):
     return cloud.make_cloud(n, seed=seed, te_k=te, ti_k=1e-3)
 
 
+def workload_config(args, n):
+    """The workload both arms run (no method keys): the same dict in the
+    reference arm's line and in ours."""
+    rdf = not args.no_rdf
+    laws = "erf-Kelbg" if args.physics == "kelbg" else "reference (Coulomb + exp-screened e-i)"
+    return {"workload": f"UCP cloud N={n} per GPU, T_e={args.te} K, T_i=1 mK, theta={args.theta}, "
+                        f"{laws} pair laws, dt=1e-11 s, "
+                        f"{'RDF pair counts every step, ' if rdf else ''}"
+                        f"TEMPORAL sums every {args.nsamp} steps",
+            "n_particles": n, "theta": args.theta, "te_k": args.te, "ti_k": 1e-3,
+            "physics": args.physics, "dt_s": DT_S, "rdf": rdf, "nsamp": args.nsamp,
+            "l2": "inputs larger than L2 (x,v,f 72 MB + trees >150 MB, rebuilt every step)"}
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -154,8 +192,7 @@ def profile_traffic(kernel):
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
-    d = json.load(open(path)).get(kernel)
-    return d
+    return json.load(open(path)).get(kernel)
 
 
 def fp_peak_tflops(sm_mhz, fp64):
@@ -166,24 +203,33 @@ def fp_peak_tflops(sm_mhz, fp64):
     return sms * lanes * 2 * sm_mhz * 1e6 / 1e12
 
 
-def cpu_sample(c_state, args, stride):
-    """Times the oracle on the same state: full tree build, walk of every
-    stride-th target; returns (particle-steps/s estimate, details)."""
+def oracle_params(args, theta=None, physics=None):
     import oracle
     from tree_b200 import units
     lam = units.kelbg_lambdas(args.te)
-    p = oracle.make_params(theta=args.ref_theta, rs=lam[1], lambdas=lam,
-                           physics=oracle.PHYS_REF)
+    phys = physics if physics is not None else (
+        oracle.PHYS_KELBG if args.physics == "kelbg" else oracle.PHYS_REF)
+    return oracle.make_params(theta=args.theta if theta is None else theta, rs=lam[1],
+                              dx_ei=0.01, dx_ii=0.1, lambdas=lam, physics=phys)
+
+
+def cpu_sample(c_state, args, stride):
+    """Times the oracle on a state at the workload's configuration: full build
+    of both trees, walk of every stride-th target; returns (particle-steps/s
+    estimate, details)."""
+    import oracle
+    from tree_b200 import units
+    p = oracle_params(args)
     x_el, x_ion = c_state["x_el"], c_state["x_ion"]
     n = len(x_el) + len(x_ion)
     t0 = time.perf_counter()
-    r = oracle.force(x_el, x_ion, p, rdf=True, stride=stride)
+    r = oracle.force(x_el, x_ion, p, rdf=not args.no_rdf, stride=stride)
     wall = time.perf_counter() - t0
     st = r["stats"]
     xe, ve = x_el.copy(), c_state["v_el"].copy()
     t1 = time.perf_counter()
-    oracle.kdk1(xe, ve, r["f_el"], units.dt_code(1e-11), units.M_ELECTRON_AMU)
-    oracle.kdk2(ve, r["f_el"], units.dt_code(1e-11), units.M_ELECTRON_AMU)
+    oracle.kdk1(xe, ve, r["f_el"], units.dt_code(DT_S), units.M_ELECTRON_AMU)
+    oracle.kdk2(ve, r["f_el"], units.dt_code(DT_S), units.M_ELECTRON_AMU)
     t_kdk = (time.perf_counter() - t1) * n / max(len(xe), 1)
     t_step = st["t_build"] + st["t_walk"] * stride + t_kdk
     return n / t_step, dict(t_build=st["t_build"], t_walk_sample=st["t_walk"],
@@ -210,6 +256,34 @@ def auto_stride(n):
     return max(1, int(round(n / 16384)))
 
 
+def power_law(xs, ys):
+    """Least-squares fit log y = a + b log x; returns (a, b)."""
+    lx, ly = np.log(np.asarray(xs, float)), np.log(np.asarray(ys, float))
+    b, a = np.polyfit(lx, ly, 1)
+    return float(a), float(b)
+
+
+def equal_accuracy(points, target=1e-4):
+    """From (theta, rms, ms_per_step) of one path at several opening angles,
+    the opening angle where rms reaches `target` and the time per step there,
+    by power laws in theta fitted to the points (an extrapolation when the
+    target lies outside them)."""
+    pts = [p for p in points if p[1] and p[1] > 0 and p[2] > 0]
+    if len(pts) < 2:
+        return None
+    th = [p[0] for p in pts]
+    a_e, b_e = power_law(th, [p[1] for p in pts])
+    a_t, b_t = power_law(th, [p[2] for p in pts])
+    if b_e <= 0:
+        return None
+    theta_t = float(np.exp((np.log(target) - a_e) / b_e))
+    ms_t = float(np.exp(a_t + b_t * np.log(theta_t)))
+    return {"target_rms": target, "theta": theta_t, "ms_per_step": ms_t,
+            "rms_exponent": b_e, "time_exponent": b_t,
+            "extrapolated": bool(theta_t < min(th) or theta_t > max(th)),
+            "points": [{"theta": p[0], "rms": p[1], "ms_per_step": p[2]} for p in pts]}
+
+
 # ------------------------------------------------------------- replicas ----
 def max_over_ranks(value, dist):
     """The largest `value` over all ranks (the value itself without a process
@@ -230,47 +304,109 @@ def whole_job_rate(n_per_rank, world, steps, ms):
 
 # ----------------------------------------------------------- reference arm ----
 def run_reference(args, rank, world):
+    """Whole steps of the reference algorithm (the oracle) on the host cores:
+    the initial force (Vinit, main.f90:777) untimed, then per step
+    VVerletNotemp1 -> Force (with RDF) -> VVerletNotemp2 (main.f90:123-131),
+    the kinetic sums on sample steps, until K steps or the time budget."""
     if rank != 0:
         return
     import oracle
+    from tree_b200 import units
+    flags = oracle.use_native()
     c = make_workload(args.n, args.seed, args.te)
-    rng = np.random.Generator(np.random.Philox(args.seed + 1))
-    # the state a few steps after t = 0: each electron near its ion
-    state = dict(x_el=c.x_ion + rng.standard_normal(c.x_ion.shape) * 0.3,
-                 x_ion=c.x_ion, v_el=c.v_el)
-    stride = args.cpu_stride or auto_stride(args.n)
-    for _ in range(args.warmup):
-        cpu_sample(state, args, stride * 4)
-    vals, det = [], None
-    for _ in range(args.steps):
-        v, det = cpu_sample(state, args, stride)
-        vals.append(v)
-    value = float(np.median(vals))
+    n = len(c.x_el) + len(c.x_ion)
+    dt = units.dt_code(DT_S)
+    p = oracle_params(args)
+    rdf = not args.no_rdf
+    xe, ve, xi, vi = c.x_el.copy(), c.v_el.copy(), c.x_ion.copy(), c.v_ion.copy()
+    t0 = time.perf_counter()
+    r = oracle.force(xe, xi, p, rdf=False)  # Vinit's force, untimed
+    t_init = time.perf_counter() - t0
+    fe, fi = r["f_el"], r["f_ion"]
+    rei = np.zeros(oracle.NBINS, np.int64)
+    rii = np.zeros(oracle.NBINS, np.int64)
+    times, phases = [], []
+    for k in range(max(args.steps, 1)):
+        a = time.perf_counter()
+        oracle.kdk1(xe, ve, fe, dt, units.M_ELECTRON_AMU)
+        oracle.kdk1(xi, vi, fi, dt, units.M_ION_AMU)
+        r = oracle.force(xe, xi, p, rdf=rdf)
+        fe, fi = r["f_el"], r["f_ion"]
+        if rdf:
+            rei += r["rdf_ei"]
+            rii += r["rdf_ii"]
+        oracle.kdk2(ve, fe, dt, units.M_ELECTRON_AMU)
+        oracle.kdk2(vi, fi, dt, units.M_ION_AMU)
+        if args.nsamp > 0 and (k + 1) % args.nsamp == 0:
+            oracle.ke(xe, ve, units.M_ELECTRON_AMU)
+            oracle.ke(xi, vi, units.M_ION_AMU)
+        times.append(time.perf_counter() - a)
+        phases.append({"build_s": r["stats"]["t_build"], "walk_s": r["stats"]["t_walk"],
+                       "n_m2p": r["stats"]["n_m2p"], "n_p2p": r["stats"]["n_p2p"]})
+        if sum(times) >= args.ref_budget:
+            break
+    steps = len(times)
+    total = sum(times)
+    value = n * steps / total
     cores = oracle.max_threads()
+    extra = None
+    if args.ref_also_theta05:
+        p05 = oracle_params(args, theta=0.5, physics=oracle.PHYS_REF)
+        a = time.perf_counter()
+        r05 = oracle.force(xe, xi, p05, rdf=rdf)
+        t05 = time.perf_counter() - a
+        extra = {"theta": 0.5, "pair_laws": "reference (Coulomb, exp-screened e-i, rs = lambda_ei)",
+                 "force_s": t05, "particle_steps_per_s_force_only": n / t05,
+                 "n_m2p": r05["stats"]["n_m2p"], "n_p2p": r05["stats"]["n_p2p"]}
+    sample = (f"{steps} whole steps (VVerletNotemp1 + Force{' with RDF' if rdf else ''} + "
+              f"VVerletNotemp2) of N={n} from the t = 0 cloud, after the untimed initial "
+              f"force ({t_init:.1f} s); stopped at K={args.steps} steps or "
+              f"{args.ref_budget:.0f} s of timed work")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * args.n / value, "higher_is_better": True,
+        "n_gpus": world, "steps": steps, "warmup": 0,
+        "ms_per_step": 1e3 * total / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Gaussian UCP cloud)",
-        "config": {"workload": f"UCP cloud N={args.n}, T_e={args.te} K, T_i=1 mK, "
-                               f"dt=1e-11 s; reference algorithm at its own opening angle "
-                               f"theta={args.ref_theta} (less accurate than the GPU arm's "
-                               f"rms <= 1e-4), reference pair laws, FP64",
-                   "n_particles": args.n, "theta": args.ref_theta},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
-                         "kind": "port",
-                         "sample": f"full build of both trees + walk of every "
-                                   f"{stride}th target, walk time x{stride}; "
-                                   f"median of {args.steps} samples",
-                         "detail": det},
+        "data": "synthetic (seeded Gaussian UCP cloud, electrons start on ions)",
+        "config": workload_config(args, n),
+        "method": {"algorithm": "reference (tree.f90:39-1133): per-species pointer octrees, "
+                                "serial insertion, one-level moments, recursive per-target "
+                                "walks (OpenMP, static schedule), FP64",
+                   "mac": f"fixed theta = {args.theta}",
+                   "implementation": f"oracle/tree_oracle.cpp (C++ restatement, {flags})"},
+        "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "untimed": {"initial_force_s": t_init},
+        "per_step_s": times, "per_step_phases": phases,
+        "rdf_pairs_counted": int(rei.sum() + rii.sum()),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_theta0.5": extra,
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ ours ----
+def _timed_run(tf, stream, dt, steps, nsamp, rdf, dist):
+    """tree_gpu_run of `steps` steps between CUDA events on the library's
+    stream; returns (ms max over ranks, rdf pair count)."""
+    import torch
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = tf.run(dt, steps, nsamp=nsamp, rdf=rdf)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    pairs = int(out[1][0].sum() + out[1][1].sum()) if rdf else None
+    return max_over_ranks(e0.elapsed_time(e1), dist), pairs
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -284,7 +420,8 @@ def run_ours(args, rank, world, dist):
            else api.MAC_FIXED)
     cfg = api.Config(theta=args.theta, te=args.te, physics=phys, precision=prec,
                      mac=mac)
-    dt = units.dt_code(1e-11)
+    dt = units.dt_code(DT_S)
+    rdf = not args.no_rdf
     c = make_workload(args.n, args.seed + rank, args.te)
     n_el, n_ion = len(c.x_el), len(c.x_ion)
     n = n_el + n_ion
@@ -295,40 +432,33 @@ def run_ours(args, rank, world, dist):
         tf.set_tuning(args.bucket, 4, args.order)
         if mac == api.MAC_LEARNED:
             from tree_b200 import learned_mac
-            params, stats, _ = learned_mac.load_model()
+            params, stats, _ = learned_mac.load_model(order=args.order)
             tf.mac_set_model(params, stats)
             tf.mac_config(args.eta, 0.05, 0.9)
     tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
-    tf.step(dt, max(args.warmup, 3))  # warm-up; e-i pairs separate
+    warm = max(args.warmup, 3)
+    tf.run(dt, warm, nsamp=args.nsamp, rdf=rdf)  # warm-up; e-i pairs separate
     torch.cuda.synchronize()
     st_warm = tf.get_state()  # every comparison arm starts from this state
     if dist:
         dist.barrier()
 
-    # ---- timed region: device-resident state, K steps in one call ----
+    # ---- timed region: device-resident state, K steps in one tree_gpu_run ----
     t_before = tf.timings()
     clocks = ClockSampler(dev)
     clocks.start()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    diag = tf.step(dt, args.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    ms, rdf_pairs = _timed_run(tf, stream, dt, args.steps, args.nsamp, rdf, dist)
     clk = clocks.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     t_after = tf.timings()
     value = whole_job_rate(n, world, args.steps, ms)
-    walk_ms = (t_after.ms_walk - t_before.ms_walk) / args.steps
-    build_ms = (t_after.ms_build - t_before.ms_build) / args.steps
+    walk_ms_sum = t_after.ms_walk - t_before.ms_walk
+    build_ms_sum = t_after.ms_build - t_before.ms_build
+    walk_ms = walk_ms_sum / args.steps
+    build_ms = build_ms_sum / args.steps
     launches = t_after.launches - t_before.launches
-    n_m2p, n_p2p = t_after.n_m2p, t_after.n_p2p
-    n_net = t_after.n_mac_net
+    d_m2p = t_after.n_m2p_total - t_before.n_m2p_total
+    d_p2p = t_after.n_p2p_total - t_before.n_p2p_total
+    d_net = t_after.n_mac_net_total - t_before.n_mac_net_total
 
     # ---- accuracy audit of the last timed step: FP64 direct sum ----
     audit_idx = None
@@ -337,7 +467,7 @@ def run_ours(args, rank, world, dist):
         audit_idx = np.sort(rng.choice(n, min(args.audit, n), replace=False))
     accuracy = audit(tf, audit_idx)
 
-    # ---- end to end: full state host->device, one step, state back ----
+    # ---- end to end: full state host->device, one step, state + RDF back ----
     e2e = None
     if not args.no_e2e:
         st = tf.get_state()
@@ -353,24 +483,25 @@ def run_ours(args, rank, world, dist):
         for _ in range(k2):
             tf.load_state(ptr["x_el"], ptr["v_el"], ptr["f_el"], ptr["x_ion"],
                           ptr["v_ion"], ptr["f_ion"])
-            tf.step(dt, 1)
+            tf.run(dt, 1, nsamp=1, rdf=rdf)
             tf.get_state_ptr(ptr["x_el"], ptr["v_el"], ptr["f_el"],
                              ptr["x_ion"], ptr["v_ion"], ptr["f_ion"])
         a1.record(stream)
         torch.cuda.synchronize()
         ems = max_over_ranks(a0.elapsed_time(a1), dist)
         e2e = {"value": whole_job_rate(n, world, k2, ems), "unit": UNIT,
-               "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n,
+               "h2d_bytes_per_step": 72 * n,
+               "d2h_bytes_per_step": 72 * n + SAMPLE_BYTES + (RDF_BYTES if rdf else 0),
                "steps": k2,
-               "path": "tree_gpu_load_state(x,v,f pinned host) + tree_gpu_step(1) "
-                       "+ tree_gpu_get_state(x,v,f pinned host)"}
+               "path": "tree_gpu_load_state(x,v,f pinned host) + tree_gpu_run(1 step, "
+                       "TEMPORAL record, RDF) + tree_gpu_get_state(x,v,f pinned host)"}
 
-    # ---- roofline of the dominant kernel (the walk) ----
+    # ---- roofline of the dominant kernel (the walk), over the timed steps ----
     fp64 = prec == api.PREC_FP64
     fm2p = FLOPS_M2P_REF if fp64 else FLOPS_M2P_MIXED[args.order]
     fp2p = FLOPS_P2P_REF if fp64 else FLOPS_P2P_MIXED
-    flops = n_m2p * fm2p + n_p2p * fp2p
-    achieved = flops / (walk_ms / 1e3) / 1e12 if walk_ms > 0 else 0.0
+    flops = d_m2p * fm2p + d_p2p * fp2p
+    achieved = flops / (walk_ms_sum / 1e3) / 1e12 if walk_ms_sum > 0 else 0.0
     sm_mhz = clk.get("sm_mhz") or 1965.0
     peak = fp_peak_tflops(sm_mhz, fp64)
     kname = "k_walk64" if fp64 else "k_walk_mixed"
@@ -382,11 +513,13 @@ def run_ours(args, rank, world, dist):
                                f"{64 if fp64 else 128} lanes x 2 x median SM clock "
                                f"{sm_mhz:.0f} MHz sampled during the run (the walk is "
                                "not a contraction; MEASURED_PEAKS.json has no CUDA-core figure)",
-                "flops_per_launch": flops, "walk_ms": walk_ms,
-                "n_m2p": n_m2p, "n_p2p": n_p2p,
+                "flops_per_launch": flops / args.steps, "walk_ms": walk_ms,
+                "n_m2p_per_launch": d_m2p / args.steps, "n_p2p_per_launch": d_p2p / args.steps,
+                "counts": f"interactions summed over the {args.steps} timed walks",
                 "flops_per_m2p": fm2p, "flops_per_p2p": fp2p,
-                "learned_mac_evals": n_net,
-                "learned_mac_tensor_tflops": n_net * FLOPS_MLP / (walk_ms / 1e3) / 1e12 if walk_ms > 0 else 0.0}
+                "learned_mac_evals_per_launch": d_net / args.steps,
+                "learned_mac_tensor_tflops": d_net * FLOPS_MLP / (walk_ms_sum / 1e3) / 1e12
+                if walk_ms_sum > 0 else 0.0}
     pk, pk_kind = peaks()
     # build phase vs HBM: ~250 B per particle algorithmic
     build_bytes = 250 * n
@@ -397,55 +530,71 @@ def run_ours(args, rank, world, dist):
     if build_roof["achieved"] and build_roof["peak"]:
         build_roof["frac"] = build_roof["achieved"] / build_roof["peak"]
 
-    # ---- comparison arms: same warm state, same number of steps ----
+    # ---- comparison arms: same warm state, same loop ----
     compare = None
     if not args.no_compare and prec == api.PREC_MIXED:
-        compare = {"from": f"the state after the {max(args.warmup, 3)} warm-up steps, "
-                           f"{args.steps} steps each, audit after the last"}
-        arms = [(f"mixed_fixed_theta{th}", api.Config(theta=th, te=args.te, physics=phys,
-                                                      precision=api.PREC_MIXED))
+        compare = {"from": f"the state after the {warm} warm-up steps; every arm runs the "
+                           f"same tree_gpu_run loop (RDF {'on' if rdf else 'off'}) and is "
+                           f"audited after its last step"}
+        arms = [(f"mixed_fixed_theta{th}", th, api.PREC_MIXED, args.steps)
                 for th in (0.30, 0.32, 0.35)]
-        arms.append(("fp64_plain_theta0.5", api.Config(theta=0.5, te=args.te, physics=phys,
-                                                       precision=api.PREC_FP64)))
-        for name, acfg in arms:
+        arms.append(("fp64_plain_theta0.5", 0.5, api.PREC_FP64, args.steps))
+        sweep = [float(t) for t in args.fp64_thetas.split(",") if t.strip()]
+        arms += [(f"fp64_plain_theta{th}", th, api.PREC_FP64, max(1, min(args.steps, 2)))
+                 for th in sweep]
+        for name, th, aprec, ksteps in arms:
+            acfg = api.Config(theta=th, te=args.te, physics=phys, precision=aprec)
             with api.TreeForce(n_el, n_ion, acfg) as tc:
                 tc.set_stream(stream.cuda_stream)
-                if acfg.precision == api.PREC_MIXED:
+                if aprec == api.PREC_MIXED:
                     tc.set_tuning(args.bucket, 4, args.order)
                 tc.load_state(st_warm["x_el"], st_warm["v_el"], st_warm["f_el"],
                               st_warm["x_ion"], st_warm["v_ion"], st_warm["f_ion"])
-                torch.cuda.synchronize()
                 tb = tc.timings()
-                b0 = torch.cuda.Event(enable_timing=True)
-                b1 = torch.cuda.Event(enable_timing=True)
-                b0.record(stream)
-                tc.step(dt, args.steps)
-                b1.record(stream)
-                torch.cuda.synchronize()
+                cms, _ = _timed_run(tc, stream, dt, ksteps, args.nsamp, rdf, dist)
                 ta = tc.timings()
-                cms = max_over_ranks(b0.elapsed_time(b1), dist) / args.steps
+                cms /= ksteps
                 acc_c = audit(tc, audit_idx)
-                compare[name] = {"theta": acfg.theta, "ms_per_step": cms,
-                                 "walk_ms": (ta.ms_walk - tb.ms_walk) / args.steps,
+                compare[name] = {"theta": th, "steps": ksteps, "ms_per_step": cms,
+                                 "walk_ms": (ta.ms_walk - tb.ms_walk) / ksteps,
                                  "particle_steps_per_s": n / (cms / 1e3),
                                  "rms_rel_err": acc_c and acc_c["rms_rel_err"],
                                  "max_rel_err": acc_c and acc_c["max_rel_err"],
-                                 "n_m2p_last": ta.n_m2p, "n_p2p_last": ta.n_p2p}
-        compare["headline_over_fp64_plain"] = (value / world /
-                                               compare["fp64_plain_theta0.5"]["particle_steps_per_s"])
+                                 "n_m2p_per_step": (ta.n_m2p_total - tb.n_m2p_total) / ksteps,
+                                 "n_p2p_per_step": (ta.n_p2p_total - tb.n_p2p_total) / ksteps}
+        ours_ms = ms / args.steps
+        compare["headline_over_fp64_plain_theta0.5"] = (
+            compare["fp64_plain_theta0.5"]["ms_per_step"] / ours_ms)
+        fp64_pts = [(v["theta"], v["rms_rel_err"], v["ms_per_step"])
+                    for k, v in compare.items()
+                    if k.startswith("fp64_plain_theta") and isinstance(v, dict)]
+        eq = equal_accuracy(fp64_pts, 1e-4)
+        if eq:
+            eq["headline_over_fp64_at_equal_accuracy"] = eq["ms_per_step"] / ours_ms
+            eq["note"] = ("plain FP64 fixed-theta path: rms error and time per step fitted as "
+                          "power laws of theta over the measured arms, evaluated where the "
+                          "rms reaches the headline's 1e-4 bar")
+        compare["fp64_plain_equal_accuracy"] = eq
+
+    # ---- ensemble of independent clouds (one handle, one launch per phase) ----
+    ens_rec = None
+    if not args.no_ensemble and prec == api.PREC_MIXED and mac == api.MAC_LEARNED:
+        ens_rec = ensemble_record(args, stream, dist, world)
 
     # ---- CPU baseline (rank 0, N = 1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
+        flags = oracle.use_native()
         st = tf.get_state()
         stride = args.cpu_stride or auto_stride(n)
         v, det = cpu_sample(st, args, stride)
         cpu = {"value": v, "unit": UNIT, "cores": oracle.max_threads(),
                "kind": "port",
-               "sample": f"oracle REF1 (reference algorithm, FP64, reference pair laws, "
-                         f"theta={args.ref_theta}) on the final state: full build + walk "
-                         f"of every {stride}th target, walk time x{stride}",
+               "sample": f"oracle (reference algorithm, FP64, theta={args.theta}, "
+                         f"{args.physics} pair laws{', RDF' if rdf else ''}) on the final "
+                         f"state: full build + walk of every {stride}th target, walk time "
+                         f"x{stride}; {flags}",
                "detail": det}
 
     tf.close()
@@ -458,65 +607,58 @@ def run_ours(args, rank, world, dist):
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if fp64 else "f32 (walk) + f64 (positions, Verlet, top cells)",
         "data": "synthetic (seeded Gaussian UCP cloud, electrons start on ions)",
-        "config": {"workload": f"UCP cloud N={n} per GPU, T_e={args.te} K, T_i=1 mK, "
-                               f"theta={args.theta}, dt=1e-11 s",
-                   "n_particles": n, "theta": args.theta, "te_k": args.te,
-                   "physics": args.physics, "precision": args.precision,
+        "config": workload_config(args, n),
+        "method": {"precision": args.precision,
                    "mac": "learned" if mac == api.MAC_LEARNED else "fixed",
                    "eta": args.eta if mac == api.MAC_LEARNED else None,
                    "order": args.order, "bucket": args.bucket,
-                   "l2": "inputs larger than L2 (x,v,f 72 MB + trees >150 MB, rebuilt every step)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "loop": "tree_gpu_run: CUDA-graph replay of the step body"},
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "clocks": clk, "e2e": e2e, "gpu_launches": launches,
         "phases_ms_per_step": {"build": build_ms, "walk": walk_ms,
                                "other": ms / args.steps - build_ms - walk_ms},
+        "rdf_pairs_counted": rdf_pairs,
         "roofline": roofline, "roofline_build": build_roof,
         "accuracy": accuracy, "cpu_baseline": cpu, "compare": compare,
-        "diag": {"epot_e": diag.epot_e, "epot_i": diag.epot_i,
-                 "mv2_el": diag.mv2_el, "mv2_ion": diag.mv2_ion},
+        "ensemble": ens_rec,
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------- ensemble ----
-def run_ensemble(args, rank, world, dist):
+def ensemble_record(args, stream, dist, world, tune_it=False, compare_separate=False):
     """Independent clouds of uneven N (log-uniform in [8192, 131072]), peak
     densities log-uniform in [1e14, 1e16] m^-3, T_e uniform in [10, 200] K, in
     one handle: one build, one persistent walk launch and one integrator launch
-    per step, replayed as CUDA graphs.  Compared with the same clouds stepped
-    one handle after another from the same state."""
+    per step, replayed as CUDA graphs.  Optionally compared with the same clouds
+    stepped one handle after another from the same state."""
     import torch
 
     from tree_b200 import api, cloud, learned_mac, tune, units
-    dev = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(dev)
-    dt = units.dt_code(1e-11)
+    dt = units.dt_code(DT_S)
+    rank = int(os.environ.get("RANK", "0"))
     clouds, te, n0 = cloud.make_ensemble(args.clouds, seed=args.seed + rank)
     x, v, n_el, n_ion = cloud.pack_ensemble(clouds)
     n = len(x)
     phys = api.PHYS_KELBG if args.physics == "kelbg" else api.PHYS_REF
-    mac = api.MAC_LEARNED if args.mac == "learned" else api.MAC_FIXED
-    cfgs = [api.Config(theta=args.theta, te=float(t), physics=phys,
+    setting = dict(ENSEMBLE_TUNED)
+    mac = api.MAC_LEARNED if setting["eta"] > 0 else api.MAC_FIXED
+    cfgs = [api.Config(theta=setting["theta"], te=float(t), physics=phys,
                        precision=api.PREC_MIXED, mac=mac) for t in te]
-    params, stats, _ = learned_mac.load_model()
-    stream = torch.cuda.Stream()
+    params, stats, _ = learned_mac.load_model(order=setting["order"])
     ens = api.Ensemble(cfgs, n_el, n_ion)
     ens.set_stream(stream.cuda_stream)
-    ens.set_tuning(args.bucket, 4, args.order)
+    ens.set_tuning(setting["bucket"], setting["blocks_per_sm"], setting["order"])
     ens.mac_set_model(params, stats)
-    ens.mac_config(args.eta, 0.05, 0.9)
+    ens.mac_config(setting["eta"], 0.05, 0.9)
     ens.set_state(x, v)
-    ens.step(dt, max(args.warmup, 3))
+    # past the error transient of the first steps (electrons leaving their ions)
+    ens.step(dt, max(args.warmup, 3) + 10)
     torch.cuda.synchronize()
     tuned = None
-    if args.tune:
-        # the force error grows while the electrons leave their ions (about
-        # ten steps of 1e-11 s): tune on a state past that transient
-        ens.step(dt, 10)
+    if tune_it:
         space = [tune.Candidate(t, e, 8, 3, g) for t in (0.20, 0.22, 0.24, 0.26, 0.28, 0.30)
                  for e in (0.0, 3e-6, 1e-5, 3e-5) for g in (3, 4)]
-        # 1024 audited targets per cloud; margin 0.8 leaves room for the state
-        # to drift during the timed steps
         best, trials = tune.autotune(ens, dt, space=space, target=1e-4, margin=0.8,
                                      audit=1024 * args.clouds, physics=phys,
                                      model=(params, stats))
@@ -524,11 +666,12 @@ def run_ensemble(args, rank, world, dist):
             tuned = {**{k: getattr(best.cand, k) for k in ("theta", "eta", "bucket",
                                                            "order", "blocks_per_sm")},
                      "ms": best.ms, "rms": best.rms, "trials": len(trials)}
+            setting = {k: tuned[k] for k in ENSEMBLE_TUNED}
     warm = ens.get_state()
     if dist:
         dist.barrier()
     t_before = ens.timings()
-    clocks = ClockSampler(dev)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", 0)))
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -543,10 +686,10 @@ def run_ensemble(args, rank, world, dist):
     # per-cloud accuracy against each cloud's own FP64 direct sum
     f = ens.get_state()["f"]
     rms = []
-    for c in range(args.clouds):
-        a, b = int(ens.offsets[c]), int(ens.offsets[c + 1])
-        t = np.sort(np.random.default_rng(c).choice(b - a, min(4096, b - a), replace=False))
-        fd, _ = ens.direct(c, t)
+    for cc in range(args.clouds):
+        a, b = int(ens.offsets[cc]), int(ens.offsets[cc + 1])
+        t = np.sort(np.random.default_rng(cc).choice(b - a, min(4096, b - a), replace=False))
+        fd, _ = ens.direct(cc, t)
         err = np.linalg.norm(f[a:b][t] - fd, axis=1) / np.linalg.norm(fd, axis=1)
         rms.append(float(np.sqrt(np.mean(err ** 2))))
     # end to end: cloud-major state host -> device, one step, state back
@@ -562,24 +705,21 @@ def run_ensemble(args, rank, world, dist):
     a1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(a0.elapsed_time(a1), dist) / k2
-    # the same clouds, one handle after another, from the same warm state
     sep_ms = None
-    if not args.no_compare:
-        tb = ens.timings()
+    if compare_separate:
         sep_ms = 0.0
-        for c in range(args.clouds):
-            a, b = int(ens.offsets[c]), int(ens.offsets[c + 1])
-            ne = int(n_el[c])
+        for cc in range(args.clouds):
+            a, b = int(ens.offsets[cc]), int(ens.offsets[cc + 1])
+            ne = int(n_el[cc])
             sl = {k: warm[k][a:b] for k in ("x", "v", "f")}
-            cfg = api.Config(theta=ens.config.theta, te=float(te[c]), physics=phys,
-                             precision=api.PREC_MIXED, mac=ens.config.mac)
+            cfg = api.Config(theta=setting["theta"], te=float(te[cc]), physics=phys,
+                             precision=api.PREC_MIXED, mac=mac)
             with api.TreeForce(ne, b - a - ne, cfg) as tc:
                 tc.set_stream(stream.cuda_stream)
-                tc.set_tuning(args.bucket, 4, args.order)
-                eta_c = args.eta if tuned is None else tuned["eta"]
-                if eta_c > 0:
+                tc.set_tuning(setting["bucket"], setting["blocks_per_sm"], setting["order"])
+                if setting["eta"] > 0:
                     tc.mac_set_model(params, stats)
-                    tc.mac_config(eta_c, 0.05, 0.9)
+                    tc.mac_config(setting["eta"], 0.05, 0.9)
                 tc.load_state(sl["x"][:ne], sl["v"][:ne], sl["f"][:ne], sl["x"][ne:],
                               sl["v"][ne:], sl["f"][ne:])
                 tc.step(dt, 1)
@@ -593,35 +733,51 @@ def run_ensemble(args, rank, world, dist):
                 torch.cuda.synchronize()
                 sep_ms += max_over_ranks(s0.elapsed_time(s1), dist) / args.steps
     ens.close()
-    if rank != 0:
-        return
-    walk_ms = (t_after.ms_walk - t_before.ms_walk) / args.steps
-    build_ms = (t_after.ms_build - t_before.ms_build) / args.steps
-    line = {
+    return {
         "metric": f"particle-steps/s, ensemble of {args.clouds} independent clouds in one handle",
-        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 (walk) + f64 (positions, Verlet, top cells)",
-        "data": "synthetic (seeded Gaussian UCP clouds, electrons start on ions)",
-        "config": {"workload": f"{args.clouds} clouds, N log-uniform in [8192, 131072] "
-                               f"(total {n}), n0 log-uniform in [1e14, 1e16] m^-3, "
-                               f"T_e uniform in [10, 200] K, T_i = 1 mK, dt = 1e-11 s",
-                   "n_particles": n, "theta": ens.config.theta,
-                   "mac": "learned" if ens.config.mac == api.MAC_LEARNED else "fixed",
-                   "eta": args.eta if tuned is None else tuned["eta"], "tuned": tuned,
-                   "l2": "inputs larger than L2"},
+        "value": value, "unit": UNIT, "steps": args.steps, "ms_per_step": ms / args.steps,
+        "workload": f"{args.clouds} clouds, N log-uniform in [8192, 131072] (total {n}), n0 "
+                    f"log-uniform in [1e14, 1e16] m^-3, T_e uniform in [10, 200] K, T_i = 1 mK, "
+                    f"dt = 1e-11 s; timed after {max(args.warmup, 3) + 10} steps; step loop "
+                    f"without RDF (tree_gpu_run keeps RDF per single cloud only)",
+        "n_particles": n, "setting": setting, "tuned_in_this_run": tuned,
         "clocks": clk, "gpu_launches": t_after.launches - t_before.launches,
-        "phases_ms_per_step": {"build": build_ms, "walk": walk_ms},
+        "phases_ms_per_step": {"build": (t_after.ms_build - t_before.ms_build) / args.steps,
+                               "walk": (t_after.ms_walk - t_before.ms_walk) / args.steps},
         "accuracy": {"targets_per_cloud": 4096, "rms_rel_err_max_cloud": max(rms),
                      "rms_rel_err_median_cloud": float(np.median(rms)),
-                     "per_cloud": [{"n": int(ens.offsets[c + 1] - ens.offsets[c]),
-                                    "te_k": round(float(te[c]), 2), "n0": float(n0[c]),
-                                    "rms": rms[c]} for c in range(args.clouds)]},
+                     "per_cloud": [{"n": int(ens.offsets[cc + 1] - ens.offsets[cc]),
+                                    "te_k": round(float(te[cc]), 2), "n0": float(n0[cc]),
+                                    "rms": rms[cc]} for cc in range(args.clouds)]},
         "e2e": {"value": whole_job_rate(n, world, 1, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n},
         "separate_handles_ms_per_step": sep_ms,
         "one_launch_speedup": (sep_ms / (ms / args.steps)) if sep_ms else None,
+    }
+
+
+def run_ensemble(args, rank, world, dist):
+    """The ensemble workload as the bench's own line."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    stream = torch.cuda.Stream()
+    rec = ensemble_record(args, stream, dist, world, tune_it=args.tune,
+                          compare_separate=not args.no_compare)
+    if rank != 0:
+        return
+    line = {
+        "metric": rec["metric"], "value": rec["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (walk) + f64 (positions, Verlet, top cells)",
+        "data": "synthetic (seeded Gaussian UCP clouds, electrons start on ions)",
+        "config": {"workload": rec["workload"], "n_particles": rec["n_particles"],
+                   "l2": "inputs larger than L2"},
+        "method": {"setting": rec["setting"], "tuned": rec["tuned_in_this_run"]},
+        "clocks": rec["clocks"], "gpu_launches": rec["gpu_launches"],
+        "phases_ms_per_step": rec["phases_ms_per_step"], "accuracy": rec["accuracy"],
+        "e2e": rec["e2e"], "separate_handles_ms_per_step": rec["separate_handles_ms_per_step"],
+        "one_launch_speedup": rec["one_launch_speedup"],
     }
     print(json.dumps(line), flush=True)
 
@@ -640,7 +796,9 @@ def main():
         backend = "nccl" if args.impl == "ours" else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        # rank 0 of the reference arm works for minutes while the others wait
+        tdist.init_process_group(backend, timeout=datetime.timedelta(
+            seconds=600 if backend == "nccl" else 1800))
         dist = tdist
     try:
         if args.impl == "reference":

@@ -93,6 +93,9 @@ typedef struct tree_gpu_timing {
   int64_t launches;  /* kernels this library launched (cumulative) */
   int64_t n_mac_net;       /* cells the learned MAC evaluated, last call */
   int64_t n_mac_fallback;  /* of those, outside the training range (fixed theta) */
+  int64_t n_m2p_total;     /* accepted cells summed over every walk of the handle */
+  int64_t n_p2p_total;     /* pair evaluations summed over every walk */
+  int64_t n_mac_net_total; /* learned-MAC evaluations summed over every walk */
 } tree_gpu_timing;
 
 typedef struct tree_gpu_handle tree_gpu_handle;

@@ -50,7 +50,8 @@ MODULE TREE_GPU_MOD
   TYPE, BIND(C) :: tree_gpu_timing
      REAL(C_DOUBLE) :: ms_build, ms_walk, ms_kdk, ms_total
      INTEGER(C_INT64_T) :: n_m2p, n_p2p, n_nodes, calls, launches, &
-          n_mac_net, n_mac_fallback
+          n_mac_net, n_mac_fallback, n_m2p_total, n_p2p_total, &
+          n_mac_net_total
   END TYPE tree_gpu_timing
 
   INTERFACE

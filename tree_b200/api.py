@@ -72,7 +72,8 @@ class Timing(ctypes.Structure):
                 ("n_m2p", ctypes.c_int64), ("n_p2p", ctypes.c_int64),
                 ("n_nodes", ctypes.c_int64), ("calls", ctypes.c_int64),
                 ("launches", ctypes.c_int64), ("n_mac_net", ctypes.c_int64),
-                ("n_mac_fallback", ctypes.c_int64)]
+                ("n_mac_fallback", ctypes.c_int64), ("n_m2p_total", ctypes.c_int64),
+                ("n_p2p_total", ctypes.c_int64), ("n_mac_net_total", ctypes.c_int64)]
 
 
 class TreeGpuError(RuntimeError):

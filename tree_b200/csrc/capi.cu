@@ -204,7 +204,10 @@ int alloc_all(tree_gpu_handle* h) {
   if ((rc = dalloc(h, &b.bounds, 5))) return rc;
   if ((rc = dalloc(h, &b.err, 1))) return rc;
   if ((rc = dalloc(h, &h->rdf, 2 * (size_t)tg::kRdfBins))) return rc;
-  if ((rc = dalloc(h, &h->counters, 4))) return rc;
+  if ((rc = dalloc(h, &h->counters, 8))) return rc;
+  // [0..3] this step's walk counts, [4..7] running totals of the handle
+  if (cudaMemset(h->counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess)
+    return fail(h, TREE_GPU_ERR_CUDA, "counter initialisation failed");
   if ((rc = dalloc(h, &h->partial, 4 * (size_t)tg::kdk_partials_needed(n) + 4)))
     return rc;
   if ((rc = dalloc(h, &h->diag, 8))) return rc;
@@ -310,7 +313,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
   if (ev) record(h, ev->e[2]);
   h->timing.launches += (h->n > 0 ? 1 : 0) + 2;  // walk + epot partial/sum
   // (the mixed walk is one kernel as well)
-  tg::epot_sum(h->epot_part, h->n, h->partial, h->diag, st);
+  tg::epot_sum(h->epot_part, h->n, h->partial, h->diag, h->counters, st);
 }
 
 // Reads the error word and node counts after a synchronised call.
@@ -346,12 +349,15 @@ int grow_nodes(tree_gpu_handle* h) {
 }
 
 void read_counters(tree_gpu_handle* h) {
-  unsigned long long c[4] = {0, 0, 0, 0};
+  unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   cudaMemcpy(c, h->counters, sizeof(c), cudaMemcpyDeviceToHost);
   h->timing.n_m2p = (int64_t)c[0];
   h->timing.n_p2p = (int64_t)c[1];
   h->timing.n_mac_net = (int64_t)c[2];
   h->timing.n_mac_fallback = (int64_t)c[3];
+  h->timing.n_m2p_total = (int64_t)c[4];
+  h->timing.n_p2p_total = (int64_t)c[5];
+  h->timing.n_mac_net_total = (int64_t)c[6];
 }
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {

@@ -103,9 +103,11 @@ __global__ void __launch_bounds__(kKdkThreads)
   if (SAMPLE) block_sum4(acc, partial);
 }
 
-// Sums rows of `partial` (nb x 4) in fixed order into out[0..3].
+// Sums rows of `partial` (nb x 4) in fixed order into out[0..3].  With cnt
+// (the walk's interaction counters of this step in cnt[0..3]), also adds
+// them to the running totals cnt[4..7].
 __global__ void k_sum_partials4(const double* __restrict__ partial, int nb,
-                                double* out) {
+                                double* out, unsigned long long* cnt = nullptr) {
   __shared__ double sh[kKdkThreads];
   for (int j = 0; j < 4; ++j) {
     double s = 0.0;
@@ -119,6 +121,7 @@ __global__ void k_sum_partials4(const double* __restrict__ partial, int nb,
     if (threadIdx.x == 0) out[j] = sh[0];
     __syncthreads();
   }
+  if (cnt && threadIdx.x < 4) cnt[4 + threadIdx.x] += cnt[threadIdx.x];
 }
 
 // Potential energy: epot_part[i] = (contribution to Epot_e, to Epot_i).
@@ -202,14 +205,14 @@ void cloud_sums(const double* x, const double* v, const double2* ep,
 }
 
 void epot_sum(const double2* ep, int n, double* partial, double* out4,
-              cudaStream_t st) {
+              unsigned long long* counters, cudaStream_t st) {
   if (n == 0) {
     cudaMemsetAsync(out4, 0, 4 * sizeof(double), st);
     return;
   }
   int g = (n + kKdkThreads - 1) / kKdkThreads;
   k_epot_partial<<<g, kKdkThreads, 0, st>>>(ep, n, partial);
-  k_sum_partials4<<<1, kKdkThreads, 0, st>>>(partial, g, out4);
+  k_sum_partials4<<<1, kKdkThreads, 0, st>>>(partial, g, out4, counters);
 }
 
 __global__ void k_sample_append(const double* __restrict__ diag, double* series,

@@ -20,9 +20,10 @@ void kick2(double* x, double* v, const double* f, int n, int n_el,
 void cloud_sums(const double* x, const double* v, const double2* ep,
                 const int32_t* start, const int32_t* elec_end, int nseg,
                 double xm_e, double xm_i, double* out, cudaStream_t st);
-// out4 = (Epot_e, Epot_i, 0, 0)
+// out4 = (Epot_e, Epot_i, 0, 0); counters[4..7] += counters[0..3] (the
+// walk's per-step interaction counts into running totals) when not NULL.
 void epot_sum(const double2* ep, int n, double* partial, double* out4,
-              cudaStream_t st);
+              unsigned long long* counters, cudaStream_t st);
 // Appends (Epot_e, Epot_i, mv2_el, mv2_ion, rad_el, rad_ion) from diag[8]
 // to series[*count] while *count < cap (one record per sample step).
 void sample_append(const double* diag, double* series, int32_t* count, int cap,

@@ -56,9 +56,9 @@ struct WarpSmem {
   // (Tyyz, Txzz, Tyzz, Txyz) -- S and T trace-free
   float4 cell[32 * kCellF4];
   // staged sources in pairs, kPartF4 float4 per pair: sources 2b and 2b+1
-  // side by side, (nhx nhx' nhy nhy') (nhz nhz' idx idx') (nlx nlx' nly nly')
-  // (nlz nlz' q q'): negated hi / lo offsets from the group centre, sorted
-  // index bits, charge
+  // side by side, (nhx nhx' nhy nhy') (nhz nhz' q q') (nlx nlx' nly nly')
+  // (nlz nlz' idx idx'): negated hi / lo offsets from the group centre,
+  // charge, sorted index bits
   float4 part[16 * kPartF4];
   // pair constants of the group's cloud: 1/lambda^2 (ee, ei, ii), 1/rs,
   // 1/lambda (ee, ei, ii)
@@ -86,6 +86,7 @@ struct MixedArgs {
   float inv_lam_ee, inv_lam_ei, inv_lam_ii;
   float rs_inv;
   double dx_ei_inv, dx_ii_inv;
+  float dx_ei_inv_f, dx_ii_inv_f;
   double* f;
   double2* epot_part;
   uint32_t* rdf;
@@ -247,26 +248,64 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
 }
 
 // ---------------------------------------------------------------- P2P ----
-// RDF count of one pair (bins in FP64 from the hi/lo offsets, so bin edges
-// match the FP64 path).  (ngx, ngy, ngz) / (nlx, nly, nlz): the source's
-// negated hi / lo offsets from the group centre.
+// Staged pair block (kPartF4 float4, sources 2b and 2b+1 side by side):
+//   q0 (nhx nhx' nhy nhy')  q1 (nhz nhz' q q')  q2 (nlx nlx' nly nly')
+//   q3 (nlz nlz' idx idx')
+// negated hi / lo FP32 parts of each source's FP64 offset from the group
+// centre, its charge (-1 electron, +1 ion; 0 for padding) and its sorted index.
+//
+// A pair's separation is formed from the hi parts alone.  Each hi part is
+// within 2^-24 of its offset, so the separation r is within 2^-24 (2h + r)
+// of the exact one (h the group's half-diagonal, which bounds the target's
+// offset); for r^2 > h^2/32 that is below 7.3e-7 r.  Closer pairs -- a few in
+// a thousand, among them every pair of the Kelbg core, the target itself and
+// particles on one point -- are redone with hi + lo, whose FP32 roundings are
+// relative to their own results, and only they need the source index.
+
+// FP64 bin of a pair near a bin edge, from the staged hi / lo parts (rare;
+// kept out of line so its registers do not weigh on the pair loop); -1
+// beyond the last bin.
+__device__ __noinline__ int rdf_bin64(const float4* __restrict__ blk, int half,
+                                      float thx, float thy, float thz, float tlx,
+                                      float tly, float tlz, double inv) {
+  const float4 q0 = blk[0], q1 = blk[1], q2 = blk[2], q3 = blk[3];
+  const float ngx = half ? q0.y : q0.x, ngy = half ? q0.w : q0.z, ngz = half ? q1.y : q1.x;
+  const float nlx = half ? q2.y : q2.x, nly = half ? q2.w : q2.z, nlz = half ? q3.y : q3.x;
+  const double ex = ((double)thx + (double)ngx) + ((double)tlx + (double)nlx);
+  const double ey = ((double)thy + (double)ngy) + ((double)tly + (double)nly);
+  const double ez = ((double)thz + (double)ngz) + ((double)tlz + (double)nlz);
+  const double t = sqrt(ex * ex + ey * ey + ez * ez) * inv;
+  return t < (double)kRdfBins ? (int)t : -1;
+}
+
+// RDF count of one pair (e-i for every target, i-i for ion targets, as
+// Search_Tree_ie/ei/ii bin them).  The bin comes from the FP32 distance,
+// within 1e-6 relative of the FP64 one (see above; 3e-7 for pairs formed with
+// hi + lo); only when that estimate lies within 2e-6 t of a bin edge (or of
+// the last bin's edge) is the distance recomputed in FP64 from the staged
+// offsets, so the bins are those of the FP64 evaluation.  s: the source
+// index, or -1 when the pair was not close (it is then not the target).
 template <int PHYS>
 __device__ __forceinline__ void rdf_count(const MixedArgs& a, float r2, float ssign, int s,
-                                          float ngx, float ngy, float ngz, float nlx,
-                                          float nly, float nlz, float thx, float thy,
-                                          float thz, float tlx, float tly, float tlz,
-                                          int p_self, int tsp) {
+                                          const float4* __restrict__ blk, int half,
+                                          float thx, float thy, float thz, float tlx,
+                                          float tly, float tlz, int p_self, int tsp) {
   const bool same = ssign == (tsp ? 1.f : -1.f);
   const bool counted = PHYS == 1 ? s != p_self : (same ? r2 > 0.01f : true);
   if (ssign != 0.f && counted && (!same || tsp == 1)) {
-    const double ex = ((double)thx + (double)ngx) + ((double)tlx + (double)nlx);
-    const double ey = ((double)thy + (double)ngy) + ((double)tly + (double)nly);
-    const double ez = ((double)thz + (double)ngz) + ((double)tlz + (double)nlz);
-    const double t = sqrt(ex * ex + ey * ey + ez * ez) * (same ? a.dx_ii_inv : a.dx_ei_inv);
-    if (t < (double)kRdfBins) {
-      int id = (int)t;
-      if (id >= 0 && id < kRdfBins) atomicAdd(&a.rdf[(same ? kRdfBins : 0) + id], 1u);
+    const float t32 = sqrtf(r2) * (same ? a.dx_ii_inv_f : a.dx_ei_inv_f);
+    const float tol = fmaf(t32, 2e-6f, 1e-30f);
+    if (t32 - tol >= (float)kRdfBins) return;  // beyond the last bin either way
+    const float fl = floorf(t32);
+    int id;
+    if (t32 - fl > tol && fl + 1.f - t32 > tol && t32 + tol < (float)kRdfBins) {
+      id = (int)fl;
+    } else {
+      id = rdf_bin64(blk, half, thx, thy, thz, tlx, tly, tlz,
+                     same ? a.dx_ii_inv : a.dx_ei_inv);
+      if (id < 0) return;
     }
+    if (id >= 0 && id < kRdfBins) atomicAdd(&a.rdf[(same ? kRdfBins : 0) + id], 1u);
   }
 }
 
@@ -336,14 +375,15 @@ __device__ __forceinline__ void p2p_one(const WarpSmem& sm, float r2, float dx, 
 
 // Pair interactions of up to 32 staged sources with this lane's target, two
 // sources per packed FP32 (f32x2) instruction.  The common pair is plain
-// Coulomb; a pair with a special member goes through p2p_one.
+// Coulomb from the hi parts; a close pair (r^2 <= close2) is redone with the
+// exact offsets, and a pair with a special member goes through p2p_one.
 template <int PHYS, bool RDF>
 __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
                                          const MixedArgs& a, double Gx,
                                          double Gy, double Gz, float thx,
                                          float thy, float thz, float tlx,
-                                         float tly, float tlz, int p_self,
-                                         int tsp, bool act, int lane,
+                                         float tly, float tlz, float close2,
+                                         int p_self, int tsp, bool act, int lane,
                                          Acc& acc) {
   {
     // this lane's source (or, past cnt, a chargeless dummy 10^6 um away)
@@ -353,13 +393,14 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
       const double4 xs = a.xs[s];
       const double rx = Gx - xs.x, ry = Gy - xs.y, rz = Gz - xs.z;
       const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
-      v[0] = hx; v[1] = hy; v[2] = hz; v[3] = __int_as_float(s);
+      v[0] = hx; v[1] = hy; v[2] = hz; v[3] = xs.w > 0.5 ? 1.f : -1.f;
       v[4] = (float)(rx - (double)hx); v[5] = (float)(ry - (double)hy);
-      v[6] = (float)(rz - (double)hz); v[7] = xs.w > 0.5 ? 1.f : -1.f;
+      v[6] = (float)(rz - (double)hz); v[7] = __int_as_float(s);
     } else {
       v[0] = v[1] = v[2] = 1.0e6f;
-      v[3] = __int_as_float(-1);
-      v[4] = v[5] = v[6] = v[7] = 0.f;
+      v[3] = 0.f;
+      v[4] = v[5] = v[6] = 0.f;
+      v[7] = __int_as_float(-1);
     }
     const bool odd = lane & 1;
     float2* pb = reinterpret_cast<float2*>(sm.part + kPartF4 * (lane >> 1)) + (odd ? 1 : 0);
@@ -379,20 +420,30 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
   const float il2_to_i = PHYS == 1 ? (tsp ? sm.pk[2] : sm.pk[1]) : 0.f;  // ion source
   const float rs2 = sm.pk[3] * sm.pk[3];
   const float2 thx2 = make_float2(thx, thx), thy2 = make_float2(thy, thy), thz2 = make_float2(thz, thz);
-  const float2 tlx2 = make_float2(tlx, tlx), tly2 = make_float2(tly, tly), tlz2 = make_float2(tlz, tlz);
   float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx, pa = fx, pq = fx;
   const int npair = (cnt + 1) >> 1;
   for (int b = 0; b < npair; ++b) {
     const float4* blk = sm.part + kPartF4 * b;
-    const float4 q0 = blk[0], q1 = blk[1], q2 = blk[2], q3 = blk[3];
-    const float2 q = make_float2(q3.z, q3.w);  // source charges: -1 e, +1 ion
-    const float2 dx = __fadd2_rn(__fadd2_rn(thx2, make_float2(q0.x, q0.y)),
-                                 __fadd2_rn(tlx2, make_float2(q2.x, q2.y)));
-    const float2 dy = __fadd2_rn(__fadd2_rn(thy2, make_float2(q0.z, q0.w)),
-                                 __fadd2_rn(tly2, make_float2(q2.z, q2.w)));
-    const float2 dz = __fadd2_rn(__fadd2_rn(thz2, make_float2(q1.x, q1.y)),
-                                 __fadd2_rn(tlz2, make_float2(q3.x, q3.y)));
-    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    const float4 q0 = blk[0], q1 = blk[1];
+    const float2 q = make_float2(q1.z, q1.w);  // source charges: -1 e, +1 ion
+    float2 dx = __fadd2_rn(thx2, make_float2(q0.x, q0.y));
+    float2 dy = __fadd2_rn(thy2, make_float2(q0.z, q0.w));
+    float2 dz = __fadd2_rn(thz2, make_float2(q1.x, q1.y));
+    float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    int s0 = -1, s1 = -1;
+    if (r2.x <= close2 || r2.y <= close2) {
+      // close pair: the exact offsets (hi + lo) and the source indices
+      const float4 q2 = blk[2], q3 = blk[3];
+      dx = __fadd2_rn(__fadd2_rn(thx2, make_float2(q0.x, q0.y)),
+                      __fadd2_rn(make_float2(tlx, tlx), make_float2(q2.x, q2.y)));
+      dy = __fadd2_rn(__fadd2_rn(thy2, make_float2(q0.z, q0.w)),
+                      __fadd2_rn(make_float2(tly, tly), make_float2(q2.z, q2.w)));
+      dz = __fadd2_rn(__fadd2_rn(thz2, make_float2(q1.x, q1.y)),
+                      __fadd2_rn(make_float2(tlz, tlz), make_float2(q3.x, q3.y)));
+      r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+      s0 = __float_as_int(q3.z);
+      s1 = __float_as_int(q3.w);
+    }
     bool sp0, sp1;
     if (PHYS == 1) {
       sp0 = r2.x * (q.x < 0.f ? il2_to_e : il2_to_i) < 40.f;
@@ -411,16 +462,14 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
       pa = __fadd2_rn(pa, ph);
       pq = __ffma2_rn(q, ph, pq);
     } else {
-      p2p_one<PHYS>(sm, r2.x, dx.x, dy.x, dz.x, q.x, __float_as_int(q1.z), p_self, tsp,
+      p2p_one<PHYS>(sm, r2.x, dx.x, dy.x, dz.x, q.x, s0, p_self, tsp,
                     fx.x, fy.x, fz.x, pa.x, pq.x);
-      p2p_one<PHYS>(sm, r2.y, dx.y, dy.y, dz.y, q.y, __float_as_int(q1.w), p_self, tsp,
+      p2p_one<PHYS>(sm, r2.y, dx.y, dy.y, dz.y, q.y, s1, p_self, tsp,
                     fx.y, fy.y, fz.y, pa.y, pq.y);
     }
     if (RDF && act) {
-      rdf_count<PHYS>(a, r2.x, q.x, __float_as_int(q1.z), q0.x, q0.z, q1.x, q2.x, q2.z,
-                      q3.x, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
-      rdf_count<PHYS>(a, r2.y, q.y, __float_as_int(q1.w), q0.y, q0.w, q1.y, q2.y, q2.w,
-                      q3.y, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
+      rdf_count<PHYS>(a, r2.x, q.x, s0, blk, 0, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
+      rdf_count<PHYS>(a, r2.y, q.y, s1, blk, 1, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
     }
   }
   __syncwarp();
@@ -495,6 +544,9 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
     const float thx = (float)rtx, thy = (float)rty, thz = (float)rtz;
     const float tlx = (float)(rtx - (double)thx), tly = (float)(rty - (double)thy),
                 tlz = (float)(rtz - (double)thz);
+    // pairs closer than h / sqrt(32) (h the group's half-diagonal) take the
+    // exact offsets (eval_p2p)
+    const float close2 = (float)((hx * hx + hy * hy + hz * hz) * (1.0 / 32.0));
     Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
     // error budget of the learned MAC: eta * min |F_prev| / eps over the group
     float budget = 0.f, hlen = 0.f;
@@ -701,7 +753,7 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
       __syncwarp();
       while (p2t - p2h >= 32) {
         eval_p2p<PHYS, RDF>(sm, p2h, 32, a, Gx, Gy, Gz, thx, thy, thz, tlx, tly,
-                            tlz, pt, tsp, act, lane, acc);
+                            tlz, close2, pt, tsp, act, lane, acc);
         p2h += 32;
         n_p2p += 32;
       }
@@ -717,7 +769,7 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
     }
     if (p2t > p2h) {
       eval_p2p<PHYS, RDF>(sm, p2h, p2t - p2h, a, Gx, Gy, Gz, thx, thy, thz, tlx,
-                          tly, tlz, pt, tsp, act, lane, acc);
+                          tly, tlz, close2, pt, tsp, act, lane, acc);
       n_p2p += p2t - p2h;
     }
     if (m2t > m2h) {
@@ -859,6 +911,8 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.rs_inv = (float)(1.0 / wp.rs);
   a.dx_ei_inv = 1.0 / wp.dx_ei;
   a.dx_ii_inv = 1.0 / wp.dx_ii;
+  a.dx_ei_inv_f = (float)a.dx_ei_inv;
+  a.dx_ii_inv_f = (float)a.dx_ii_inv;
   a.f = f;
   a.epot_part = epot_part;
   a.rdf = rdf;

@@ -1,6 +1,6 @@
 """Trains the learned multipole acceptance criterion on the GPU.
 
-    python -m tree_b200.learned_mac [--n 262144] [--out tree_b200/data/mac_model.npz]
+    python -m tree_b200.learned_mac [--n 262144] [--order 3] [--out tree_b200/data/mac_model.npz]
 
 Training data is generated by the method itself: seeded clouds of N = 262,144
 particles at electron temperatures across [10, 200] K are evolved a few steps
@@ -26,13 +26,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(HERE, "data", "mac_model.npz")
 
 
+def model_path(order=3):
+    """The shipped model for a far-field order (its labels are the errors of
+    that order's expansion)."""
+    return DEFAULT_MODEL if order == 3 else os.path.join(HERE, "data", f"mac_model_o{order}.npz")
+
+
 def collect_and_train(n=262144, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
                       steps_list=(2, 6, 20), theta=(0.2, 0.9), rho=(0.2, 0.9),
                       max_count=16384, keep=0.1, cap=12_000_000, epochs=10,
-                      batch=8192, lr=2e-3, tau=0.99, seed=11, verbose=True):
+                      batch=8192, lr=2e-3, tau=0.99, seed=11, order=3, verbose=True):
     dt = units.dt_code(1e-11)
     half = n // 2
-    report = {"n": n, "te_list": list(te_list), "steps_list": list(steps_list),
+    report = {"n": n, "order": order, "te_list": list(te_list), "steps_list": list(steps_list),
               "theta": list(theta), "rho": list(rho), "max_count": max_count,
               "keep": keep,
               "tau": tau, "epochs": epochs, "batch": batch, "lr": lr, "collects": []}
@@ -40,6 +46,7 @@ def collect_and_train(n=262144, te_list=(10.0, 25.0, 50.0, 100.0, 200.0),
     cfg = api.Config(theta=0.5, te=te_list[0], physics=api.PHYS_KELBG,
                      precision=api.PREC_MIXED, mac=api.MAC_FIXED)
     with api.TreeForce(half, half, cfg) as tf:
+        tf.set_tuning(8, 4, order)  # labels at the walk's expansion order
         k = 0
         for te in te_list:
             tf.set_config(api.Config(theta=0.5, te=te, physics=api.PHYS_KELBG,
@@ -90,7 +97,11 @@ def write_bin(path, params, stats):
     np.concatenate([np.asarray(params, "<f4"), np.asarray(stats, "<f4")]).tofile(path)
 
 
-def load_model(path=DEFAULT_MODEL):
+def load_model(path=DEFAULT_MODEL, order=None):
+    """(params, stats, report) of a model file; with `order`, the shipped model
+    of that far-field order."""
+    if order is not None:
+        path = model_path(order)
     d = np.load(path)
     report = json.loads(bytes(d["report"]).decode()) if "report" in d else {}
     return d["params"], d["stats"], report
@@ -102,15 +113,19 @@ def main():
     ap.add_argument("--epochs", type=int, default=10)
     ap.add_argument("--keep", type=float, default=0.1,
                     help="sampling probability of a tested cell in the acceptance band")
-    ap.add_argument("--out", default=DEFAULT_MODEL)
+    ap.add_argument("--order", type=int, default=3, choices=(2, 3, 4),
+                    help="far-field expansion order the labels are computed at")
+    ap.add_argument("--out", default="")
     ap.add_argument("--dump-samples", default="")
     args = ap.parse_args()
-    params, stats, report, (f, y, e) = collect_and_train(n=args.n, epochs=args.epochs, keep=args.keep)
-    save_model(args.out, params, stats, report)
+    out = args.out or model_path(args.order)
+    params, stats, report, (f, y, e) = collect_and_train(n=args.n, epochs=args.epochs,
+                                                         keep=args.keep, order=args.order)
+    save_model(out, params, stats, report)
     if args.dump_samples:
         idx = np.random.default_rng(0).choice(len(y), min(len(y), 150_000), replace=False)
         np.savez_compressed(args.dump_samples, feats=f[idx], labels=y[idx], extra=e[idx])
-    print("saved", args.out)
+    print("saved", out)
 
 
 if __name__ == "__main__":
