@@ -1041,30 +1041,38 @@ __global__ void k_net_leaves(const double* __restrict__ x,
 
 // Net moments of twig `cur` from its children (all final): centroid, then
 // Q, D, S and T about it by the parallel-axis rules, in the children's
-// pre-order; writes the FP64 record and the trace-free FP32 copies.
+// pre-order (ascending octant digit, the order of the child table); writes the
+// FP64 record and the trace-free FP32 copies.  The child indices come from one
+// read of the child table, so the loads of all children are independent.
 __device__ bool net_twig(int cur, double smax0, double theta, int cap,
-                         double4* node_c, const int32_t* __restrict__ node_skip,
-                         const int8_t* __restrict__ node_level, MixedNodes mx,
-                         int32_t* err) {
+                         double4* node_c, const int8_t* __restrict__ node_level,
+                         MixedNodes mx, int32_t* err) {
   const double4 gc = ldcg_d4(&node_c[cur]);  // geometric centre (topology)
-  int end = node_skip[cur];
-  if (end > cap) end = cap;
+  int kid[8];
+  {
+    const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)cur);
+    const int4 k0 = __ldg(kk), k1 = __ldg(kk + 1);
+    kid[0] = k0.x; kid[1] = k0.y; kid[2] = k0.z; kid[3] = k0.w;
+    kid[4] = k1.x; kid[5] = k1.y; kid[6] = k1.z; kid[7] = k1.w;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    if (kid[j] >= cap || (kid[j] >= 0 && kid[j] <= cur)) {
+      set_error(err, kErrWalk);
+      return false;
+    }
   // pass 1: count and centroid
   double nsum = 0.0, X0 = 0.0, X1 = 0.0, X2 = 0.0;
-  int c = cur + 1;
-  while (c < end) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int c = kid[j];
+    if (c < 0) continue;
     const double4 cc = ldcg_d4(&node_c[c]);
     const double nc = __ldcg(mx.m64 + kM64 * (int64_t)c).x;
     nsum += nc;
     X0 += nc * cc.x;
     X1 += nc * cc.y;
     X2 += nc * cc.z;
-    int nx = node_skip[c];
-    if (nx <= c) {
-      set_error(err, kErrWalk);
-      return false;
-    }
-    c = nx;
   }
   X0 /= nsum;
   X1 /= nsum;
@@ -1073,8 +1081,10 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
   double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
   double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
   double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  c = cur + 1;
-  while (c < end) {
+#pragma unroll 1
+  for (int j = 0; j < 8; ++j) {
+    const int c = kid[j];
+    if (c < 0) continue;
     const double4 cc = ldcg_d4(&node_c[c]);
     const double2* cm = mx.m64 + kM64 * (int64_t)c;
     const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
@@ -1096,10 +1106,10 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       }
 #pragma unroll
       for (int u = 0; u < 10; ++u) {
-        const int i = kTI[u][0], j = kTI[u][1], k = kTI[u][2];
-        T[u] += Tc[u] + d[i] * S2[j][k] + d[j] * S2[i][k] + d[k] * S2[i][j] +
-                d[i] * d[j] * Dc[k] + d[i] * Dc[j] * d[k] + Dc[i] * d[j] * d[k] +
-                qc * d[i] * d[j] * d[k];
+        const int i = kTI[u][0], jj = kTI[u][1], k = kTI[u][2];
+        T[u] += Tc[u] + d[i] * S2[jj][k] + d[jj] * S2[i][k] + d[k] * S2[i][jj] +
+                d[i] * d[jj] * Dc[k] + d[i] * Dc[jj] * d[k] + Dc[i] * d[jj] * d[k] +
+                qc * d[i] * d[jj] * d[k];
       }
     }
     Q += qc;
@@ -1113,7 +1123,6 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     Sxy += a4.y + 0.5 * (dcx * ey + ex * dcy) + 0.5 * qc * ex * ey;
     Syz += a5.x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez;
     Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
-    c = node_skip[c];
   }
   const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
   const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
@@ -1162,71 +1171,98 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
   return true;
 }
 
-// Level-synchronous pass over the twigs: counted and listed by level, then
-// one launch per level from the deepest up, one thread per twig.  Every
-// child is final when its parent's level runs (a launch boundary orders
-// them), so no arrival counters or fences are needed and the critical path
-// is one round of loads per level.
-// Counts per level go through a block-local histogram: ~43 global counters
-// hit by every twig would serialise on their atomics.
-__global__ void k_level_count(const int32_t* __restrict__ node_pt,
-                              const int8_t* __restrict__ node_level,
-                              const int32_t* __restrict__ bounds, int cap,
-                              int32_t* lvl) {
-  __shared__ int32_t h[kLevelSlots];
-  for (int l = threadIdx.x; l < kLevelSlots; l += blockDim.x) h[l] = 0;
-  __syncthreads();
+// Upward pass over the twigs in two launches.  Subtrees of at most
+// kSubtreeMax particles -- twigs that small whose parent holds more, or that
+// are roots -- are completed one per block, deepest level first with a block
+// barrier between levels (every child is final when its parent's level
+// runs).  The few twigs above them count the twig children they wait for; the
+// block that completes a subtree root decrements its parent's count, and the
+// last arrival completes the parent and climbs on (fence, atomic, fence: the
+// children's records are visible to the thread that completes the parent).
+// The arithmetic per twig is net_twig's, in the same child order, whichever
+// thread runs it.
+constexpr int kSubtreeMax = 512;
+constexpr int kNetThreads = 128;
+constexpr int kNetBlocksPerSm = 8;
+
+// Marks the pass: node_done[t] = twig children of each twig t above the
+// subtrees; list / *nlist: the subtree roots.
+__global__ void k_net_mark(const int32_t* __restrict__ bounds, int cap,
+                           const int32_t* __restrict__ node_pt,
+                           const int32_t* __restrict__ node_parent,
+                           int32_t* node_done, MixedNodes mx, int32_t* list,
+                           int32_t* nlist) {
   const int m = bounds[2] < cap ? bounds[2] : cap;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m && node_pt[i] < 0) atomicAdd(&h[node_level[i]], 1);
-  __syncthreads();
-  for (int l = threadIdx.x; l < kLevelSlots; l += blockDim.x)
-    if (h[l]) atomicAdd(&lvl[l], h[l]);
-}
-
-__global__ void k_level_offsets(int32_t* lvl) {
-  if (threadIdx.x != 0) return;
-  int run = 0;
-  for (int l = 0; l < kLevelSlots; ++l) {
-    lvl[kLevelSlots + l] = run;
-    lvl[2 * kLevelSlots + l] = 0;
-    run += lvl[l];
+  if (i >= m || node_pt[i] >= 0) return;  // twigs only
+  if (mx.count[i] > kSubtreeMax) {
+    const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)i);
+    const int4 k0 = kk[0], k1 = kk[1];
+    const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+    int tw = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) tw += (kv[j] >= 0 && kv[j] < cap && node_pt[kv[j]] < 0) ? 1 : 0;
+    node_done[i] = tw;
+  } else {
+    const int par = node_parent[i];
+    if (par < 0 || mx.count[par] > kSubtreeMax) list[atomicAdd(nlist, 1)] = i;
   }
 }
 
-// Places each twig in its level's list: a rank inside the block (shared
-// atomics), then one global reservation per level and block.
-__global__ void k_level_scatter(const int32_t* __restrict__ node_pt,
-                                const int8_t* __restrict__ node_level,
-                                const int32_t* __restrict__ bounds, int cap,
-                                int32_t* lvl, int32_t* list) {
-  __shared__ int32_t h[kLevelSlots], base[kLevelSlots];
-  for (int l = threadIdx.x; l < kLevelSlots; l += blockDim.x) h[l] = 0;
-  __syncthreads();
-  const int m = bounds[2] < cap ? bounds[2] : cap;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool twig = i < m && node_pt[i] < 0;
-  const int l = twig ? node_level[i] : 0;
-  const int rank = twig ? atomicAdd(&h[l], 1) : 0;
-  __syncthreads();
-  for (int k = threadIdx.x; k < kLevelSlots; k += blockDim.x)
-    base[k] = h[k] ? lvl[kLevelSlots + k] + atomicAdd(&lvl[2 * kLevelSlots + k], h[k]) : 0;
-  __syncthreads();
-  if (twig) list[base[l] + rank] = i;
-}
-
-__global__ void k_net_level(int level, const Geom* __restrict__ geom, double theta,
-                            int cap, double4* node_c,
-                            const int32_t* __restrict__ node_skip,
-                            const int8_t* __restrict__ node_level, MixedNodes mx,
-                            Ensemble ens, int32_t* err) {
-  if (*((volatile int32_t*)err) & kErrCapacity) return;
-  const int cnt = mx.lvl[level], base = mx.lvl[kLevelSlots + level];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
-    const int cur = mx.lvl_list[base + k];
-    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[cur]) : 0;
-    if (!net_twig(cur, geom[seg].smax0, theta, cap, node_c, node_skip, node_level, mx, err))
-      return;
+__global__ void __launch_bounds__(kNetThreads)
+    k_net_subtrees(const Geom* __restrict__ geom, double theta, int cap,
+                   double4* node_c, const int32_t* __restrict__ node_skip,
+                   const int32_t* __restrict__ node_pt,
+                   const int32_t* __restrict__ node_parent, int32_t* node_done,
+                   const int8_t* __restrict__ node_level, MixedNodes mx,
+                   Ensemble ens, const int32_t* __restrict__ list,
+                   const int32_t* __restrict__ nlist, int32_t* cursor, int32_t* err) {
+  __shared__ int s_k, s_lmax, s_stop;
+  const int total = *nlist;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_k = atomicAdd(cursor, 1);
+      s_lmax = 0;
+      s_stop = (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) != 0;
+    }
+    __syncthreads();
+    const int k = s_k;
+    if (k >= total || s_stop) return;
+    const int r = list[k];
+    int end = node_skip[r];
+    if (end > cap) end = cap;
+    const int lr = node_level[r];
+    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[r]) : 0;
+    const double smax0 = geom[seg].smax0;
+    int lm = lr;
+    for (int i = r + threadIdx.x; i < end; i += kNetThreads)
+      if (__ldg(&node_pt[i]) < 0) lm = max(lm, (int)__ldg(&node_level[i]));
+    atomicMax(&s_lmax, lm);
+    __syncthreads();
+    const int lmax = s_lmax;
+    bool ok = true;
+    for (int lev = lmax; lev >= lr; --lev) {
+      for (int i = r + threadIdx.x; i < end; i += kNetThreads)
+        if (__ldg(&node_pt[i]) < 0 && __ldg(&node_level[i]) == lev)
+          ok = ok && net_twig(i, smax0, theta, cap, node_c, node_level, mx, err);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && ok) {
+      __threadfence();
+      int par = node_parent[r];
+      for (int guard = 0; par >= 0; ++guard) {
+        if (guard > kMaxLevel + 2) {
+          set_error(err, kErrWalk);
+          break;
+        }
+        if (atomicSub(&node_done[par], 1) != 1) break;
+        __threadfence();
+        if (!net_twig(par, smax0, theta, cap, node_c, node_level, mx, err)) break;
+        __threadfence();
+        par = node_parent[par];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1395,21 +1431,24 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   }
   k_net_leaves<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.cap, b.node_c,
                                  b.mx, ens, b.err);
-  cudaMemsetAsync(b.mx.lvl, 0, sizeof(int32_t) * kLevelSlots, st);
-  k_level_count<<<gcap, T, 0, st>>>(b.node_pt, b.node_level, b.bounds, b.cap, b.mx.lvl);
-  k_level_offsets<<<1, 32, 0, st>>>(b.mx.lvl);
-  k_level_scatter<<<gcap, T, 0, st>>>(b.node_pt, b.node_level, b.bounds, b.cap,
-                                      b.mx.lvl, b.mx.lvl_list);
-  launches += 3;
+  // lvl[0]: subtree roots listed, lvl[1]: their cursor
+  cudaMemsetAsync(b.mx.lvl, 0, 2 * sizeof(int32_t), st);
+  k_net_mark<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_parent, b.node_done,
+                                 b.mx, b.mx.lvl_list, b.mx.lvl);
   {
-    int lgrid = (n + T - 1) / T;
-    if (lgrid > 4 * 148) lgrid = 4 * 148;
-    for (int level = kMaxLevel; level >= 0; --level) {
-      k_net_level<<<lgrid, T, 0, st>>>(level, b.geom, theta, b.cap, b.node_c,
-                                       b.node_skip, b.node_level, b.mx, ens, b.err);
-      ++launches;
-    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int sgrid = (n + kSubtreeMax - 1) / kSubtreeMax * 4;
+    if (sgrid > sms * kNetBlocksPerSm) sgrid = sms * kNetBlocksPerSm;
+    if (sgrid < 1) sgrid = 1;
+    k_net_subtrees<<<sgrid, kNetThreads, 0, st>>>(b.geom, theta, b.cap, b.node_c,
+                                                  b.node_skip, b.node_pt, b.node_parent,
+                                                  b.node_done, b.node_level, b.mx, ens,
+                                                  b.mx.lvl_list, b.mx.lvl, b.mx.lvl + 1,
+                                                  b.err);
   }
+  launches += 3;
   // the level lists of the upward pass are free again: a single cloud keeps
   // its group-level histogram there, an ensemble has one row per cloud
   const int nsg = ens.nseg > 0 ? ens.nseg : 1;

@@ -1,7 +1,7 @@
 // walk_mixed.cu -- warp-group Barnes-Hut walk in mixed precision.
 //
 // The mixed path walks ONE combined tree of both species (net-charge moments
-// about each cell's particle centroid, built level by level by k_net_level).
+// about each cell's particle centroid, built bottom-up by k_net_subtrees).
 // One warp owns a target group -- a contiguous sorted range of at most 32
 // particles of either species inside one cell, built by k_groups -- and
 // builds ONE interaction list for it:
