@@ -240,8 +240,10 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
 
 /* Tunables of the mixed-precision walk: twigs holding at most `bucket`
  * particles (1..8) are summed particle by particle instead of being opened;
- * `blocks_per_sm` (1..4) sets the persistent grid; `order` (2 or 3) is the
- * far-field expansion order (quadrupole, or octupole as well; default 3).
+ * `blocks_per_sm` (1..4) sets the persistent grid; `order` (2..4) is the
+ * far-field expansion order (quadrupole; octupole as well, the default 3; or
+ * hexadecapole as well, 4).  A learned acceptance model predicts the error of
+ * one order: load one trained at the order in use.
  * No counterpart in the reference; chosen by the autotuner (tree_b200/tune.py). */
 int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
                         int32_t blocks_per_sm, int32_t order);

@@ -157,3 +157,41 @@ def test_mixed_rdf_counts_pairs(device_lib):
     diff = np.abs(rei - 2 * want)
     # pair offsets are exact to ~1e-14 um (hi/lo split); bins are FP64
     assert diff.sum() <= 1e-5 * 2 * want.sum()
+
+
+def test_far_field_orders_converge(device_lib):
+    """A compact cluster far from a group of targets: the error of its
+    accepted cells falls with each expansion order (quadrupole, octupole,
+    hexadecapole) by about the cluster's size over its distance."""
+    rng = np.random.default_rng(31)
+    src_e = rng.uniform(-1.0, 1.0, (40, 3))
+    src_i = rng.uniform(-1.0, 1.0, (60, 3))
+    tgt = rng.uniform(-0.2, 0.2, (24, 3)) + np.array([9.0, 3.0, -4.0])
+    xe = np.vstack([src_e, tgt[:12]])
+    xi = np.vstack([src_i, tgt[12:]])
+    targets = np.concatenate([np.arange(40, 52), 52 + 60 + np.arange(12)])
+    errs = {}
+    for order in (2, 3, 4):
+        with api.TreeForce(len(xe), len(xi), _mixed(0.6)) as tf:
+            tf.set_tuning(1, 4, order)  # bucket 1: every accepted cell is a multipole
+            f_el, f_ion, _, _ = tf.force(xe, xi)
+            assert tf.timings().n_m2p > 0
+            fd, _ = tf.direct(targets)
+        f = np.vstack([f_el, f_ion])[targets]
+        errs[order] = float(np.sqrt(np.mean(_rel(f, fd) ** 2)))
+    assert errs[3] < 0.5 * errs[2] and errs[4] < 0.5 * errs[3], errs
+
+
+@pytest.mark.parametrize("theta", [0.5, 0.7])
+def test_hexadecapole_more_accurate_than_octupole(device_lib, theta):
+    xe, xi = _displaced(65536, 17, shift=1.0)
+    rng = np.random.default_rng(3)
+    t = np.sort(rng.choice(65536, 4096, replace=False))
+    rms = {}
+    for order in (3, 4):
+        with api.TreeForce(len(xe), len(xi), _mixed(theta)) as tf:
+            tf.set_tuning(8, 4, order)
+            f_el, f_ion, _, _ = tf.force(xe, xi)
+            fd, _ = tf.direct(t)
+        rms[order] = float(np.sqrt(np.mean(_rel(np.vstack([f_el, f_ion])[t], fd) ** 2)))
+    assert rms[4] < 0.7 * rms[3], rms

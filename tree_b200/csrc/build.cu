@@ -985,16 +985,23 @@ __constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
 //        + D_i d_j d_k + Q_c d_i d_j d_k      (S2 = 2 S of the child)
 // -- the octupole the quadrupole expansion leaves out, whose size sets the
 // error of accepting the cell.
-// m64 per node (11 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
+// Also the fourth moment H_ijkl = sum q a_i a_j a_k a_l, combined with
+//   H += H_c + 4 sym(d T_c) + 6 sym(d d S2_c) + 4 sym(d d d D_c) + Q_c d d d d
+// (sym: the distinct index placements), for the hexadecapole far field.
+// m64 per node (19 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
 // (Szz, Sxy) | (Syz, Szx) | T in the order xxx yyy zzz xxy xxz xyy yyz xzz
-// yzz xyz (all raw, for the FP64 labels of the learned criterion).  The FP32
+// yzz xyz | H in the order xxxx yyyy zzzz xxxy xxxz xyyy yyyz xzzz yzzz xxyy
+// xxzz yyzz xxyz xyyz xyzz, 0 (all raw, for the FP64 labels of the learned
+// criterion).  The FP32
 // copies the walk evaluates are trace-free, which drops every trace term from
 // the far-field formula (phi = Q/r + D.d/r^3 + 3 d.S'.d/r^5 + 5/2 T'(d,d,d)/r^7):
 // S' = S - tr(S)/3 I and T'_ijk = T_ijk - (d_ij V_k + d_ik V_j + d_jk V_i)/5
 // with V_k = T_iik.  mom per node (3 x float4): (Q, Dx, Dy, Dz),
 // (S'xx, S'yy, S'zz, Sxy), (Syz, Szx, trace S, q_ion); mom3 per node
 // (3 x float4): (T'xxx, T'yyy, T'zzz, T'xxy), (T'xxz, T'xyy, T'yyz, T'xzz),
-// (T'yzz, Txyz, |T'|_F, 0); geom (s, dx, n, |S'|_F).
+// (T'yzz, Txyz, |T'|_F, 0); mom4 per node (3 x float4): trace-free H'
+// (xxxx, xxxy, xxxz, xxyy), (xxyz, xyyy, xyyz, yyyy), (yyyz, xxzz, xyzz,
+// yyzz); geom (s, dx, n, |S'|_F).
 // Leaves of the combined tree (one per sorted particle) and the sorted
 // positions the walk reads.
 __global__ void k_net_leaves(const double* __restrict__ x,
@@ -1030,6 +1037,10 @@ __global__ void k_net_leaves(const double* __restrict__ x,
     f3[0] = make_float4(0.f, 0.f, 0.f, 0.f);
     f3[1] = make_float4(0.f, 0.f, 0.f, 0.f);
     f3[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4* f4 = mx.mom4 + 3 * (int64_t)leaf;
+    f4[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f4[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    f4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
     float4* f = mx.mom + 3 * (int64_t)leaf;
     f[0] = make_float4((float)q, 0.f, 0.f, 0.f);
     f[1] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1081,6 +1092,7 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
   double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
   double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
   double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 1
   for (int j = 0; j < 8; ++j) {
     const int c = kid[j];
@@ -1111,6 +1123,34 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
                 d[i] * d[jj] * Dc[k] + d[i] * Dc[jj] * d[k] + Dc[i] * d[jj] * d[k] +
                 qc * d[i] * d[jj] * d[k];
       }
+      // fourth moment, parallel axis: H += H_c + 4 sym(d T_c) + 6 sym(d d S2_c)
+      // + 4 sym(d d d D_c) + Q_c d d d d over the 15 components
+      const double Txxx = Tc[0], Tyyy = Tc[1], Tzzz = Tc[2], Txxy = Tc[3], Txxz = Tc[4],
+                   Txyy = Tc[5], Tyyz = Tc[6], Txzz = Tc[7], Tyzz = Tc[8], Txyz = Tc[9];
+      const double S2xx = S2[0][0], S2yy = S2[1][1], S2zz = S2[2][2], S2xy = S2[0][1],
+                   S2yz = S2[1][2], S2xz = S2[0][2];
+      double Hc[16];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const double2 h2 = __ldcg(cm + 11 + u);
+        Hc[2 * u] = h2.x;
+        Hc[2 * u + 1] = h2.y;
+      }
+      H[0] += Hc[0] + 4.0 * ex * Txxx + 6.0 * ex * ex * S2xx + 4.0 * ex * ex * ex * dcx + qc * ex * ex * ex * ex;
+      H[1] += Hc[1] + 4.0 * ey * Tyyy + 6.0 * ey * ey * S2yy + 4.0 * ey * ey * ey * dcy + qc * ey * ey * ey * ey;
+      H[2] += Hc[2] + 4.0 * ez * Tzzz + 6.0 * ez * ez * S2zz + 4.0 * ez * ez * ez * dcz + qc * ez * ez * ez * ez;
+      H[3] += Hc[3] + 3.0 * ex * Txxy + ey * Txxx + 3.0 * ex * ex * S2xy + 3.0 * ex * ey * S2xx + 3.0 * ex * ex * ey * dcx + ex * ex * ex * dcy + qc * ex * ex * ex * ey;
+      H[4] += Hc[4] + 3.0 * ex * Txxz + ez * Txxx + 3.0 * ex * ex * S2xz + 3.0 * ex * ez * S2xx + 3.0 * ex * ex * ez * dcx + ex * ex * ex * dcz + qc * ex * ex * ex * ez;
+      H[5] += Hc[5] + ex * Tyyy + 3.0 * ey * Txyy + 3.0 * ex * ey * S2yy + 3.0 * ey * ey * S2xy + ey * ey * ey * dcx + 3.0 * ex * ey * ey * dcy + qc * ex * ey * ey * ey;
+      H[6] += Hc[6] + 3.0 * ey * Tyyz + ez * Tyyy + 3.0 * ey * ey * S2yz + 3.0 * ey * ez * S2yy + 3.0 * ey * ey * ez * dcy + ey * ey * ey * dcz + qc * ey * ey * ey * ez;
+      H[7] += Hc[7] + ex * Tzzz + 3.0 * ez * Txzz + 3.0 * ex * ez * S2zz + 3.0 * ez * ez * S2xz + ez * ez * ez * dcx + 3.0 * ex * ez * ez * dcz + qc * ex * ez * ez * ez;
+      H[8] += Hc[8] + ey * Tzzz + 3.0 * ez * Tyzz + 3.0 * ey * ez * S2zz + 3.0 * ez * ez * S2yz + ez * ez * ez * dcy + 3.0 * ey * ez * ez * dcz + qc * ey * ez * ez * ez;
+      H[9] += Hc[9] + 2.0 * ex * Txyy + 2.0 * ey * Txxy + ex * ex * S2yy + 4.0 * ex * ey * S2xy + ey * ey * S2xx + 2.0 * ex * ey * ey * dcx + 2.0 * ex * ex * ey * dcy + qc * ex * ex * ey * ey;
+      H[10] += Hc[10] + 2.0 * ex * Txzz + 2.0 * ez * Txxz + ex * ex * S2zz + 4.0 * ex * ez * S2xz + ez * ez * S2xx + 2.0 * ex * ez * ez * dcx + 2.0 * ex * ex * ez * dcz + qc * ex * ex * ez * ez;
+      H[11] += Hc[11] + 2.0 * ey * Tyzz + 2.0 * ez * Tyyz + ey * ey * S2zz + 4.0 * ey * ez * S2yz + ez * ez * S2yy + 2.0 * ey * ez * ez * dcy + 2.0 * ey * ey * ez * dcz + qc * ey * ey * ez * ez;
+      H[12] += Hc[12] + 2.0 * ex * Txyz + ey * Txxz + ez * Txxy + ex * ex * S2yz + 2.0 * ex * ey * S2xz + 2.0 * ex * ez * S2xy + ey * ez * S2xx + 2.0 * ex * ey * ez * dcx + ex * ex * ez * dcy + ex * ex * ey * dcz + qc * ex * ex * ey * ez;
+      H[13] += Hc[13] + ex * Tyyz + 2.0 * ey * Txyz + ez * Txyy + 2.0 * ex * ey * S2yz + ex * ez * S2yy + ey * ey * S2xz + 2.0 * ey * ez * S2xy + ey * ey * ez * dcx + 2.0 * ex * ey * ez * dcy + ex * ey * ey * dcz + qc * ex * ey * ey * ez;
+      H[14] += Hc[14] + ex * Tyzz + ey * Txzz + 2.0 * ez * Txyz + ex * ey * S2zz + 2.0 * ex * ez * S2yz + 2.0 * ey * ez * S2xz + ez * ez * S2xy + ey * ez * ez * dcx + ex * ez * ez * dcy + 2.0 * ex * ey * ez * dcz + qc * ex * ey * ez * ez;
     }
     Q += qc;
     qi += a2.y;
@@ -1139,6 +1179,32 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
   m[5] = make_double2(Syz, Szx);
 #pragma unroll
   for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+#pragma unroll
+  for (int u = 0; u < 7; ++u) m[11 + u] = make_double2(H[2 * u], H[2 * u + 1]);
+  m[18] = make_double2(H[14], 0.0);
+  {
+    // trace-free H' = H - sym(delta C)/7 + sym(delta delta) tr C/35, C_kl = H_mmkl;
+    // the walk's hexadecapole reads 12 components (H order: xxxx yyyy zzzz
+    // xxxy xxxz xyyy yyyz xzzz yzzz xxyy xxzz yyzz xxyz xyyz xyzz)
+    const double Cxx = H[0] + H[9] + H[10], Cyy = H[9] + H[1] + H[11],
+                 Czz = H[10] + H[11] + H[2], Cxy = H[3] + H[5] + H[14],
+                 Cxz = H[4] + H[13] + H[7], Cyz = H[12] + H[6] + H[8];
+    const double c = Cxx + Cyy + Czz;
+    const double a7 = 1.0 / 7.0, a35 = 1.0 / 35.0;
+    float4* f4 = mx.mom4 + 3 * (int64_t)cur;
+    f4[0] = make_float4((float)(H[0] - 6.0 * a7 * Cxx + 3.0 * a35 * c),  // xxxx
+                        (float)(H[3] - 3.0 * a7 * Cxy),                  // xxxy
+                        (float)(H[4] - 3.0 * a7 * Cxz),                  // xxxz
+                        (float)(H[9] - a7 * (Cxx + Cyy) + a35 * c));      // xxyy
+    f4[1] = make_float4((float)(H[12] - a7 * Cyz),                       // xxyz
+                        (float)(H[5] - 3.0 * a7 * Cxy),                  // xyyy
+                        (float)(H[13] - a7 * Cxz),                       // xyyz
+                        (float)(H[1] - 6.0 * a7 * Cyy + 3.0 * a35 * c));  // yyyy
+    f4[2] = make_float4((float)(H[6] - 3.0 * a7 * Cyz),                  // yyyz
+                        (float)(H[10] - a7 * (Cxx + Czz) + a35 * c),     // xxzz
+                        (float)(H[14] - a7 * Cxy),                       // xyzz
+                        (float)(H[11] - a7 * (Cyy + Czz) + a35 * c));     // yyzz
+  }
   // trace-free parts (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz)
   const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
   double Tt[10];

@@ -8,15 +8,16 @@ namespace tg {
 
 // Node data of the combined tree that the mixed-precision walk reads.
 constexpr int kGroupMax = 32;  // targets per warp group
-constexpr int kM64 = 11;       // double2 per node of net-charge moments
+constexpr int kM64 = 19;       // double2 per node of net-charge moments
 struct MixedNodes {
   int32_t* kids;     // 8 per node: child index per octant digit, -1 if none
   int32_t* first;    // first sorted particle of the node's range
   int32_t* count;    // particles in the node
   int8_t* digit;     // octant of the node inside its parent
-  double2* m64;      // 11 per node: (n, Q) (Dx, Dy) (Dz, q_ion) (Sxx, Syy) (Szz, Sxy) (Syz, Szx) T[10]
+  double2* m64;      // 19 per node: (n, Q) (Dx, Dy) (Dz, q_ion) (Sxx, Syy) (Szz, Sxy) (Syz, Szx) T[10] H[15] 0
   float4* mom;       // 3 per node: (Q, Dx, Dy, Dz) (Sxx, Syy, Szz, Sxy) (Syz, Szx, trS, q_ion)
   float4* mom3;      // 3 per node: third moment T (10) and |T|_F
+  float4* mom4;      // 3 per node: 12 components of the trace-free fourth moment H'
   float4* geom;      // per node: (box side s, |centroid - box centre|, n, 0)
   double4* xs;       // per sorted particle: position, w = 1 for ions
   int2* groups;      // target groups (first sorted particle, count)

@@ -957,9 +957,9 @@ int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
                         int32_t blocks_per_sm, int32_t order) {
   if (!h) return TREE_GPU_ERR_ARG;
   if (bucket < 1 || bucket > 8 || blocks_per_sm < 1 || blocks_per_sm > 4 ||
-      order < 2 || order > 3)
+      order < 2 || order > 4)
     return fail(h, TREE_GPU_ERR_ARG,
-                "bucket must be 1..8, blocks_per_sm 1..4, order 2..3");
+                "bucket must be 1..8, blocks_per_sm 1..4, order 2..4");
   h->tune.bucket = bucket;
   h->tune.blocks_per_sm = blocks_per_sm;
   h->tune.order = order;

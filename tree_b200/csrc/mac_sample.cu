@@ -6,8 +6,9 @@
 // it tests whose acceptance ratio rho = s / (d - dx) lies in the band
 // [rho_lo, rho_hi] becomes one sample: its 16 features (mac.cuh) and the
 // exact error of accepting it for the group -- the FP64 multipole field at
-// the walk's expansion order (net monopole + dipole + quadrupole, and the
-// octupole for order 3, about the centroid) minus the FP64 Coulomb sum over
+// the walk's expansion order (net monopole + dipole + quadrupole, the
+// octupole for order 3 and the hexadecapole for order 4, about the centroid)
+// minus the FP64 Coulomb sum over
 // the cell's particles, maximised over the group's targets.
 // Cells with more than max_count particles are not sampled; the walk treats
 // them with the fixed-theta test (they fall outside the training range).
@@ -144,6 +145,48 @@ __global__ void __launch_bounds__(32 * kSmpWarps)
           fx += g3 * ex - 7.5 * ri7 * Tx + 1.5 * ri5 * Vx;
           fy += g3 * ey - 7.5 * ri7 * Ty + 1.5 * ri5 * Vy;
           fz += g3 * ez - 7.5 * ri7 * Tz + 1.5 * ri5 * Vz;
+        }
+        if (a.order >= 4) {  // hexadecapole term, as in the walk (walk_mixed.cu)
+          double H[16];
+#pragma unroll
+          for (int u2 = 0; u2 < 8; ++u2) {
+            const double2 h2 = m[11 + u2];
+            H[2 * u2] = h2.x;
+            H[2 * u2 + 1] = h2.y;
+          }
+          // trace-free projection (order xxxx yyyy zzzz xxxy xxxz xyyy yyyz
+          // xzzz yzzz xxyy xxzz yyzz xxyz xyyz xyzz)
+          const double Cxx = H[0] + H[9] + H[10], Cyy = H[9] + H[1] + H[11],
+                       Czz = H[10] + H[11] + H[2], Cxy = H[3] + H[5] + H[14],
+                       Cxz = H[4] + H[13] + H[7], Cyz = H[12] + H[6] + H[8];
+          const double tc = Cxx + Cyy + Czz, a7 = 1.0 / 7.0, a35 = 1.0 / 35.0;
+          const double hxxxx = H[0] - 6.0 * a7 * Cxx + 3.0 * a35 * tc;
+          const double hxxxy = H[3] - 3.0 * a7 * Cxy, hxxxz = H[4] - 3.0 * a7 * Cxz;
+          const double hxxyy = H[9] - a7 * (Cxx + Cyy) + a35 * tc;
+          const double hxxyz = H[12] - a7 * Cyz, hxyyy = H[5] - 3.0 * a7 * Cxy;
+          const double hxyyz = H[13] - a7 * Cxz;
+          const double hyyyy = H[1] - 6.0 * a7 * Cyy + 3.0 * a35 * tc;
+          const double hyyyz = H[6] - 3.0 * a7 * Cyz;
+          const double hxxzz = H[10] - a7 * (Cxx + Czz) + a35 * tc;
+          const double hxyzz = H[14] - a7 * Cxy;
+          const double hyyzz = H[11] - a7 * (Cyy + Czz) + a35 * tc;
+          const double nx = ex * ri, ny = ey * ri, nz = ez * ri;
+          const double xx = nx * nx, yy = ny * ny, zz = nz * nz;
+          const double P1 = nx * (xx - 3.0 * zz), P2 = 3.0 * ny * (xx - zz);
+          const double P3 = nz * (3.0 * xx - zz), P4 = 3.0 * nx * (yy - zz);
+          const double P5 = 6.0 * nx * ny * nz, P6 = ny * (yy - 3.0 * zz);
+          const double P7 = nz * (3.0 * yy - zz);
+          const double Vx = hxxxx * P1 + hxxxy * P2 + hxxxz * P3 + hxxyy * P4 +
+                            hxxyz * P5 + hxyyy * P6 + hxyyz * P7;
+          const double Vy = hxxxy * P1 + hxxyy * P2 + hxxyz * P3 + hxyyy * P4 +
+                            hxyyz * P5 + hyyyy * P6 + hyyyz * P7;
+          const double Vz = hxxxz * P1 + hxxyz * P2 + hxxzz * P3 + hxyyz * P4 +
+                            hxyzz * P5 + hyyyz * P6 + hyyzz * P7;
+          const double H4 = nx * Vx + ny * Vy + nz * Vz;
+          const double ri6 = ri3 * ri3;
+          fx += 4.375 * ri6 * (9.0 * H4 * nx - 4.0 * Vx);
+          fy += 4.375 * ri6 * (9.0 * H4 * ny - 4.0 * Vy);
+          fz += 4.375 * ri6 * (9.0 * H4 * nz - 4.0 * Vz);
         }
         const int j0 = __ldg(&a.first[cn]), j1 = j0 + __ldg(&a.count[cn]);
         for (int j = j0; j < j1; ++j) {

@@ -42,7 +42,7 @@ constexpr int kMaxBlocksPerSm = 4;
 constexpr int kMinBlocksPerSm = 3;  // 80 registers: 24 resident warps per SM
 
 constexpr int kCandRing = 64;     // power of two, > 31 + 32
-constexpr int kCellF4 = 6;        // float4 per staged far-field cell
+constexpr int kCellF4 = 9;        // float4 per staged far-field cell (order 4)
 constexpr int kPartF4 = 5;        // float4 per staged source pair (4 used + pad)
 
 struct WarpSmem {
@@ -51,15 +51,21 @@ struct WarpSmem {
   int cq_node[kCandRing];  // learned-MAC candidates waiting for a full batch
   float cq_d[kCandRing];
   float cq_b[kCandRing];
-  // staged cells, kCellF4 float4 each: (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion),
-  // (Sxx, Syy, Szz, Sxy), (Syz, Szx, Txxx, Tyyy), (Tzzz, Txxy, Txxz, Txyy),
-  // (Tyyz, Txzz, Tyzz, Txyz) -- S and T trace-free
-  float4 cell[32 * kCellF4];
-  // staged sources in pairs, kPartF4 float4 per pair: sources 2b and 2b+1
-  // side by side, (nhx nhx' nhy nhy') (nhz nhz' q q') (nlx nlx' nly nly')
-  // (nlz nlz' idx idx'): negated hi / lo offsets from the group centre,
-  // charge, sorted index bits
-  float4 part[16 * kPartF4];
+  // The far-field and pair staging areas (and the learned MAC's feature
+  // rows, in `cell`) are used one at a time by the warp: one buffer.
+  union {
+    // staged cells, kCellF4 float4 each: (dx, dy, dz, Q), (Dx, Dy, Dz, q_ion),
+    // (Sxx, Syy, Szz, Sxy), (Syz, Szx, Txxx, Tyyy), (Tzzz, Txxy, Txxz, Txyy),
+    // (Tyyz, Txzz, Tyzz, Txyz), then for order 4 (Hxxxx, Hxxxy, Hxxxz, Hxxyy),
+    // (Hxxyz, Hxyyy, Hxyyz, Hyyyy), (Hyyyz, Hxxzz, Hxyzz, Hyyzz) -- S, T and
+    // H trace-free
+    float4 cell[32 * kCellF4];
+    // staged sources in pairs, kPartF4 float4 per pair: sources 2b and 2b+1
+    // side by side, (nhx nhx' nhy nhy') (nhz nhz' q q') (nlx nlx' nly nly')
+    // (nlz nlz' idx idx'): negated hi / lo offsets from the group centre,
+    // charge, sorted index bits
+    float4 part[16 * kPartF4];
+  };
   // pair constants of the group's cloud: 1/lambda^2 (ee, ei, ii), 1/rs,
   // 1/lambda (ee, ei, ii)
   float pk[8];
@@ -98,6 +104,7 @@ struct MixedArgs {
   const float* fmax;
   const float4* geom;
   const float4* mom3;
+  const float4* mom4;
   const float* margins;  // m_lo, m_hi, pre-filter coefficients c0..c4
   const double* f_prev;
   float eta_over_eps;
@@ -177,6 +184,12 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
     } else {
       cl[3] = make_float4(m2.x, m2.y, 0.f, 0.f);
     }
+    if (ORDER >= 4) {
+      const float4* hp = a.mom4 + 3 * (int64_t)node;
+      cl[6] = __ldg(hp);
+      cl[7] = __ldg(hp + 1);
+      cl[8] = __ldg(hp + 2);
+    }
   }
   __syncwarp();
   float fx = 0.f, fy = 0.f, fz = 0.f, pa = 0.f, pi = 0.f;
@@ -232,6 +245,39 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
       gx = fmaf(c7, Tx, gx);
       gy = fmaf(c7, Ty, gy);
       gz = fmaf(c7, Tz, gz);
+    }
+    if (ORDER >= 4) {
+      // hexadecapole: r^2 (-grad phi) += 39.375 s^4 H(n,n,n,n) n - 17.5 s^4
+      // H(., n, n, n); r phi += 4.375 s^4 H(n,n,n,n) (phi = 35/8 H(d,d,d,d)
+      // / r^9).  H is trace-free, so each component of H(., n, n, n) is a
+      // combination of seven cubic harmonics P1..P7 of n; the z component
+      // reads the three dependent components xxzz, xyzz, yyzz staged with
+      // the others.
+      const float4 H0 = cl[6], H1 = cl[7], H2 = cl[8];
+      const float xx = nx * nx, yy = ny * ny, zz3 = 3.f * nz * nz;
+      const float P1 = nx * (xx - zz3);
+      const float P6 = ny * (yy - zz3);
+      const float P2 = 3.f * ny * fmaf(nz, -nz, xx);
+      const float P4 = 3.f * nx * fmaf(nz, -nz, yy);
+      const float P3 = nz * fmaf(3.f, xx, -nz * nz);
+      const float P7 = nz * fmaf(3.f, yy, -nz * nz);
+      const float P5 = 6.f * nx * ny * nz;
+      // (xxxx xxxy xxxz xxyy) (xxyz xyyy xyyz yyyy) (yyyz xxzz xyzz yyzz)
+      const float Vx = fmaf(H0.x, P1, fmaf(H0.y, P2, fmaf(H0.z, P3, fmaf(H0.w, P4,
+                       fmaf(H1.x, P5, fmaf(H1.y, P6, H1.z * P7))))));
+      const float Vy = fmaf(H0.y, P1, fmaf(H0.w, P2, fmaf(H1.x, P3, fmaf(H1.y, P4,
+                       fmaf(H1.z, P5, fmaf(H1.w, P6, H2.x * P7))))));
+      const float Vz = fmaf(H0.z, P1, fmaf(H1.x, P2, fmaf(H2.y, P3, fmaf(H1.z, P4,
+                       fmaf(H2.z, P5, fmaf(H2.x, P6, H2.w * P7))))));
+      const float H4 = fmaf(nx, Vx, fmaf(ny, Vy, nz * Vz));
+      const float s4 = s2 * s2;
+      const float s4H = s4 * H4;
+      gp = fmaf(39.375f, s4H, gp);
+      php = fmaf(4.375f, s4H, php);
+      const float c9 = -17.5f * s4;
+      gx = fmaf(c9, Vx, gx);
+      gy = fmaf(c9, Vy, gy);
+      gz = fmaf(c9, Vz, gz);
     }
     fx = fmaf(s2, fmaf(gp, nx, gx), fx);
     fy = fmaf(s2, fmaf(gp, ny, gy), fy);
@@ -825,6 +871,7 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.digit, (size_t)cap);
   rc |= realloc_dev(&mb.m64, (size_t)kM64 * cap);
   rc |= realloc_dev(&mb.mom3, 3 * (size_t)cap);
+  rc |= realloc_dev(&mb.mom4, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.geom, (size_t)cap);
   rc |= realloc_dev(&mb.lvl_list, (size_t)cap);
@@ -848,7 +895,7 @@ int mixed_alloc_particles(MixedBuffers& mb, int n) {
 
 void mixed_free(MixedBuffers& mb) {
   void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
-                  mb.mom3, mb.geom, mb.xs, mb.groups, mb.stack, mb.control,
+                  mb.mom3, mb.mom4, mb.geom, mb.xs, mb.groups, mb.stack, mb.control,
                   mb.lvl_list, mb.lvl};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -864,6 +911,7 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
   m.m64 = mb.m64;
   m.mom = mb.mom;
   m.mom3 = mb.mom3;
+  m.mom4 = mb.mom4;
   m.geom = mb.geom;
   m.xs = mb.xs;
   m.groups = mb.groups;
@@ -928,6 +976,7 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.fmax = L ? learned->fmax : nullptr;
   a.geom = mb.geom;
   a.mom3 = mb.mom3;
+  a.mom4 = mb.mom4;
   a.margins = L ? learned->margins : nullptr;
   a.f_prev = L ? learned->f_prev : nullptr;
   a.eta_over_eps = L ? (float)(learned->eta / kEps) : 0.f;
@@ -958,7 +1007,8 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   } while (0)
 #define TG_LAUNCH_O(P, R, LL)                                                 \
   do {                                                                        \
-    if (tune.order >= 3) TG_LAUNCH(P, R, LL, 3);                              \
+    if (tune.order >= 4) TG_LAUNCH(P, R, LL, 4);                              \
+    else if (tune.order == 3) TG_LAUNCH(P, R, LL, 3);                         \
     else TG_LAUNCH(P, R, LL, 2);                                              \
   } while (0)
   if (wp.physics == 1) {

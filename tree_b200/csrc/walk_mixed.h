@@ -19,6 +19,7 @@ struct MixedBuffers {
   double2* m64 = nullptr;
   float4* mom = nullptr;
   float4* mom3 = nullptr;
+  float4* mom4 = nullptr;
   float4* geom = nullptr;
   double4* xs = nullptr;
   int2* groups = nullptr;
@@ -33,7 +34,7 @@ struct MixedBuffers {
 struct MixedTuning {
   int bucket = 8;          // twigs with <= bucket particles are summed directly
   int blocks_per_sm = 4;   // persistent grid: SMs x blocks_per_sm blocks
-  int order = 3;           // far-field order: 2 quadrupole, 3 octupole
+  int order = 3;           // far-field order: 2 quadrupole, 3 octupole, 4 hexadecapole
 };
 
 // Learned acceptance: a cell the fixed-theta test opens, with s/(d - dx) <=
