@@ -43,7 +43,7 @@ DT_S = 1e-11
 # (FMA = 2; divisions, square roots and exponentials count as one flop each).
 FLOPS_M2P_REF = 194    # tree.f90:736-779 evaluated literally (FP64 path)
 FLOPS_P2P_REF = 30     # leaf laws of tree.f90 / erf-Kelbg with the x^2>40 shortcut
-FLOPS_M2P_MIXED = {2: 50, 3: 100}  # FP32 trace-free far field to quadrupole / octupole
+FLOPS_M2P_MIXED = {2: 50, 3: 100, 4: 195}  # FP32 trace-free far field to order 2 / 3 / 4
 FLOPS_P2P_MIXED = 24   # FP32 erf-Kelbg pair with hi/lo offsets
 FLOPS_MLP = 2 * (16 * 64 + 64 * 64 + 64)  # one learned-MAC evaluation (BF16 mma + FP32)
 RDF_BYTES = 2 * 10001 * 8  # the two 64-bit RDF histograms read back per call

@@ -1,0 +1,42 @@
+"""Host-side helpers of bench.py (no GPU): the equal-accuracy fit of the plain
+FP64 arms and the workload description both arms print."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def test_equal_accuracy_recovers_power_laws():
+    # rms = 0.04 theta^3, ms = 50 theta^-3: rms 1e-4 at theta = (1/400)^(1/3)
+    pts = [(th, 0.04 * th ** 3, 50.0 * th ** -3) for th in (0.5, 0.35, 0.25)]
+    eq = bench.equal_accuracy(pts, 1e-4)
+    want = (1e-4 / 0.04) ** (1 / 3)
+    assert eq["theta"] == pytest.approx(want, rel=1e-9)
+    assert eq["ms_per_step"] == pytest.approx(50.0 * want ** -3, rel=1e-9)
+    assert eq["rms_exponent"] == pytest.approx(3.0) and eq["extrapolated"]
+
+
+def test_equal_accuracy_needs_two_usable_points():
+    assert bench.equal_accuracy([(0.5, 1e-2, 100.0)]) is None
+    assert bench.equal_accuracy([(0.5, None, 100.0), (0.3, 1e-3, 300.0)]) is None
+    # error growing as theta shrinks: no crossing to report
+    assert bench.equal_accuracy([(0.5, 1e-3, 100.0), (0.3, 1e-2, 300.0)]) is None
+
+
+def test_both_arms_describe_the_same_workload():
+    import argparse
+    args = argparse.Namespace(te=50.0, theta=0.3, physics="kelbg", no_rdf=False, nsamp=10)
+    a = bench.workload_config(args, 1048576)
+    b = bench.workload_config(args, 1048576)
+    assert a == b and a["rdf"] and a["n_particles"] == 1048576
+    assert not {"precision", "mac", "eta", "order", "bucket"} & set(a)
+
+
+def test_whole_job_rate():
+    assert bench.whole_job_rate(1000, 2, 10, 20.0) == pytest.approx(1e6)
+    assert np.isfinite(bench.whole_job_rate(1, 1, 1, 1e-3))
