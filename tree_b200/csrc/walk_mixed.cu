@@ -40,6 +40,10 @@ constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
 constexpr int kMaxBucket = 8;
 constexpr int kMaxBlocksPerSm = 4;
 constexpr int kMinBlocksPerSm = 3;  // 80 registers: 24 resident warps per SM
+// With RDF counts the walk runs one block of kRdfWarps per SM that keeps both
+// histograms (2 x 10001 u32) in shared memory and adds them to the global
+// bins once, when the block ends.
+constexpr int kRdfWarps = 16;
 
 constexpr int kCandRing = 64;     // power of two, > 31 + 32
 constexpr int kCellF4 = 9;        // float4 per staged far-field cell (order 4)
@@ -332,7 +336,8 @@ __device__ __noinline__ int rdf_bin64(const float4* __restrict__ blk, int half,
 // offsets, so the bins are those of the FP64 evaluation.  s: the source
 // index, or -1 when the pair was not close (it is then not the target).
 template <int PHYS>
-__device__ __forceinline__ void rdf_count(const MixedArgs& a, float r2, float ssign, int s,
+__device__ __forceinline__ void rdf_count(const MixedArgs& a, uint32_t* hist, float r2,
+                                          float ssign, int s,
                                           const float4* __restrict__ blk, int half,
                                           float thx, float thy, float thz, float tlx,
                                           float tly, float tlz, int p_self, int tsp) {
@@ -351,7 +356,7 @@ __device__ __forceinline__ void rdf_count(const MixedArgs& a, float r2, float ss
                      same ? a.dx_ii_inv : a.dx_ei_inv);
       if (id < 0) return;
     }
-    if (id >= 0 && id < kRdfBins) atomicAdd(&a.rdf[(same ? kRdfBins : 0) + id], 1u);
+    if (id >= 0 && id < kRdfBins) atomicAdd(&hist[(same ? kRdfBins : 0) + id], 1u);
   }
 }
 
@@ -430,7 +435,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
                                          float thy, float thz, float tlx,
                                          float tly, float tlz, float close2,
                                          int p_self, int tsp, bool act, int lane,
-                                         Acc& acc) {
+                                         uint32_t* hist, Acc& acc) {
   {
     // this lane's source (or, past cnt, a chargeless dummy 10^6 um away)
     float v[8];
@@ -514,8 +519,8 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
                     fx.y, fy.y, fz.y, pa.y, pq.y);
     }
     if (RDF && act) {
-      rdf_count<PHYS>(a, r2.x, q.x, s0, blk, 0, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
-      rdf_count<PHYS>(a, r2.y, q.y, s1, blk, 1, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
+      rdf_count<PHYS>(a, hist, r2.x, q.x, s0, blk, 0, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
+      rdf_count<PHYS>(a, hist, r2.y, q.y, s1, blk, 1, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
     }
   }
   __syncwarp();
@@ -528,23 +533,39 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
 }
 
 // --------------------------------------------------------------- walk ----
-// Dynamic shared memory: WarpSmem[kMxWarps], then (learned MAC only) the
-// packed network and the features' training range.
-template <bool LEARNED>
+// Dynamic shared memory: WarpSmem per warp, then (learned MAC only) the
+// packed network and the features' training range, then (RDF only) the two
+// block histograms.
+constexpr size_t walk_learned_bytes() {
+  return (sizeof(MlpPacked) + sizeof(float) * (2 * kMacFeatures + 8) + 15) / 16 * 16;
+}
+template <bool LEARNED, bool RDF>
 constexpr size_t walk_smem_bytes() {
-  return sizeof(WarpSmem) * kMxWarps +
-         (LEARNED ? sizeof(MlpPacked) + sizeof(float) * (2 * kMacFeatures + 8) : 0);
+  return sizeof(WarpSmem) * (RDF ? kRdfWarps : kMxWarps) + (LEARNED ? walk_learned_bytes() : 0) +
+         (RDF ? sizeof(uint32_t) * 2 * kRdfBins : 0);
 }
 
+// the largest variant must fit one block's opt-in shared memory (227 KB)
+static_assert(walk_smem_bytes<true, true>() <= 232448, "walk shared memory over 227 KB");
+static_assert(walk_smem_bytes<true, false>() * kMinBlocksPerSm <= 233472 - 3 * 1024,
+              "three walk blocks no longer fit one SM");
+
 template <int PHYS, bool RDF, bool LEARNED, int ORDER>
-__global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
+__global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : kMinBlocksPerSm)
     k_walk_mixed(MixedArgs a) {
+  constexpr int kW = RDF ? kRdfWarps : kMxWarps;
   extern __shared__ float4 dyn_smem[];
   WarpSmem* smem = reinterpret_cast<WarpSmem*>(dyn_smem);
-  MlpPacked* mlp = reinterpret_cast<MlpPacked*>(smem + kMxWarps);
+  unsigned char* tail = reinterpret_cast<unsigned char*>(smem + kW);
+  MlpPacked* mlp = reinterpret_cast<MlpPacked*>(tail);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(tail + (LEARNED ? walk_learned_bytes() : 0));
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   WarpSmem& sm = smem[wib];
+  if (RDF) {
+    for (int i = threadIdx.x; i < 2 * kRdfBins; i += blockDim.x) hist[i] = 0u;
+    __syncthreads();
+  }
   if (LEARNED) {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(a.packed);
     uint32_t* dst = reinterpret_cast<uint32_t*>(mlp);
@@ -564,7 +585,7 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
       frange[2 * kMacFeatures + threadIdx.x] = __ldg(&a.margins[threadIdx.x]);
     __syncthreads();
   }
-  const int gwarp = blockIdx.x * kMxWarps + wib;
+  const int gwarp = blockIdx.x * kW + wib;
   int32_t* stack = a.stack + (int64_t)gwarp * kStackCap;
   const unsigned lt = (1u << lane) - 1u;
   if (*((volatile int32_t*)a.err) & (kErrCapacity | kErrDepth | kErrNonFinite)) return;
@@ -799,7 +820,7 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
       __syncwarp();
       while (p2t - p2h >= 32) {
         eval_p2p<PHYS, RDF>(sm, p2h, 32, a, Gx, Gy, Gz, thx, thy, thz, tlx, tly,
-                            tlz, close2, pt, tsp, act, lane, acc);
+                            tlz, close2, pt, tsp, act, lane, hist, acc);
         p2h += 32;
         n_p2p += 32;
       }
@@ -815,7 +836,7 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
     }
     if (p2t > p2h) {
       eval_p2p<PHYS, RDF>(sm, p2h, p2t - p2h, a, Gx, Gy, Gz, thx, thy, thz, tlx,
-                          tly, tlz, close2, pt, tsp, act, lane, acc);
+                          tly, tlz, close2, pt, tsp, act, lane, hist, acc);
       n_p2p += p2t - p2h;
     }
     if (m2t > m2h) {
@@ -851,6 +872,14 @@ __global__ void __launch_bounds__(kMxThreads, kMinBlocksPerSm)
     }
   }
   if (lane == 0) atomicMax(&a.control[1], max_stack);
+  if (RDF) {
+    // every warp of the block has left the group loop: add the block's bins
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * kRdfBins; i += blockDim.x) {
+      const uint32_t v = hist[i];
+      if (v) atomicAdd(&a.rdf[i], v);
+    }
+  }
 }
 
 // ------------------------------------------------------------- memory ----
@@ -988,22 +1017,22 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.roots = ens.roots;
   a.cloud_pk = cloud_pk;
   int bps = tune.blocks_per_sm < 1 ? 1 : (tune.blocks_per_sm > kMaxBlocksPerSm ? kMaxBlocksPerSm : tune.blocks_per_sm);
-  int grid = (mb.grid_warps / (kMaxBlocksPerSm * kMxWarps)) * bps;
+  const int sms_grid = mb.grid_warps / (kMaxBlocksPerSm * kMxWarps);
+  int grid = sms_grid * bps;
   const bool r = rdf != nullptr;
-  const size_t s0 = walk_smem_bytes<false>(), s1 = walk_smem_bytes<true>();
   int dev = 0;
   cudaGetDevice(&dev);
 #define TG_LAUNCH(P, R, LL, O)                                                \
   do {                                                                        \
     auto kfn = k_walk_mixed<P, R, LL, O>;                                     \
-    const size_t sb = LL ? s1 : s0;                                           \
+    const size_t sb = walk_smem_bytes<LL, R>();                               \
     static unsigned attr_set = 0; /* devices with the smem limit raised */    \
     if (dev < 32 && !(attr_set & (1u << dev))) {                              \
       cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
                            (int)sb);                                          \
       attr_set |= 1u << dev;                                                  \
     }                                                                         \
-    kfn<<<grid, kMxThreads, sb, st>>>(a);                                     \
+    kfn<<<R ? sms_grid : grid, R ? 32 * kRdfWarps : kMxThreads, sb, st>>>(a); \
   } while (0)
 #define TG_LAUNCH_O(P, R, LL)                                                 \
   do {                                                                        \
