@@ -11,14 +11,15 @@ precision: the precision form -- seeded clouds at T_e in {10, 50, 200} K,
     targets, and the time per step.
 drift: the total energy 1/2 (mv2_el + mv2_ion) + Epot_e + Epot_i, sampled every
     10 steps over `steps` steps from the same seeded cloud, for the
-    mixed-precision walk with the learned criterion (theta 0.30, eta 3e-5) and
+    mixed-precision walk with the learned criterion (--order, --theta, --eta;
+    default 3, 0.30, 3e-5) and
     for the plain FP64 fixed-theta path (theta 0.5); reports the largest
     excursion |E - E_0| relative to the mean kinetic energy for both.
 learned: the learned-MAC form -- the mixed walk with the learned criterion
-    (theta 0.30, eta 3e-5) for `steps` steps from a seeded cloud at T_e = 50 K;
+    (--order, --theta, --eta) for `steps` steps from a seeded cloud at T_e = 50 K;
     at steps 1, 10, 100 and the last, the rms and max relative force error on
     16,384 seeded targets; the time per step, against a fixed-theta mixed walk
-    (theta 0.30) and the plain FP64 fixed-theta path (theta 0.5) timed over a
+    (same theta and order) and the plain FP64 fixed-theta path (theta 0.5) timed over a
     few steps from the final state (after one untimed step each), beside the
     learned walk timed over the same steps from the same state.
 
@@ -72,21 +73,21 @@ def precision(n, steps, seed, tes=(10.0, 50.0, 200.0), thetas=(0.3, 0.5, 0.7)):
                               "ms_per_step": (t1.ms_total - t0.ms_total) / steps}), flush=True)
 
 
-def drift(n, steps, seed, nsamp=10):
+def drift(n, steps, seed, nsamp=10, order=3, theta=0.30, eta=3e-5):
     dt = units.dt_code(1e-11)
     c = cloud.make_cloud(n, seed=seed)
-    params, stats, _ = learned_mac.load_model()
-    out = {}
-    arms = (("mixed_learned", api.Config(theta=0.30, physics=api.PHYS_KELBG,
+    params, stats, _ = learned_mac.load_model(order=order)
+    out = {"order": order, "theta": theta, "eta": eta}
+    arms = (("mixed_learned", api.Config(theta=theta, physics=api.PHYS_KELBG,
                                          precision=api.PREC_MIXED, mac=api.MAC_LEARNED)),
             ("fp64_plain", api.Config(theta=0.5, physics=api.PHYS_KELBG,
                                       precision=api.PREC_FP64)))
     for name, cfg in arms:
         with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
             if cfg.precision == api.PREC_MIXED:
-                tf.set_tuning(8, 4, 3)
+                tf.set_tuning(8, 4, order)
                 tf.mac_set_model(params, stats)
-                tf.mac_config(3e-5, 0.05, 0.9)
+                tf.mac_config(eta, 0.05, 0.9)
             tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
             t0 = tf.timings()
             rec = tf.run(dt, steps, nsamp=nsamp)
@@ -101,20 +102,20 @@ def drift(n, steps, seed, nsamp=10):
           flush=True)
 
 
-def learned(n, steps, seed, nplain=3):
+def learned(n, steps, seed, nplain=3, order=3, theta=0.30, eta=3e-5):
     dt = units.dt_code(1e-11)
     c = cloud.make_cloud(n, seed=seed)
     rng = np.random.default_rng(seed + 17)
     idx = np.sort(rng.choice(n, min(16384, n), replace=False))
-    params, stats, _ = learned_mac.load_model()
+    params, stats, _ = learned_mac.load_model(order=order)
     marks = sorted({m for m in (1, 10, 100, steps) if m <= steps})
-    cfg = api.Config(theta=0.30, physics=api.PHYS_KELBG, precision=api.PREC_MIXED,
+    cfg = api.Config(theta=theta, physics=api.PHYS_KELBG, precision=api.PREC_MIXED,
                      mac=api.MAC_LEARNED)
-    out = {"mode": "learned", "n": n, "steps": steps}
+    out = {"mode": "learned", "n": n, "steps": steps, "order": order}
     with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
-        tf.set_tuning(8, 4, 3)
+        tf.set_tuning(8, 4, order)
         tf.mac_set_model(params, stats)
-        tf.mac_config(3e-5, 0.05, 0.9)
+        tf.mac_config(eta, 0.05, 0.9)
         tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
         done, rows, ms = 0, [], 0.0
         for m in marks:
@@ -131,18 +132,18 @@ def learned(n, steps, seed, nplain=3):
         t0 = tf.timings()
         tf.step(dt, nplain)
         t1 = tf.timings()
-        out["learned"] = {"theta": 0.30, "eta": 3e-5, "audits": rows,
+        out["learned"] = {"theta": theta, "eta": eta, "audits": rows,
                           "ms_per_step": ms / steps,
                           "ms_per_step_from_final_state": (t1.ms_total - t0.ms_total) / nplain}
     # comparison arms from the final state: a few steps each, then an audit
-    arms = (("mixed_fixed_theta0.30", api.Config(theta=0.30, physics=api.PHYS_KELBG,
-                                                  precision=api.PREC_MIXED)),
+    arms = (("mixed_fixed_same_theta", api.Config(theta=theta, physics=api.PHYS_KELBG,
+                                                   precision=api.PREC_MIXED)),
             ("fp64_plain_theta0.5", api.Config(theta=0.5, physics=api.PHYS_KELBG,
                                                precision=api.PREC_FP64)))
     for name, acfg in arms:
         with api.TreeForce(len(c.x_el), len(c.x_ion), acfg) as tf:
             if acfg.precision == api.PREC_MIXED:
-                tf.set_tuning(8, 4, 3)
+                tf.set_tuning(8, 4, order)
             tf.load_state(st["x_el"], st["v_el"], st["f_el"], st["x_ion"], st["v_ion"], st["f_ion"])
             tf.step(dt, 1)  # graph capture and node-array growth, untimed
             t0 = tf.timings()
@@ -153,7 +154,7 @@ def learned(n, steps, seed, nplain=3):
                          "steps": nplain, "rms": rms, "max": mx}
     lf = out["learned"]["ms_per_step_from_final_state"]
     out["learned_over_fp64_plain"] = out["fp64_plain_theta0.5"]["ms_per_step"] / lf
-    out["learned_over_fixed"] = out["mixed_fixed_theta0.30"]["ms_per_step"] / lf
+    out["learned_over_fixed"] = out["mixed_fixed_same_theta"]["ms_per_step"] / lf
     print(json.dumps(out), flush=True)
 
 
@@ -163,13 +164,18 @@ def main():
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--order", type=int, default=3, help="far-field order (drift, learned)")
+    ap.add_argument("--theta", type=float, default=0.30, help="opening angle (drift, learned)")
+    ap.add_argument("--eta", type=float, default=3e-5, help="learned budget (drift, learned)")
     args = ap.parse_args()
     if args.mode == "precision":
         precision(args.n or 1048576, args.steps or 1000, args.seed)
     elif args.mode == "drift":
-        drift(args.n or 1048576, args.steps or 1000, args.seed)
+        drift(args.n or 1048576, args.steps or 1000, args.seed, order=args.order,
+              theta=args.theta, eta=args.eta)
     else:
-        learned(args.n or 4194304, args.steps or 500, args.seed)
+        learned(args.n or 4194304, args.steps or 500, args.seed, order=args.order,
+                theta=args.theta, eta=args.eta)
 
 
 if __name__ == "__main__":
