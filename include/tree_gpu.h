@@ -162,7 +162,10 @@ typedef struct tree_gpu_sample {
  * device.  rdf_ei / rdf_ii (kRdfBins = 10001 entries each, either may be
  * NULL) accumulate the near-field pair counts of EVERY step, as NS%RDF_ei /
  * NS%RDF_ii do in Force (tree.f90:918, 1126); the caller dumps and resets
- * them as RDF (sample.f90:5-50) does every Ndump steps. */
+ * them as RDF (sample.f90:5-50) does every Ndump steps.  The FP64 path bins
+ * the reference's leaf pairs by their FP64 distance; the mixed path bins the
+ * pairs it sums directly by their FP32 distance (within ~1e-6 relative, so a
+ * pair that close to a bin edge may fall in the neighbouring bin). */
 int tree_gpu_run(tree_gpu_handle* h, double dt, int32_t nsteps, int32_t nsamp,
                  tree_gpu_sample* series, int32_t series_cap, int32_t* n_series,
                  int64_t* rdf_ei, int64_t* rdf_ii);

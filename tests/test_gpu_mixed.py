@@ -152,27 +152,31 @@ def test_mixed_rdf_counts_pairs(device_lib):
         tf.force(xe, xi, rei, rii)
     # theta -> 0: every e-i pair is a leaf pair, counted once per target side
     d = np.linalg.norm(xe[:, None, :] - xi[None, :, :], axis=2)
-    want = np.bincount(np.minimum((d / 0.01).astype(np.int64), 10001).ravel(),
-                       minlength=10002)[:10001]
-    diff = np.abs(rei - 2 * want)
-    # pair offsets are exact to ~1e-14 um (hi/lo split); bins are FP64
-    assert diff.sum() <= 1e-5 * 2 * want.sum()
+    want = 2 * np.bincount(np.minimum((d / 0.01).astype(np.int64), 10001).ravel(),
+                           minlength=10002)[:10001]
+    # bins come from the FP32 distance (about 1e-6 relative): a pair that
+    # close to a bin edge may be counted in the neighbouring bin, so the
+    # totals agree and the cumulative counts differ by a few such pairs
+    assert abs(int(rei.sum()) - int(want.sum())) <= 1e-4 * want.sum()
+    assert np.abs(np.cumsum(rei) - np.cumsum(want)).max() <= 2e-3 * want.sum()
+    assert np.abs(rei - want).sum() <= 1e-2 * want.sum()
 
 
 def test_far_field_orders_converge(device_lib):
-    """A compact cluster far from a group of targets: the error of its
-    accepted cells falls with each expansion order (quadrupole, octupole,
-    hexadecapole) by about the cluster's size over its distance."""
+    """A compact cluster a few cluster sizes from a group of targets (near
+    enough that the truncation error stays far above FP32 rounding): the
+    error of its accepted cells falls with each expansion order (quadrupole,
+    octupole, hexadecapole) by about the cluster's size over its distance."""
     rng = np.random.default_rng(31)
     src_e = rng.uniform(-1.0, 1.0, (40, 3))
     src_i = rng.uniform(-1.0, 1.0, (60, 3))
-    tgt = rng.uniform(-0.2, 0.2, (24, 3)) + np.array([9.0, 3.0, -4.0])
+    tgt = rng.uniform(-0.2, 0.2, (24, 3)) + np.array([4.5, 1.0, -1.0])
     xe = np.vstack([src_e, tgt[:12]])
     xi = np.vstack([src_i, tgt[12:]])
     targets = np.concatenate([np.arange(40, 52), 52 + 60 + np.arange(12)])
     errs = {}
     for order in (2, 3, 4):
-        with api.TreeForce(len(xe), len(xi), _mixed(0.6)) as tf:
+        with api.TreeForce(len(xe), len(xi), _mixed(0.9)) as tf:
             tf.set_tuning(1, 4, order)  # bucket 1: every accepted cell is a multipole
             f_el, f_ion, _, _ = tf.force(xe, xi)
             assert tf.timings().n_m2p > 0

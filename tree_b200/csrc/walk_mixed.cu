@@ -95,8 +95,7 @@ struct MixedArgs {
   float inv_lam2_ee, inv_lam2_ei, inv_lam2_ii;
   float inv_lam_ee, inv_lam_ei, inv_lam_ii;
   float rs_inv;
-  double dx_ei_inv, dx_ii_inv;
-  float dx_ei_inv_f, dx_ii_inv_f;
+  float dx_ei_inv_f, dx_ii_inv_f;  // 1 / RDF bin widths
   double* f;
   double2* epot_part;
   uint32_t* rdf;
@@ -312,52 +311,33 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
 // particles on one point -- are redone with hi + lo, whose FP32 roundings are
 // relative to their own results, and only they need the source index.
 
-// FP64 bin of a pair near a bin edge, from the staged hi / lo parts (rare;
-// kept out of line so its registers do not weigh on the pair loop); -1
-// beyond the last bin.
-__device__ __noinline__ int rdf_bin64(const float4* __restrict__ blk, int half,
-                                      float thx, float thy, float thz, float tlx,
-                                      float tly, float tlz, double inv) {
-  const float4 q0 = blk[0], q1 = blk[1], q2 = blk[2], q3 = blk[3];
-  const float ngx = half ? q0.y : q0.x, ngy = half ? q0.w : q0.z, ngz = half ? q1.y : q1.x;
-  const float nlx = half ? q2.y : q2.x, nly = half ? q2.w : q2.z, nlz = half ? q3.y : q3.x;
-  const double ex = ((double)thx + (double)ngx) + ((double)tlx + (double)nlx);
-  const double ey = ((double)thy + (double)ngy) + ((double)tly + (double)nly);
-  const double ez = ((double)thz + (double)ngz) + ((double)tlz + (double)nlz);
-  const double t = sqrt(ex * ex + ey * ey + ez * ez) * inv;
-  return t < (double)kRdfBins ? (int)t : -1;
-}
-
-// RDF count of one pair (e-i for every target, i-i for ion targets, as
-// Search_Tree_ie/ei/ii bin them).  The bin comes from the FP32 distance,
-// within 1e-6 relative of the FP64 one (see above; 3e-7 for pairs formed with
-// hi + lo); only when that estimate lies within 2e-6 t of a bin edge (or of
-// the last bin's edge) is the distance recomputed in FP64 from the staged
-// offsets, so the bins are those of the FP64 evaluation.  s: the source
-// index, or -1 when the pair was not close (it is then not the target).
+// RDF counts of two pairs (e-i for every target, i-i for ion targets, as
+// Search_Tree_ie/ei/ii bin them).  The bin is the FP32 distance r = r2 /
+// sqrt(r2) (rsqrt within 2 ulp) over the bin width: within about 1e-6
+// relative of the FP64 distance (see above), so a pair within that of a bin
+// edge can land in the neighbouring bin; the FP64 path bins in FP64.
+// s0 / s1: the source indices, or -1 when a pair was not close (it is then
+// not the target).
 template <int PHYS>
-__device__ __forceinline__ void rdf_count(const MixedArgs& a, uint32_t* hist, float r2,
-                                          float ssign, int s,
-                                          const float4* __restrict__ blk, int half,
-                                          float thx, float thy, float thz, float tlx,
-                                          float tly, float tlz, int p_self, int tsp) {
-  const bool same = ssign == (tsp ? 1.f : -1.f);
-  const bool counted = PHYS == 1 ? s != p_self : (same ? r2 > 0.01f : true);
-  if (ssign != 0.f && counted && (!same || tsp == 1)) {
-    const float t32 = sqrtf(r2) * (same ? a.dx_ii_inv_f : a.dx_ei_inv_f);
-    const float tol = fmaf(t32, 2e-6f, 1e-30f);
-    if (t32 - tol >= (float)kRdfBins) return;  // beyond the last bin either way
-    const float fl = floorf(t32);
-    int id;
-    if (t32 - fl > tol && fl + 1.f - t32 > tol && t32 + tol < (float)kRdfBins) {
-      id = (int)fl;
-    } else {
-      id = rdf_bin64(blk, half, thx, thy, thz, tlx, tly, tlz,
-                     same ? a.dx_ii_inv : a.dx_ei_inv);
-      if (id < 0) return;
-    }
-    if (id >= 0 && id < kRdfBins) atomicAdd(&hist[(same ? kRdfBins : 0) + id], 1u);
-  }
+__device__ __forceinline__ void rdf_count2(const MixedArgs& a, uint32_t* hist, float2 r2,
+                                           float2 rinv, float2 q, int s0, int s1,
+                                           int p_self, int tsp) {
+  const float tq = tsp ? 1.f : -1.f;
+  const bool same0 = q.x == tq, same1 = q.y == tq;
+  const float2 inv = make_float2(same0 ? a.dx_ii_inv_f : a.dx_ei_inv_f,
+                                 same1 ? a.dx_ii_inv_f : a.dx_ei_inv_f);
+  const float2 t = __fmul2_rn(__fmul2_rn(r2, rinv), inv);
+  // counted pairs: a source (q != 0) of the other species, or an ion for an
+  // ion target; never the target itself (Kelbg) or inside the same-species
+  // cutoff (reference laws)
+  const bool ok0 = q.x != 0.f && (!same0 || tsp == 1) &&
+                   (PHYS == 1 ? s0 != p_self : (same0 ? r2.x > 0.01f : true));
+  const bool ok1 = q.y != 0.f && (!same1 || tsp == 1) &&
+                   (PHYS == 1 ? s1 != p_self : (same1 ? r2.y > 0.01f : true));
+  // r2 = 0 (distinct particles on one point): bin 0
+  const float t0 = r2.x > 0.f ? t.x : 0.f, t1 = r2.y > 0.f ? t.y : 0.f;
+  if (ok0 && t0 < (float)kRdfBins) atomicAdd(&hist[(same0 ? kRdfBins : 0) + (int)t0], 1u);
+  if (ok1 && t1 < (float)kRdfBins) atomicAdd(&hist[(same1 ? kRdfBins : 0) + (int)t1], 1u);
 }
 
 // One source against this lane's target with every case of the pair laws:
@@ -503,8 +483,8 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
       sp0 = q.x == tq ? !(r2.x > 0.01f) : r2.x * rs2 < 400.f;
       sp1 = q.y == tq ? !(r2.y > 0.01f) : r2.y * rs2 < 400.f;
     }
+    const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
     if (!(sp0 || sp1)) {
-      const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
       const float2 ph = __fmul2_rn(q, rinv);
       const float2 fs = __fmul2_rn(ph, __fmul2_rn(rinv, rinv));
       fx = __ffma2_rn(fs, dx, fx);
@@ -518,10 +498,7 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
       p2p_one<PHYS>(sm, r2.y, dx.y, dy.y, dz.y, q.y, s1, p_self, tsp,
                     fx.y, fy.y, fz.y, pa.y, pq.y);
     }
-    if (RDF && act) {
-      rdf_count<PHYS>(a, hist, r2.x, q.x, s0, blk, 0, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
-      rdf_count<PHYS>(a, hist, r2.y, q.y, s1, blk, 1, thx, thy, thz, tlx, tly, tlz, p_self, tsp);
-    }
+    if (RDF && act) rdf_count2<PHYS>(a, hist, r2, rinv, q, s0, s1, p_self, tsp);
   }
   __syncwarp();
   kahan_add(acc.sx, acc.cx, fx.x + fx.y);
@@ -986,10 +963,8 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.inv_lam_ei = (float)(1.0 / wp.lam_ei);
   a.inv_lam_ii = (float)(1.0 / wp.lam_ii);
   a.rs_inv = (float)(1.0 / wp.rs);
-  a.dx_ei_inv = 1.0 / wp.dx_ei;
-  a.dx_ii_inv = 1.0 / wp.dx_ii;
-  a.dx_ei_inv_f = (float)a.dx_ei_inv;
-  a.dx_ii_inv_f = (float)a.dx_ii_inv;
+  a.dx_ei_inv_f = (float)(1.0 / wp.dx_ei);
+  a.dx_ii_inv_f = (float)(1.0 / wp.dx_ii);
   a.f = f;
   a.epot_part = epot_part;
   a.rdf = rdf;
