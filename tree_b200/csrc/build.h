@@ -73,6 +73,27 @@ struct BuildBuffers {
   Ensemble ens;
 };
 
+// Largest c with start[c] <= i (start[0] = 0, nseg entries searched).
+__device__ __forceinline__ int seg_of(const int32_t* __restrict__ start, int nseg,
+                                      int i) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&start[mid]) <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Sorted particle p's common levels with its neighbours: lo with p - 1, hi
+// with p + 1 (-1 where the species ends).
+__device__ __forceinline__ void lo_hi(const int8_t* __restrict__ L, int p,
+                                      int& lo, int& hi) {
+  lo = p == 0 ? -1 : (int)L[p - 1];
+  hi = (int)L[p];
+  if (lo < 0 && hi < 0) hi = 0;  // single-particle species: root + leaf
+}
+
 int radix_blocks(int n);
 int scan_partials_needed(int n);
 int exclusive_scan(const int32_t* in, int32_t* out, int n, int32_t* partial,
@@ -88,5 +109,9 @@ int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
 // one combined tree with net-charge moments and target groups (mixed path).
 int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
                 double theta, int mode, cudaStream_t st);
+// The net-charge moments of the combined tree (mode 1) once its topology and
+// child tables exist.
+int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double theta,
+                const Ensemble& ens, cudaStream_t st);
 
 }  // namespace tg
