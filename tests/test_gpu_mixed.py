@@ -163,26 +163,34 @@ def test_mixed_rdf_counts_pairs(device_lib):
 
 
 def test_far_field_orders_converge(device_lib):
-    """A compact cluster a few cluster sizes from a group of targets (near
-    enough that the truncation error stays far above FP32 rounding): the
-    error of its accepted cells falls with each expansion order (quadrupole,
-    octupole, hexadecapole) by about the cluster's size over its distance."""
+    """A neutral cluster (50 electrons, 50 ions in [-1, 1]^3) and one target
+    5.5 cluster half-widths away along each axis in turn, so that the target's
+    force is the cluster's field alone and the truncation error of the
+    accepted cells (about a quarter of the cluster each, extent over distance
+    about 0.2) stays far above FP32 rounding: the error falls with each
+    expansion order (quadrupole, octupole, hexadecapole)."""
     rng = np.random.default_rng(31)
-    src_e = rng.uniform(-1.0, 1.0, (40, 3))
-    src_i = rng.uniform(-1.0, 1.0, (60, 3))
-    tgt = rng.uniform(-0.2, 0.2, (24, 3)) + np.array([4.5, 1.0, -1.0])
-    xe = np.vstack([src_e, tgt[:12]])
-    xi = np.vstack([src_i, tgt[12:]])
-    targets = np.concatenate([np.arange(40, 52), 52 + 60 + np.arange(12)])
+    src_e = rng.uniform(-1.0, 1.0, (50, 3))
+    src_i = rng.uniform(-1.0, 1.0, (50, 3))
+    tgts = [np.array(v) for v in ((5.5, 0.1, -0.2), (-5.5, 0.3, 0.1), (0.2, 5.5, 0.1),
+                                  (-0.1, -5.5, 0.2), (0.1, -0.2, 5.5), (0.3, 0.1, -5.5))]
     errs = {}
     for order in (2, 3, 4):
-        with api.TreeForce(len(xe), len(xi), _mixed(0.9)) as tf:
-            tf.set_tuning(1, 4, order)  # bucket 1: every accepted cell is a multipole
-            f_el, f_ion, _, _ = tf.force(xe, xi)
-            assert tf.timings().n_m2p > 0
-            fd, _ = tf.direct(targets)
-        f = np.vstack([f_el, f_ion])[targets]
-        errs[order] = float(np.sqrt(np.mean(_rel(f, fd) ** 2)))
+        rel = []
+        for k, t in enumerate(tgts):
+            ion = k % 2 == 1
+            xe = src_e if ion else np.vstack([src_e, t[None]])
+            xi = np.vstack([src_i, t[None]]) if ion else src_i
+            target = len(xe) + 50 if ion else 50
+            with api.TreeForce(len(xe), len(xi), _mixed(0.9)) as tf:
+                tf.set_tuning(1, 4, order)  # bucket 1: every accepted cell is a multipole
+                f_el, f_ion, _, _ = tf.force(xe, xi)
+                assert tf.timings().n_m2p > 0
+                fd, _ = tf.direct(np.array([target]))
+            f = np.vstack([f_el, f_ion])[[target]]
+            rel.append(float(_rel(f, fd)[0]))
+        errs[order] = float(np.sqrt(np.mean(np.square(rel))))
+    assert errs[4] > 1e-6, errs  # truncation, not FP32 rounding
     assert errs[3] < 0.5 * errs[2] and errs[4] < 0.5 * errs[3], errs
 
 
