@@ -157,6 +157,15 @@ MODULE TREE_GPU_MOD
        INTEGER(C_INT64_T), INTENT(OUT) :: n_nodes
      END FUNCTION
 
+     INTEGER(C_INT) FUNCTION tree_gpu_net_dump(h, cap, centre, moments, first, &
+          count, level, sorted, n_nodes) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_INT64_T
+       TYPE(C_PTR), VALUE :: h
+       INTEGER(C_INT64_T), VALUE :: cap
+       TYPE(C_PTR), VALUE :: centre, moments, first, count, level, sorted
+       INTEGER(C_INT64_T), INTENT(OUT) :: n_nodes
+     END FUNCTION
+
      INTEGER(C_INT) FUNCTION tree_gpu_set_stream(h, stream) BIND(C)
        IMPORT :: C_INT, C_PTR
        TYPE(C_PTR), VALUE :: h, stream

@@ -32,7 +32,7 @@ EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
            "tree_gpu_set_state", "tree_gpu_load_state", "tree_gpu_step",
            "tree_gpu_run", "tree_gpu_set_graphs", "tree_gpu_get_nloop",
            "tree_gpu_get_state", "tree_gpu_direct", "tree_gpu_direct_static",
-           "tree_gpu_tree_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning",
+           "tree_gpu_tree_dump", "tree_gpu_net_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning",
            "tree_gpu_mac_collect", "tree_gpu_mac_samples", "tree_gpu_mac_clear",
            "tree_gpu_mac_train", "tree_gpu_mac_set_model",
            "tree_gpu_mac_get_model", "tree_gpu_mac_config", "tree_gpu_mlp_grad",
@@ -111,6 +111,8 @@ def load_library(path: str = LIB_PATH):
     L.tree_gpu_tree_dump.argtypes = [vp, ctypes.c_int32, ctypes.c_int64, dp,
                                      dp, dp, ctypes.POINTER(ctypes.c_int32),
                                      lp, lp, lp]
+    L.tree_gpu_net_dump.argtypes = [vp, ctypes.c_int64, dp, dp, lp, lp,
+                                    ctypes.POINTER(ctypes.c_int32), dp, lp]
     L.tree_gpu_direct.argtypes = [vp, lp, ctypes.c_int64, dp, dp]
     L.tree_gpu_direct_static.argtypes = [vp, ctypes.c_int64, ctypes.c_int64,
                                          ctypes.POINTER(Params), vp,
@@ -364,6 +366,29 @@ class TreeForce:
             skip.ctypes.data_as(lp), pt.ctypes.data_as(lp), ctypes.byref(n)))
         return dict(centre=centre, moments=mom, rcrit=rcrit, level=level,
                     skip=skip, pt=pt)
+
+    def net_dump(self):
+        """The combined tree of the mixed path after the last build (pre-order):
+        centre (m, 3), moments (m, 38) -- n, Q, D[3], q_ion, S[6] (xx yy zz xy
+        yz zx), T[10], H[15], 0 -- first, count, level (m,), and the sorted
+        particles (n, 4): x, y, z, 1 for ions."""
+        n = ctypes.c_int64()
+        self._check(self.lib.tree_gpu_net_dump(self.h, 0, None, None, None, None, None,
+                                               None, ctypes.byref(n)))
+        m = n.value
+        centre = np.zeros((m, 3))
+        mom = np.zeros((m, 38))
+        first = np.zeros(m, np.int64)
+        count = np.zeros(m, np.int64)
+        level = np.zeros(m, np.int32)
+        xs = np.zeros((self.n_el + self.n_ion, 4))
+        lp = ctypes.POINTER(ctypes.c_int64)
+        self._check(self.lib.tree_gpu_net_dump(
+            self.h, m, _dp(centre), _dp(mom), first.ctypes.data_as(lp),
+            count.ctypes.data_as(lp), level.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            _dp(xs), ctypes.byref(n)))
+        return dict(centre=centre, moments=mom, first=first, count=count, level=level,
+                    sorted=xs)
 
     def set_stream(self, stream_handle: int | None):
         """Enqueue later work on a caller's cudaStream_t (an integer handle,

@@ -946,6 +946,57 @@ int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
   return TREE_GPU_OK;
 }
 
+int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* moments,
+                      int64_t* first, int64_t* count, int32_t* level, double* sorted,
+                      int64_t* n_nodes) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (h->b.ens.nseg > 0)
+    return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: no combined-tree dump");
+  if (h->prm.precision != TREE_GPU_PREC_MIXED)
+    return fail(h, TREE_GPU_ERR_ARG, "the combined tree exists on the mixed path only");
+  int32_t bnd[4];
+  CK(cudaMemcpy(bnd, h->b.bounds, sizeof(bnd), cudaMemcpyDeviceToHost));
+  const int m = std::min(bnd[2], h->b.cap);
+  if (n_nodes) *n_nodes = m;
+  if (!centre && !moments && !first && !count && !level && !sorted) return TREE_GPU_OK;
+  if (cap < m) return fail(h, TREE_GPU_ERR_ARG, "dump buffer too small");
+  std::vector<double4> c(m);
+  std::vector<double2> mm((size_t)tg::kM64 * m);
+  std::vector<int32_t> fi(m), co(m), pt(m);
+  std::vector<int8_t> lv(m);
+  if (m) {
+    CK(cudaMemcpy(c.data(), h->b.node_c, m * sizeof(double4), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(mm.data(), h->b.mx.m64, (size_t)tg::kM64 * m * sizeof(double2),
+                  cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(fi.data(), h->b.mx.first, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(co.data(), h->b.mx.count, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pt.data(), h->b.node_pt, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(lv.data(), h->b.node_level, m * sizeof(int8_t), cudaMemcpyDeviceToHost));
+  }
+  for (int i = 0; i < m; ++i) {
+    if (centre) {
+      centre[3 * (size_t)i] = c[i].x;
+      centre[3 * (size_t)i + 1] = c[i].y;
+      centre[3 * (size_t)i + 2] = c[i].z;
+    }
+    if (moments) {
+      // the FP64 record (n, Q) (Dx, Dy) (Dz, q_ion) (Sxx, Syy) (Szz, Sxy) (Syz, Szx) T H
+      double* o = moments + 38 * (size_t)i;
+      const bool leaf = pt[i] >= 0;
+      for (int u = 0; u < tg::kM64; ++u) {
+        o[2 * u] = leaf ? 0.0 : mm[(size_t)tg::kM64 * i + u].x;
+        o[2 * u + 1] = leaf ? 0.0 : mm[(size_t)tg::kM64 * i + u].y;
+      }
+    }
+    if (first) first[i] = fi[i];
+    if (count) count[i] = co[i];
+    if (level) level[i] = lv[i];
+  }
+  if (sorted && h->n > 0)
+    CK(cudaMemcpy(sorted, h->mb.xs, (size_t)h->n * sizeof(double4), cudaMemcpyDeviceToHost));
+  return TREE_GPU_OK;
+}
+
 int tree_gpu_set_stream(tree_gpu_handle* h, void* stream) {
   if (!h) return TREE_GPU_ERR_ARG;
   CK(cudaStreamSynchronize(h->st));

@@ -15,38 +15,47 @@ namespace tg {
 __constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
 
 // Combined tree (both species in one tree) for the mixed-precision walk.  Per
-// node: particle count n, centroid X (the expansion centre), net charge Q,
-// dipole D = sum q (x - X), second moment S = 1/2 sum q (x - X)(x - X)^T and
-// the ion count.  Children are combined exactly (parallel axis):
-//   d_c = X_c - X,  D = sum D_c + Q_c d_c,
-//   S = sum S_c + (D_c d_c^T + d_c D_c^T)/2 + Q_c d_c d_c^T / 2.
-// In a quasi-neutral plasma Q ~ 0 for large cells and the far field is the
-// small net (dipole/quadrupole) field, so its truncation error is relative to
-// that net field rather than to each species' monopole.
-// Also the third moment T_ijk = sum q a_i a_j a_k (a = x - X), combined with
+// twig: particle count n, centroid X (the expansion centre), net charge Q,
+// ion count, dipole D = sum q a, second moment S = 1/2 sum q a a^T, third
+// moment T_ijk = sum q a_i a_j a_k and fourth moment H_ijkl = sum q a_i a_j
+// a_k a_l (a = x - X).  In a quasi-neutral plasma Q ~ 0 for large cells and
+// the far field is the small net (dipole, quadrupole, ...) field, so its
+// truncation error is relative to that net field rather than to each
+// species' monopole.
+//
+// Twigs of at most kMidCount particles sum their particles directly (P2M):
+// every such twig is independent of the others, so the whole lower tree is
+// one parallel pass with no waiting on children.  The few twigs above are
+// combined from their children by the parallel-axis rules (d_c = X_c - X):
+//   D = sum D_c + Q_c d_c,
+//   S = sum S_c + (D_c d_c^T + d_c D_c^T)/2 + Q_c d_c d_c^T / 2,
 //   T += T_c + d_i S2_jk + d_j S2_ik + d_k S2_ij + d_i d_j D_k + d_i D_j d_k
-//        + D_i d_j d_k + Q_c d_i d_j d_k      (S2 = 2 S of the child)
-// -- the octupole the quadrupole expansion leaves out, whose size sets the
-// error of accepting the cell.
-// Also the fourth moment H_ijkl = sum q a_i a_j a_k a_l, combined with
+//        + D_i d_j d_k + Q_c d_i d_j d_k      (S2 = 2 S of the child),
 //   H += H_c + 4 sym(d T_c) + 6 sym(d d S2_c) + 4 sym(d d d D_c) + Q_c d d d d
-// (sym: the distinct index placements), for the hexadecapole far field.
-// m64 per node (19 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
+// (sym: the distinct index placements); a leaf child is a point charge.
+//
+// m64 per twig (19 x double2): (n, Q) | (Dx, Dy) | (Dz, q_ion) | (Sxx, Syy) |
 // (Szz, Sxy) | (Syz, Szx) | T in the order xxx yyy zzz xxy xxz xyy yyz xzz
 // yzz xyz | H in the order xxxx yyyy zzzz xxxy xxxz xyyy yyyz xzzz yzzz xxyy
 // xxzz yyzz xxyz xyyz xyzz, 0 (all raw, for the FP64 labels of the learned
-// criterion).  The FP32
-// copies the walk evaluates are trace-free, which drops every trace term from
-// the far-field formula (phi = Q/r + D.d/r^3 + 3 d.S'.d/r^5 + 5/2 T'(d,d,d)/r^7):
+// criterion).  The FP32 copies the walk evaluates are trace-free, which drops
+// every trace term from the far-field formula (phi = Q/r + D.d/r^3 +
+// 3 d.S'.d/r^5 + 5/2 T'(d,d,d)/r^7 + 35/8 H'(d,d,d,d)/r^9):
 // S' = S - tr(S)/3 I and T'_ijk = T_ijk - (d_ij V_k + d_ik V_j + d_jk V_i)/5
-// with V_k = T_iik.  mom per node (3 x float4): (Q, Dx, Dy, Dz),
-// (S'xx, S'yy, S'zz, Sxy), (Syz, Szx, trace S, q_ion); mom3 per node
+// with V_k = T_iik.  mom per twig (3 x float4): (Q, Dx, Dy, Dz),
+// (S'xx, S'yy, S'zz, Sxy), (Syz, Szx, trace S, q_ion); mom3 per twig
 // (3 x float4): (T'xxx, T'yyy, T'zzz, T'xxy), (T'xxz, T'xyy, T'yyz, T'xzz),
-// (T'yzz, Txyz, |T'|_F, 0); mom4 per node (3 x float4): trace-free H'
+// (T'yzz, Txyz, |T'|_F, 0); mom4 per twig (3 x float4): trace-free H'
 // (xxxx, xxxy, xxxz, xxyy), (xxyz, xyyy, xyyz, yyyy), (yyyz, xxzz, xyzz,
-// yyzz); geom (s, dx, n, |S'|_F).
-// Leaves of the combined tree (one per sorted particle) and the sorted
-// positions the walk reads.
+// yyzz); geom (s, dx, n, |S'|_F).  Leaves carry no moment records: the walk
+// sums them as particles and the parallel-axis pass treats them as point
+// charges.
+constexpr int kMidCount = 2048;   // twigs up to this size: direct sums (P2M)
+constexpr int kSmallCount = 64;   // twigs up to this size: 8 lanes each, else a warp
+
+// Leaves of the combined tree (one per sorted particle): the position with
+// w = -1 (the walk's leaf mark), and the sorted positions the walk and the
+// direct sums read (w = 1 for ions).
 __global__ void k_net_leaves(const double* __restrict__ x,
                              const uint32_t* __restrict__ vals,
                              const int8_t* __restrict__ L,
@@ -65,45 +74,255 @@ __global__ void k_net_leaves(const double* __restrict__ x,
   // sorting keeps each cloud's index range, so p and o share the cloud
   const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, p) : 0;
   const bool ion = (int)o >= (ens.nseg > 0 ? __ldg(&ens.elec_end[seg]) : n_el_charge);
-  const double q = ion ? 1.0 : -1.0;
   const double px = x[3 * (int64_t)o], py = x[3 * (int64_t)o + 1],
                pz = x[3 * (int64_t)o + 2];
   node_c[leaf] = make_double4(px, py, pz, -1.0);
-  {
-    double2* m = mx.m64 + kM64 * (int64_t)leaf;
-    m[0] = make_double2(1.0, q);
-    m[1] = make_double2(0.0, 0.0);
-    m[2] = make_double2(0.0, ion ? 1.0 : 0.0);
+  mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
+}
+
+// ---- the records of one twig ----
+// Count, centroid, net charge, ion count, dipole and second moment of twig
+// cur: node_c (centroid, critical radius smax / theta + |X - box centre|),
+// m64[0..5], mom and geom.  gc: the twig's geometric centre.
+__device__ void net_store_low(int cur, double nsum, double X0, double X1, double X2,
+                              double Q, double qi, double Dx, double Dy, double Dz,
+                              double Sxx, double Syy, double Szz, double Sxy, double Syz,
+                              double Szx, double4 gc, double smax0, double theta,
+                              const int8_t* __restrict__ node_level, double4* node_c,
+                              const MixedNodes& mx) {
+  const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
+  const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+  const int lev = node_level[cur];
+  double smax = smax0;
+  for (int l = 0; l < lev; ++l) smax = smax * 0.5;
+  node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
+  double2* m = mx.m64 + kM64 * (int64_t)cur;
+  m[0] = make_double2(nsum, Q);
+  m[1] = make_double2(Dx, Dy);
+  m[2] = make_double2(Dz, qi);
+  m[3] = make_double2(Sxx, Syy);
+  m[4] = make_double2(Szz, Sxy);
+  m[5] = make_double2(Syz, Szx);
+  const double trS = Sxx + Syy + Szz;
+  const double Sxxt = Sxx - trS / 3.0, Syyt = Syy - trS / 3.0, Szzt = Szz - trS / 3.0;
+  const double sn = sqrt(Sxxt * Sxxt + Syyt * Syyt + Szzt * Szzt +
+                         2.0 * (Sxy * Sxy + Syz * Syz + Szx * Szx));
+  float4* f = mx.mom + 3 * (int64_t)cur;
+  f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
+  f[1] = make_float4((float)Sxxt, (float)Syyt, (float)Szzt, (float)Sxy);
+  f[2] = make_float4((float)Syz, (float)Szx, (float)trS, (float)qi);
+  mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, (float)sn);
+}
+
+// Third moment T of twig cur (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz):
+// m64[6..10] and the trace-free mom3 with its Frobenius norm.
+__device__ void net_store_T(int cur, const double (&T)[10], const MixedNodes& mx) {
+  double2* m = mx.m64 + kM64 * (int64_t)cur;
 #pragma unroll
-    for (int u = 3; u < kM64; ++u) m[u] = make_double2(0.0, 0.0);
-    float4* f3 = mx.mom3 + 3 * (int64_t)leaf;
-    f3[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-    f3[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-    f3[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4* f4 = mx.mom4 + 3 * (int64_t)leaf;
-    f4[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-    f4[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-    f4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4* f = mx.mom + 3 * (int64_t)leaf;
-    f[0] = make_float4((float)q, 0.f, 0.f, 0.f);
-    f[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-    f[2] = make_float4(0.f, 0.f, 0.f, ion ? 1.f : 0.f);
-    mx.geom[leaf] = make_float4(0.f, 0.f, 1.f, 0.f);
-    mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
+  for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+  const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
+  double Tt[10];
+  Tt[0] = T[0] - 0.6 * Vx;
+  Tt[1] = T[1] - 0.6 * Vy;
+  Tt[2] = T[2] - 0.6 * Vz;
+  Tt[3] = T[3] - 0.2 * Vy;
+  Tt[4] = T[4] - 0.2 * Vz;
+  Tt[5] = T[5] - 0.2 * Vx;
+  Tt[6] = T[6] - 0.2 * Vz;
+  Tt[7] = T[7] - 0.2 * Vx;
+  Tt[8] = T[8] - 0.2 * Vy;
+  Tt[9] = T[9];
+  double tn = 0.0;
+#pragma unroll
+  for (int u = 0; u < 10; ++u) tn += kTMult[u] * Tt[u] * Tt[u];
+  float4* f3 = mx.mom3 + 3 * (int64_t)cur;
+  f3[0] = make_float4((float)Tt[0], (float)Tt[1], (float)Tt[2], (float)Tt[3]);
+  f3[1] = make_float4((float)Tt[4], (float)Tt[5], (float)Tt[6], (float)Tt[7]);
+  f3[2] = make_float4((float)Tt[8], (float)Tt[9], (float)sqrt(tn), 0.f);
+}
+
+// Fourth moment H of twig cur (order xxxx yyyy zzzz xxxy xxxz xyyy yyyz xzzz
+// yzzz xxyy xxzz yyzz xxyz xyyz xyzz): m64[11..18] and the 12 components of
+// the trace-free H' = H - sym(delta C)/7 + sym(delta delta) tr C/35 with
+// C_kl = H_mmkl that the walk's hexadecapole reads.
+__device__ void net_store_H(int cur, const double (&H)[15], const MixedNodes& mx) {
+  double2* m = mx.m64 + kM64 * (int64_t)cur;
+#pragma unroll
+  for (int u = 0; u < 7; ++u) m[11 + u] = make_double2(H[2 * u], H[2 * u + 1]);
+  m[18] = make_double2(H[14], 0.0);
+  const double Cxx = H[0] + H[9] + H[10], Cyy = H[9] + H[1] + H[11],
+               Czz = H[10] + H[11] + H[2], Cxy = H[3] + H[5] + H[14],
+               Cxz = H[4] + H[13] + H[7], Cyz = H[12] + H[6] + H[8];
+  const double c = Cxx + Cyy + Czz;
+  const double a7 = 1.0 / 7.0, a35 = 1.0 / 35.0;
+  float4* f4 = mx.mom4 + 3 * (int64_t)cur;
+  f4[0] = make_float4((float)(H[0] - 6.0 * a7 * Cxx + 3.0 * a35 * c),  // xxxx
+                      (float)(H[3] - 3.0 * a7 * Cxy),                  // xxxy
+                      (float)(H[4] - 3.0 * a7 * Cxz),                  // xxxz
+                      (float)(H[9] - a7 * (Cxx + Cyy) + a35 * c));      // xxyy
+  f4[1] = make_float4((float)(H[12] - a7 * Cyz),                       // xxyz
+                      (float)(H[5] - 3.0 * a7 * Cxy),                  // xyyy
+                      (float)(H[13] - a7 * Cxz),                       // xyyz
+                      (float)(H[1] - 6.0 * a7 * Cyy + 3.0 * a35 * c));  // yyyy
+  f4[2] = make_float4((float)(H[6] - 3.0 * a7 * Cyz),                  // yyyz
+                      (float)(H[10] - a7 * (Cxx + Czz) + a35 * c),     // xxzz
+                      (float)(H[14] - a7 * Cxy),                       // xyzz
+                      (float)(H[11] - a7 * (Cyy + Czz) + a35 * c));     // yyzz
+}
+
+// ---- direct moments (P2M) ----
+// Sum over the G lanes of an aligned lane group (butterfly: every lane of the
+// group ends with the same total, added in the same order).
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Moments of twig t straight from its particles (the sorted range first ..
+// first + count - 1 of xs): the centroid, then Q, q_ion, D, S and T about it,
+// then H.  G lanes share the twig: lane `sub` takes every G-th particle and
+// the group adds the lanes' sums after each pass; lane 0 of the group stores.
+// Every lane of the warp calls this together (t < 0: a group without a twig,
+// which still takes part in the shuffles).
+template <int G>
+__device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double theta,
+                        double4* node_c, const int8_t* __restrict__ node_level,
+                        const MixedNodes& mx, const Ensemble& ens) {
+  int first = 0, cnt = 0;
+  if (t >= 0) {
+    first = __ldg(&mx.first[t]);
+    cnt = __ldg(&mx.count[t]);
+  }
+  const double4* __restrict__ xs = mx.xs + first;
+  // pass 1: centroid
+  double X0 = 0.0, X1 = 0.0, X2 = 0.0;
+  for (int j = sub; j < cnt; j += G) {
+    const double4 p = ldg_d4(&xs[j]);
+    X0 += p.x;
+    X1 += p.y;
+    X2 += p.z;
+  }
+  X0 = group_sum<G>(X0);
+  X1 = group_sum<G>(X1);
+  X2 = group_sum<G>(X2);
+  const double nsum = (double)cnt;
+  if (cnt > 0) {
+    X0 /= nsum;
+    X1 /= nsum;
+    X2 /= nsum;
+  }
+  // pass 2: Q, q_ion, D, 2 S and T about the centroid
+  double Q = 0, qi = 0, Dx = 0, Dy = 0, Dz = 0;
+  double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
+  double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int j = sub; j < cnt; j += G) {
+    const double4 p = ldg_d4(&xs[j]);
+    const double q = p.w > 0.5 ? 1.0 : -1.0;
+    const double ax = p.x - X0, ay = p.y - X1, az = p.z - X2;
+    const double qx = q * ax, qy = q * ay, qz = q * az;
+    const double qxx = qx * ax, qyy = qy * ay, qzz = qz * az;
+    const double qxy = qx * ay, qyz = qy * az, qzx = qz * ax;
+    Q += q;
+    qi += p.w;
+    Dx += qx;
+    Dy += qy;
+    Dz += qz;
+    Sxx += qxx;
+    Syy += qyy;
+    Szz += qzz;
+    Sxy += qxy;
+    Syz += qyz;
+    Szx += qzx;
+    T[0] += qxx * ax;  // xxx
+    T[1] += qyy * ay;  // yyy
+    T[2] += qzz * az;  // zzz
+    T[3] += qxx * ay;  // xxy
+    T[4] += qxx * az;  // xxz
+    T[5] += qyy * ax;  // xyy
+    T[6] += qyy * az;  // yyz
+    T[7] += qzz * ax;  // xzz
+    T[8] += qzz * ay;  // yzz
+    T[9] += qxy * az;  // xyz
+  }
+  Q = group_sum<G>(Q);
+  qi = group_sum<G>(qi);
+  Dx = group_sum<G>(Dx);
+  Dy = group_sum<G>(Dy);
+  Dz = group_sum<G>(Dz);
+  Sxx = 0.5 * group_sum<G>(Sxx);
+  Syy = 0.5 * group_sum<G>(Syy);
+  Szz = 0.5 * group_sum<G>(Szz);
+  Sxy = 0.5 * group_sum<G>(Sxy);
+  Syz = 0.5 * group_sum<G>(Syz);
+  Szx = 0.5 * group_sum<G>(Szx);
+#pragma unroll
+  for (int u = 0; u < 10; ++u) T[u] = group_sum<G>(T[u]);
+  if (t >= 0 && sub == 0) {
+    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, first) : 0;
+    const double4 gc = ldg_d4(&node_c[t]);  // geometric centre (topology)
+    net_store_low(t, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx, gc,
+                  geom[seg].smax0, theta, node_level, node_c, mx);
+    net_store_T(t, T, mx);
+  }
+  // pass 3: H about the centroid
+  double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int j = sub; j < cnt; j += G) {
+    const double4 p = ldg_d4(&xs[j]);
+    const double q = p.w > 0.5 ? 1.0 : -1.0;
+    const double ax = p.x - X0, ay = p.y - X1, az = p.z - X2;
+    const double qxx = q * ax * ax, qyy = q * ay * ay, qzz = q * az * az;
+    H[0] += qxx * ax * ax;   // xxxx
+    H[1] += qyy * ay * ay;   // yyyy
+    H[2] += qzz * az * az;   // zzzz
+    H[3] += qxx * ax * ay;   // xxxy
+    H[4] += qxx * ax * az;   // xxxz
+    H[5] += qyy * ay * ax;   // xyyy
+    H[6] += qyy * ay * az;   // yyyz
+    H[7] += qzz * az * ax;   // xzzz
+    H[8] += qzz * az * ay;   // yzzz
+    H[9] += qxx * ay * ay;   // xxyy
+    H[10] += qxx * az * az;  // xxzz
+    H[11] += qyy * az * az;  // yyzz
+    H[12] += qxx * ay * az;  // xxyz
+    H[13] += qyy * ax * az;  // xyyz
+    H[14] += qzz * ax * ay;  // xyzz
+  }
+#pragma unroll
+  for (int u = 0; u < 15; ++u) H[u] = group_sum<G>(H[u]);
+  if (t >= 0 && sub == 0) net_store_H(t, H, mx);
+}
+
+// ---- parallel-axis moments of the twigs above ----
+// The first K double2 of child c's moment record, or a point charge's (n = 1,
+// charge q, ion count) for a leaf.
+template <int K>
+__device__ __forceinline__ void child_rec(int c, bool leaf, const MixedNodes& mx,
+                                          double2 (&r)[K]) {
+  if (leaf) {
+    const double w = __ldg(&mx.xs[__ldg(&mx.first[c])].w);
+#pragma unroll
+    for (int u = 0; u < K; ++u) r[u] = make_double2(0.0, 0.0);
+    r[0] = make_double2(1.0, w > 0.5 ? 1.0 : -1.0);
+    if (K > 2) r[2 % K].y = w;
+  } else {
+    const double2* cm = mx.m64 + kM64 * (int64_t)c;
+#pragma unroll
+    for (int u = 0; u < K; ++u) r[u] = __ldcg(cm + u);
   }
 }
 
 // Net moments of twig `cur` from its children (all final): centroid, then
 // Q, D, S, T and H about it by the parallel-axis rules, each summed over the
 // children in pre-order (ascending octant digit, the order of the child
-// table); writes the FP64 record and the trace-free FP32 copies.  One pass
-// over the children per moment order keeps few accumulators live at a time
-// (the children's records are re-read from L1/L2); the child indices come
-// from one read of the child table, so the loads of all children are
-// independent.
+// table).  One pass over the children per moment order keeps few
+// accumulators live at a time (the children's records are re-read from
+// L1/L2); the child indices come from one read of the child table, so the
+// loads of all children are independent.
 __device__ bool net_twig(int cur, double smax0, double theta, int cap,
                          double4* node_c, const int8_t* __restrict__ node_level,
-                         MixedNodes mx, int32_t* err) {
+                         const MixedNodes& mx, int32_t* err) {
   const double4 gc = ldcg_d4(&node_c[cur]);  // geometric centre (topology)
   int kid[8];
   {
@@ -125,7 +344,7 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     const int c = kid[j];
     if (c < 0) continue;
     const double4 cc = ldcg_d4(&node_c[c]);
-    const double nc = __ldcg(mx.m64 + kM64 * (int64_t)c).x;
+    const double nc = cc.w < 0.0 ? 1.0 : __ldcg(mx.m64 + kM64 * (int64_t)c).x;
     nsum += nc;
     X0 += nc * cc.x;
     X1 += nc * cc.y;
@@ -134,7 +353,6 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
   X0 /= nsum;
   X1 /= nsum;
   X2 /= nsum;
-  double2* m = mx.m64 + kM64 * (int64_t)cur;
   // pass 2: net charge, dipole and second moment about the centroid
   {
     double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
@@ -144,9 +362,9 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       const int c = kid[j];
       if (c < 0) continue;
       const double4 cc = ldcg_d4(&node_c[c]);
-      const double2* cm = mx.m64 + kM64 * (int64_t)c;
-      const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
-                    a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
+      double2 r[6];
+      child_rec<6>(c, cc.w < 0.0, mx, r);
+      const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3], a4 = r[4], a5 = r[5];
       const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
       const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
       Q += qc;
@@ -161,30 +379,10 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       Syz += a5.x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez;
       Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
     }
-    const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
-    const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
-    const int lev = node_level[cur];
-    double smax = smax0;
-    for (int l = 0; l < lev; ++l) smax = smax * 0.5;
-    node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
-    m[0] = make_double2(nsum, Q);
-    m[1] = make_double2(Dx, Dy);
-    m[2] = make_double2(Dz, qi);
-    m[3] = make_double2(Sxx, Syy);
-    m[4] = make_double2(Szz, Sxy);
-    m[5] = make_double2(Syz, Szx);
-    const double trS = Sxx + Syy + Szz;
-    const double Sxxt = Sxx - trS / 3.0, Syyt = Syy - trS / 3.0, Szzt = Szz - trS / 3.0;
-    const double sn = sqrt(Sxxt * Sxxt + Syyt * Syyt + Szzt * Szzt +
-                           2.0 * (Sxy * Sxy + Syz * Syz + Szx * Szx));
-    float4* f = mx.mom + 3 * (int64_t)cur;
-    f[0] = make_float4((float)Q, (float)Dx, (float)Dy, (float)Dz);
-    f[1] = make_float4((float)Sxxt, (float)Syyt, (float)Szzt, (float)Sxy);
-    f[2] = make_float4((float)Syz, (float)Szx, (float)trS, (float)qi);
-    mx.geom[cur] = make_float4((float)smax, (float)dx, (float)nsum, (float)sn);
+    net_store_low(cur, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx, gc,
+                  smax0, theta, node_level, node_c, mx);
   }
-  // pass 3: third moment, parallel axis (T in the order xxx yyy zzz xxy xxz
-  // xyy yyz xzz yzz xyz)
+  // pass 3: third moment
   {
     double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 1
@@ -192,9 +390,9 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       const int c = kid[j];
       if (c < 0) continue;
       const double4 cc = ldcg_d4(&node_c[c]);
-      const double2* cm = mx.m64 + kM64 * (int64_t)c;
-      const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
-                    a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
+      double2 r[11];
+      child_rec<11>(c, cc.w < 0.0, mx, r);
+      const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3], a4 = r[4], a5 = r[5];
       const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
       const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
       const double S2xx = 2 * a3.x, S2yy = 2 * a3.y, S2zz = 2 * a4.x, S2xy = 2 * a4.y,
@@ -202,9 +400,8 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       double Tc[10];
 #pragma unroll
       for (int u = 0; u < 5; ++u) {
-        const double2 t2 = __ldcg(cm + 6 + u);
-        Tc[2 * u] = t2.x;
-        Tc[2 * u + 1] = t2.y;
+        Tc[2 * u] = r[6 + u].x;
+        Tc[2 * u + 1] = r[6 + u].y;
       }
     T[0] += Tc[0] + ex * S2xx + ex * S2xx + ex * S2xx + ex * ex * dcx + ex * dcx * ex + dcx * ex * ex + qc * ex * ex * ex;
     T[1] += Tc[1] + ey * S2yy + ey * S2yy + ey * S2yy + ey * ey * dcy + ey * dcy * ey + dcy * ey * ey + qc * ey * ey * ey;
@@ -217,32 +414,9 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     T[8] += Tc[8] + ey * S2zz + ez * S2yz + ez * S2yz + ey * ez * dcz + ey * dcz * ez + dcy * ez * ez + qc * ey * ez * ez;
     T[9] += Tc[9] + ex * S2yz + ey * S2xz + ez * S2xy + ex * ey * dcz + ex * dcy * ez + dcx * ey * ez + qc * ex * ey * ez;
     }
-#pragma unroll
-    for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
-    // trace-free parts (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz)
-    const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
-    double Tt[10];
-    Tt[0] = T[0] - 0.6 * Vx;
-    Tt[1] = T[1] - 0.6 * Vy;
-    Tt[2] = T[2] - 0.6 * Vz;
-    Tt[3] = T[3] - 0.2 * Vy;
-    Tt[4] = T[4] - 0.2 * Vz;
-    Tt[5] = T[5] - 0.2 * Vx;
-    Tt[6] = T[6] - 0.2 * Vz;
-    Tt[7] = T[7] - 0.2 * Vx;
-    Tt[8] = T[8] - 0.2 * Vy;
-    Tt[9] = T[9];
-    double tn = 0.0;
-#pragma unroll
-    for (int u = 0; u < 10; ++u) tn += kTMult[u] * Tt[u] * Tt[u];
-    float4* f3 = mx.mom3 + 3 * (int64_t)cur;
-    f3[0] = make_float4((float)Tt[0], (float)Tt[1], (float)Tt[2], (float)Tt[3]);
-    f3[1] = make_float4((float)Tt[4], (float)Tt[5], (float)Tt[6], (float)Tt[7]);
-    f3[2] = make_float4((float)Tt[8], (float)Tt[9], (float)sqrt(tn), 0.f);
+    net_store_T(cur, T, mx);
   }
-  // pass 4: fourth moment, parallel axis: H += H_c + 4 sym(d T_c) + 6 sym(d d
-  // S2_c) + 4 sym(d d d D_c) + Q_c d d d d (H in the order xxxx yyyy zzzz xxxy
-  // xxxz xyyy yyyz xzzz yzzz xxyy xxzz yyzz xxyz xyyz xyzz)
+  // pass 4: fourth moment
   {
     double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 1
@@ -250,23 +424,20 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       const int c = kid[j];
       if (c < 0) continue;
       const double4 cc = ldcg_d4(&node_c[c]);
-      const double2* cm = mx.m64 + kM64 * (int64_t)c;
-      const double2 a0 = __ldcg(cm), a1 = __ldcg(cm + 1), a2 = __ldcg(cm + 2),
-                    a3 = __ldcg(cm + 3), a4 = __ldcg(cm + 4), a5 = __ldcg(cm + 5);
+      double2 r[19];
+      child_rec<19>(c, cc.w < 0.0, mx, r);
+      const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3], a4 = r[4], a5 = r[5];
       const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
       const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
       const double S2xx = 2 * a3.x, S2yy = 2 * a3.y, S2zz = 2 * a4.x, S2xy = 2 * a4.y,
                    S2yz = 2 * a5.x, S2xz = 2 * a5.y;
-      const double2 t0 = __ldcg(cm + 6), t1 = __ldcg(cm + 7), t2 = __ldcg(cm + 8),
-                    t3 = __ldcg(cm + 9), t4 = __ldcg(cm + 10);
-      const double Txxx = t0.x, Tyyy = t0.y, Tzzz = t1.x, Txxy = t1.y, Txxz = t2.x,
-                   Txyy = t2.y, Tyyz = t3.x, Txzz = t3.y, Tyzz = t4.x, Txyz = t4.y;
+      const double Txxx = r[6].x, Tyyy = r[6].y, Tzzz = r[7].x, Txxy = r[7].y, Txxz = r[8].x,
+                   Txyy = r[8].y, Tyyz = r[9].x, Txzz = r[9].y, Tyzz = r[10].x, Txyz = r[10].y;
       double Hc[16];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        const double2 h2 = __ldcg(cm + 11 + u);
-        Hc[2 * u] = h2.x;
-        Hc[2 * u + 1] = h2.y;
+        Hc[2 * u] = r[11 + u].x;
+        Hc[2 * u + 1] = r[11 + u].y;
       }
     H[0] += Hc[0] + 4.0 * ex * Txxx + 6.0 * ex * ex * S2xx + 4.0 * ex * ex * ex * dcx + qc * ex * ex * ex * ex;
     H[1] += Hc[1] + 4.0 * ey * Tyyy + 6.0 * ey * ey * S2yy + 4.0 * ey * ey * ey * dcy + qc * ey * ey * ey * ey;
@@ -284,190 +455,185 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     H[13] += Hc[13] + ex * Tyyz + 2.0 * ey * Txyz + ez * Txyy + 2.0 * ex * ey * S2yz + ex * ez * S2yy + ey * ey * S2xz + 2.0 * ey * ez * S2xy + ey * ey * ez * dcx + 2.0 * ex * ey * ez * dcy + ex * ey * ey * dcz + qc * ex * ey * ey * ez;
     H[14] += Hc[14] + ex * Tyzz + ey * Txzz + 2.0 * ez * Txyz + ex * ey * S2zz + 2.0 * ex * ez * S2yz + 2.0 * ey * ez * S2xz + ez * ez * S2xy + ey * ez * ez * dcx + ex * ez * ez * dcy + 2.0 * ex * ey * ez * dcz + qc * ex * ey * ez * ez;
     }
-#pragma unroll
-    for (int u = 0; u < 7; ++u) m[11 + u] = make_double2(H[2 * u], H[2 * u + 1]);
-    m[18] = make_double2(H[14], 0.0);
-    // trace-free H' = H - sym(delta C)/7 + sym(delta delta) tr C/35, C_kl = H_mmkl;
-    // the walk's hexadecapole reads 12 components
-    const double Cxx = H[0] + H[9] + H[10], Cyy = H[9] + H[1] + H[11],
-                 Czz = H[10] + H[11] + H[2], Cxy = H[3] + H[5] + H[14],
-                 Cxz = H[4] + H[13] + H[7], Cyz = H[12] + H[6] + H[8];
-    const double c = Cxx + Cyy + Czz;
-    const double a7 = 1.0 / 7.0, a35 = 1.0 / 35.0;
-    float4* f4 = mx.mom4 + 3 * (int64_t)cur;
-    f4[0] = make_float4((float)(H[0] - 6.0 * a7 * Cxx + 3.0 * a35 * c),  // xxxx
-                        (float)(H[3] - 3.0 * a7 * Cxy),                  // xxxy
-                        (float)(H[4] - 3.0 * a7 * Cxz),                  // xxxz
-                        (float)(H[9] - a7 * (Cxx + Cyy) + a35 * c));      // xxyy
-    f4[1] = make_float4((float)(H[12] - a7 * Cyz),                       // xxyz
-                        (float)(H[5] - 3.0 * a7 * Cxy),                  // xyyy
-                        (float)(H[13] - a7 * Cxz),                       // xyyz
-                        (float)(H[1] - 6.0 * a7 * Cyy + 3.0 * a35 * c));  // yyyy
-    f4[2] = make_float4((float)(H[6] - 3.0 * a7 * Cyz),                  // yyyz
-                        (float)(H[10] - a7 * (Cxx + Czz) + a35 * c),     // xxzz
-                        (float)(H[14] - a7 * Cxy),                       // xyzz
-                        (float)(H[11] - a7 * (Cyy + Czz) + a35 * c));     // yyzz
+    net_store_H(cur, H, mx);
   }
   return true;
 }
 
-// Upward pass over the twigs in two launches.  "Small" twigs hold at most
-// kSubCount particles and kSubNodes nodes (a child of a small twig is small);
-// each maximal small subtree is completed by one warp: per-node counts of
-// pending twig children in shared memory, a shared queue of ready twigs, and
-// rounds in which the lanes complete every ready twig at once and release
-// the parents whose last child they completed.  The twigs above count the
-// twig children they wait for in global memory; the lane that completes a
-// subtree root decrements its parent's count, and the last arrival completes
-// the parent and climbs on (fence, atomic, fence: the children's records are
-// visible to the thread that completes the parent).  The arithmetic per twig
-// is net_twig's whichever lane runs it.
-constexpr int kSubCount = 64;
-constexpr int kSubNodes = 512;
-constexpr int kNetWarps = 4;
-constexpr int kNetBlocksPerSm = 8;
+// ---- the pass ----
+// Twigs are sorted into work classes by particle count: 32-64, 16-31, 8-15,
+// 4-7 and 2-3 (one thread each, in that order, so that a warp's twigs take
+// about as many iterations), 65 .. kMidCount (a warp each), and the twigs
+// above kMidCount whose twig children are all below it (where the
+// parallel-axis climb starts).  The other twigs above kMidCount count the
+// children of their own kind that they wait for in node_done.
+constexpr int kNetClasses = 7;  // class index: 0..4 one thread, 5 a warp, 6 climb start
+constexpr int kNetThreads = 256;
 
-__device__ __forceinline__ bool net_small(int i, int cap, const int32_t* __restrict__ node_skip,
-                                          const MixedNodes& mx) {
-  int end = node_skip[i];
-  if (end > cap) end = cap;
-  return mx.count[i] <= kSubCount && end - i <= kSubNodes;
+__device__ __forceinline__ int net_class_of(int c) {
+  if (c > kMidCount) return 6;
+  if (c > kSmallCount) return 5;
+  return c >= 32 ? 0 : c >= 16 ? 1 : c >= 8 ? 2 : c >= 4 ? 3 : 4;
 }
 
-// Marks the pass: node_done[t] = twig children of each twig t above the small
-// subtrees; list / *nlist: the roots of the maximal small subtrees.
-__global__ void k_net_mark(const int32_t* __restrict__ bounds, int cap,
-                           const int32_t* __restrict__ node_pt,
-                           const int32_t* __restrict__ node_parent,
-                           const int32_t* __restrict__ node_skip,
-                           int32_t* node_done, MixedNodes mx, int32_t* list,
-                           int32_t* nlist) {
+// Class of twig i (-1: a leaf, or a large twig reached by the climb); sets
+// node_done of the large twigs when `mark` is on.
+__device__ __forceinline__ int net_class(int i, int cap, const int32_t* __restrict__ node_pt,
+                                         const MixedNodes& mx, int32_t* node_done,
+                                         bool mark) {
+  if (node_pt[i] >= 0) return -1;
+  const int k = net_class_of(mx.count[i]);
+  if (k != 6) return k;
+  if (!mark) return node_done[i] == 0 ? 6 : -1;
+  const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)i);
+  const int4 k0 = kk[0], k1 = kk[1];
+  const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+  int big = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    big += (kv[j] >= 0 && kv[j] < cap && node_pt[kv[j]] < 0 && mx.count[kv[j]] > kMidCount)
+               ? 1 : 0;
+  node_done[i] = big;
+  return big == 0 ? 6 : -1;
+}
+
+// Pass 1 of the sort into classes: totals per class (tot[0..6]).
+__global__ void __launch_bounds__(kNetThreads)
+    k_net_mark(const int32_t* __restrict__ bounds, int cap,
+               const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
+               int32_t* tot) {
+  __shared__ int32_t h[kNetClasses];
+  if (threadIdx.x < kNetClasses) h[threadIdx.x] = 0;
+  __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m || node_pt[i] >= 0) return;  // twigs only
-  if (!net_small(i, cap, node_skip, mx)) {
-    const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)i);
-    const int4 k0 = kk[0], k1 = kk[1];
-    const int kv[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
-    int tw = 0;
+  if (i < m) {
+    const int k = net_class(i, cap, node_pt, mx, node_done, true);
+    if (k >= 0) atomicAdd(&h[k], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < kNetClasses && h[threadIdx.x] > 0) atomicAdd(&tot[threadIdx.x], h[threadIdx.x]);
+}
+
+// Pass 2: each twig appended to its class's range of the list (classes in
+// index order; order inside a class is arbitrary -- the arithmetic per twig
+// is not).  cur[0..6]: per-class cursors.
+__global__ void __launch_bounds__(kNetThreads)
+    k_net_fill(const int32_t* __restrict__ bounds, int cap,
+               const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
+               const int32_t* __restrict__ tot, int32_t* cur, int32_t* list) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = i < m ? net_class(i, cap, node_pt, mx, node_done, false) : -1;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) tw += (kv[j] >= 0 && kv[j] < cap && node_pt[kv[j]] < 0) ? 1 : 0;
-    node_done[i] = tw;
-  } else {
-    const int par = node_parent[i];
-    if (par < 0 || !net_small(par, cap, node_skip, mx)) list[atomicAdd(nlist, 1)] = i;
+  for (int c = 0; c < kNetClasses; ++c) {
+    const unsigned bm = __ballot_sync(0xffffffffu, k == c);
+    if (bm != 0) {
+      const int leader = __ffs(bm) - 1;
+      int off = 0;
+      if (lane == leader) off = atomicAdd(&cur[c], __popc(bm));
+      off = __shfl_sync(0xffffffffu, off, leader);
+      if (k == c) list[base + off + __popc(bm & ((1u << lane) - 1u))] = i;
+    }
+    base += tot[c];
   }
 }
 
-__global__ void __launch_bounds__(32 * kNetWarps, 4)
-    k_net_subtrees(const Geom* __restrict__ geom, double theta, int cap,
-                   double4* node_c, const int32_t* __restrict__ node_skip,
-                   const int32_t* __restrict__ node_pt,
-                   const int32_t* __restrict__ node_parent, int32_t* node_done,
-                   const int8_t* __restrict__ node_level, MixedNodes mx,
-                   Ensemble ens, const int32_t* __restrict__ list,
-                   const int32_t* __restrict__ nlist, int32_t* cursor, int32_t* err) {
-  __shared__ int32_t s_pend[kNetWarps][kSubNodes];  // pending twig children
-  __shared__ int16_t s_queue[kNetWarps][kSubNodes];  // ready twigs (local index)
-  __shared__ int32_t s_tail[kNetWarps];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int32_t* pend = s_pend[w];
-  int16_t* queue = s_queue[w];
-  const int total = *nlist;
-  for (;;) {
-    int k = 0;
-    if (lane == 0) k = atomicAdd(cursor, 1);
-    k = __shfl_sync(0xffffffffu, k, 0);
-    if (k >= total) return;
-    if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
-    const int r = list[k];
-    int end = node_skip[r];
-    if (end > cap) end = cap;
-    const int nn = end - r;  // <= kSubNodes (a small subtree)
-    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[r]) : 0;
+// One thread per twig of classes 0..4 (list[0 .. tot[0] + ... + tot[4])).
+__global__ void __launch_bounds__(kNetThreads)
+    k_net_p2m_thread(const Geom* __restrict__ geom, double theta, double4* node_c,
+                     const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
+                     const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
+                     int32_t* err) {
+  const int total = tot[0] + tot[1] + tot[2] + tot[3] + tot[4];
+  if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
+    net_p2m<1>(list[k], 0, geom, theta, node_c, node_level, mx, ens);
+}
+
+// One warp per twig of class 5.
+__global__ void __launch_bounds__(kNetThreads)
+    k_net_p2m_warp(const Geom* __restrict__ geom, double theta, double4* node_c,
+                   const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
+                   const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
+                   int32_t* err) {
+  const int b0 = tot[0] + tot[1] + tot[2] + tot[3] + tot[4];
+  const int total = tot[5];
+  const int lane = threadIdx.x & 31;
+  int e = 0;
+  if (lane == 0) e = *((volatile int32_t*)err);
+  if (__shfl_sync(0xffffffffu, e, 0) & (kErrCapacity | kErrWalk)) return;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < total; k += nw) {
+    net_p2m<32>(list[b0 + k], lane, geom, theta, node_c, node_level, mx, ens);
+    __syncwarp();
+  }
+}
+
+// The twigs above kMidCount: one thread per climb start computes its twig
+// from the children, then climbs while it is the last child to arrive at the
+// parent (fence, atomic, fence: the children's records are visible to the
+// thread that completes the parent).
+__global__ void __launch_bounds__(128)
+    k_net_top(const Geom* __restrict__ geom, double theta, int cap, double4* node_c,
+              const int32_t* __restrict__ node_parent, int32_t* node_done,
+              const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
+              const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
+              int32_t* err) {
+  const int b0 = tot[0] + tot[1] + tot[2] + tot[3] + tot[4] + tot[5];
+  const int total = tot[6];
+  if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    int t = list[b0 + k];
+    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, __ldg(&mx.first[t])) : 0;
     const double smax0 = geom[seg].smax0;
-    for (int j = lane; j < nn; j += 32) pend[j] = 0;
-    if (lane == 0) s_tail[w] = 0;
-    __syncwarp();
-    // pending counts: every twig below the root registers with its parent
-    for (int j = lane + 1; j < nn; j += 32)
-      if (__ldg(&node_pt[r + j]) < 0) atomicAdd(&pend[__ldg(&node_parent[r + j]) - r], 1);
-    __syncwarp();
-    // the first round: twigs whose children are all leaves (in index order)
-    for (int j0 = 0; j0 < nn; j0 += 32) {
-      const int j = j0 + lane;
-      const bool ready = j < nn && __ldg(&node_pt[r + j]) < 0 && pend[j] == 0;
-      const unsigned bm = __ballot_sync(0xffffffffu, ready);
-      const int base = s_tail[w];
-      if (ready) queue[base + __popc(bm & ((1u << lane) - 1u))] = (int16_t)j;
-      __syncwarp();
-      if (lane == 0) s_tail[w] = base + __popc(bm);
-      __syncwarp();
-    }
-    // rounds: complete the ready twigs, release parents whose last child ends
-    bool ok = true;
-    int head = 0;
-    for (int guard = 0; ; ++guard) {
-      const int tail = s_tail[w];
-      if (head >= tail || guard > kSubNodes) break;
-      const int cnt = min(32, tail - head);
-      __syncwarp();
-      if (lane < cnt) {
-        const int j = queue[head + lane];
-        ok = net_twig(r + j, smax0, theta, cap, node_c, node_level, mx, err) && ok;
-        if (j > 0) {
-          const int pj = __ldg(&node_parent[r + j]) - r;
-          if (atomicSub(&pend[pj], 1) == 1) queue[atomicAdd(&s_tail[w], 1)] = (int16_t)pj;
-        } else if (ok) {
-          // the subtree root: climb through the twigs above
-          __threadfence();
-          int par = node_parent[r];
-          for (int g2 = 0; par >= 0; ++g2) {
-            if (g2 > kMaxLevel + 2) {
-              set_error(err, kErrWalk);
-              break;
-            }
-            if (atomicSub(&node_done[par], 1) != 1) break;
-            __threadfence();
-            if (!net_twig(par, smax0, theta, cap, node_c, node_level, mx, err)) break;
-            __threadfence();
-            par = node_parent[par];
-          }
-        }
+    for (int g = 0; t >= 0; ++g) {
+      if (g > kMaxLevel + 2) {
+        set_error(err, kErrWalk);
+        break;
       }
-      head += cnt;
-      __syncwarp();
+      if (!net_twig(t, smax0, theta, cap, node_c, node_level, mx, err)) break;
+      __threadfence();
+      t = node_parent[t];
+      if (t < 0 || atomicSub(&node_done[t], 1) != 1) break;
+      __threadfence();
     }
-    (void)ok;
-    __syncwarp();
   }
 }
 
-// The net-moment pass of the combined tree: leaves, marking of the small
-// subtrees, then the subtrees and the twigs above them.  Returns launches.
+// The net-charge moments of the combined tree (leaves, sort of the twigs
+// into classes, direct sums, climb).  Returns launches.
 int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double theta,
                 const Ensemble& ens, cudaStream_t st) {
-  const int T = 256;
+  const int T = kNetThreads;
   const int gb = (n + T - 1) / T;
   const int gcap = (b.cap + T - 1) / T;
+  int32_t* tot = b.mx.lvl;       // 7 class totals
+  int32_t* cur = b.mx.lvl + 8;   // 7 class cursors
   k_net_leaves<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.cap, b.node_c,
                                  b.mx, ens, b.err);
-  // lvl[0]: subtree roots listed, lvl[1]: their cursor
-  cudaMemsetAsync(b.mx.lvl, 0, 2 * sizeof(int32_t), st);
-  k_net_mark<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_parent, b.node_skip,
-                                 b.node_done, b.mx, b.mx.lvl_list, b.mx.lvl);
+  cudaMemsetAsync(b.mx.lvl, 0, 16 * sizeof(int32_t), st);
+  k_net_mark<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, tot);
+  k_net_fill<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, tot, cur,
+                                 b.mx.lvl_list);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int sgrid = (n + kSubCount - 1) / kSubCount;
-  if (sgrid > sms * kNetBlocksPerSm) sgrid = sms * kNetBlocksPerSm;
-  if (sgrid < 1) sgrid = 1;
-  k_net_subtrees<<<sgrid, 32 * kNetWarps, 0, st>>>(b.geom, theta, b.cap, b.node_c,
-                                                   b.node_skip, b.node_pt, b.node_parent,
-                                                   b.node_done, b.node_level, b.mx, ens,
-                                                   b.mx.lvl_list, b.mx.lvl, b.mx.lvl + 1,
-                                                   b.err);
-  return 3;
+  int g1 = (n / 2 + T - 1) / T;  // at most n - 1 twigs
+  if (g1 > sms * 8) g1 = sms * 8;
+  if (g1 < 1) g1 = 1;
+  k_net_p2m_thread<<<g1, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.mx, ens, tot,
+                                     b.mx.lvl_list, b.err);
+  int g2 = (n / kSmallCount * 32 + T - 1) / T;
+  if (g2 > sms * 8) g2 = sms * 8;
+  if (g2 < 1) g2 = 1;
+  k_net_p2m_warp<<<g2, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.mx, ens, tot,
+                                   b.mx.lvl_list, b.err);
+  k_net_top<<<sms, 128, 0, st>>>(b.geom, theta, b.cap, b.node_c, b.node_parent, b.node_done,
+                                 b.node_level, b.mx, ens, tot, b.mx.lvl_list, b.err);
+  return 6;
 }
 
 }  // namespace tg
