@@ -235,8 +235,10 @@ int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
                        int32_t* level, int64_t* skip, int64_t* pt,
                        int64_t* n_nodes);
 
-/* Debug: the combined tree of the mixed-precision path after the last build,
- * in pre-order (single-cloud handles of precision MIXED).  Per node:
+/* Debug: the combined tree of the mixed-precision path, rebuilt from the
+ * current device positions with every record written (the step's own builds
+ * write a twig's FP64 record only where the build reads it), in pre-order
+ * (single-cloud handles of precision MIXED).  Per node:
  * centre[3] (the expansion centre: a twig's centroid, a leaf's particle),
  * moments[38] (a twig's FP64 record: n, Q, Dx, Dy, Dz, q_ion, Sxx, Syy, Szz,
  * Sxy, Syz, Szx with S = 1/2 sum q a a^T, T[10] in the order xxx yyy zzz xxy

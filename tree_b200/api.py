@@ -368,7 +368,8 @@ class TreeForce:
                     skip=skip, pt=pt)
 
     def net_dump(self):
-        """The combined tree of the mixed path after the last build (pre-order):
+        """The combined tree of the mixed path, rebuilt from the current device
+        positions with every FP64 record written (pre-order):
         centre (m, 3), moments (m, 38) -- n, Q, D[3], q_ion, S[6] (xx yy zz xy
         yz zx), T[10], H[15], 0 -- first, count, level (m,), and the sorted
         particles (n, 4): x, y, z, 1 for ions."""

@@ -1055,7 +1055,7 @@ __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
 
 // ------------------------------------------------------------- driver ----
 int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
-                double theta, int mode, cudaStream_t st) {
+                double theta, int mode, cudaStream_t st, bool full_records) {
   // mode 0: one tree per species (parity path); mode 1: one combined tree
   const int split = mode == 0 ? n_el : n;
   const int T = 256;
@@ -1109,7 +1109,7 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
                                b.node_done, b.node_level, b.err);
     return launches + 1;
   }
-  launches += net_moments(b, x, n, n_el, theta, ens, st);
+  launches += net_moments(b, x, n, n_el, theta, ens, full_records, st);
   // the level lists of the upward pass are free again: a single cloud keeps
   // its group-level histogram there, an ensemble has one row per cloud
   const int nsg = ens.nseg > 0 ? ens.nseg : 1;

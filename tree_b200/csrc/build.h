@@ -107,11 +107,14 @@ int radix_sort(K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, int n,
 // Builds the trees for positions x (AoS, electrons first).  mode 0: one tree
 // per species with the reference's one-level moments (parity path); mode 1:
 // one combined tree with net-charge moments and target groups (mixed path).
+// full_records (mode 1): write every twig's FP64 moment record (m64), which
+// only the learned criterion's sampler and the debug dump read; otherwise only
+// the records that the build itself needs are written.
 int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
-                double theta, int mode, cudaStream_t st);
+                double theta, int mode, cudaStream_t st, bool full_records = false);
 // The net-charge moments of the combined tree (mode 1) once its topology and
 // child tables exist.
 int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double theta,
-                const Ensemble& ens, cudaStream_t st);
+                const Ensemble& ens, bool full_records, cudaStream_t st);
 
 }  // namespace tg

@@ -946,6 +946,22 @@ int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
   return TREE_GPU_OK;
 }
 
+// The combined tree of the current device positions with every twig's FP64
+// record written (the sampler's labels and the dump read them).
+static int build_full_records(tree_gpu_handle* h) {
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    h->timing.launches += tg::build_trees(h->b, h->x, h->n, (int)h->n_el,
+                                          h->prm.theta, 1, h->st, true);
+    bool grow = false;
+    int rc = check_device_status(h, &grow);
+    if (rc) return rc;
+    if (!grow) break;
+    if ((rc = grow_nodes(h))) return rc;
+    if (attempt == 2) return fail(h, TREE_GPU_ERR_CAPACITY, "capacity");
+  }
+  return TREE_GPU_OK;
+}
+
 int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* moments,
                       int64_t* first, int64_t* count, int32_t* level, double* sorted,
                       int64_t* n_nodes) {
@@ -954,6 +970,8 @@ int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* m
     return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: no combined-tree dump");
   if (h->prm.precision != TREE_GPU_PREC_MIXED)
     return fail(h, TREE_GPU_ERR_ARG, "the combined tree exists on the mixed path only");
+  if (h->n == 0) return fail(h, TREE_GPU_ERR_STATE, "no particles");
+  if (int rc = build_full_records(h)) return rc;
   int32_t bnd[4];
   CK(cudaMemcpy(bnd, h->b.bounds, sizeof(bnd), cudaMemcpyDeviceToHost));
   const int m = std::min(bnd[2], h->b.cap);
@@ -1281,17 +1299,8 @@ int tree_gpu_mac_collect(tree_gpu_handle* h, double theta_lo, double theta_hi,
     CK(cudaMemsetAsync(h->smp_count, 0, sizeof(int32_t) * 2, h->st));
     h->smp_cap = cap;
   }
-  // combined tree of the current device positions
-  for (int attempt = 0; attempt < 3; ++attempt) {
-    h->timing.launches += tg::build_trees(h->b, h->x, h->n, (int)h->n_el,
-                                          h->prm.theta, 1, h->st);
-    bool grow = false;
-    int rc = check_device_status(h, &grow);
-    if (rc) return rc;
-    if (!grow) break;
-    if ((rc = grow_nodes(h))) return rc;
-    if (attempt == 2) return fail(h, TREE_GPU_ERR_CAPACITY, "capacity");
-  }
+  // combined tree of the current device positions, every FP64 record written
+  if (int rc = build_full_records(h)) return rc;
   tg::SampleArgs a;
   a.node_c = h->b.node_c;
   a.mom = h->mb.mom;

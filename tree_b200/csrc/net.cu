@@ -81,6 +81,10 @@ __global__ void k_net_leaves(const double* __restrict__ x,
 }
 
 // ---- the records of one twig ----
+// The FP32 records and node_c are always written; the FP64 record m64 only
+// where it is read: by the parallel-axis pass (children of the large twigs,
+// and the large twigs themselves) and, on request, for every twig (the
+// learned criterion's training labels, the debug dump).
 // Count, centroid, net charge, ion count, dipole and second moment of twig
 // cur: node_c (centroid, critical radius smax / theta + |X - box centre|),
 // m64[0..5], mom and geom.  gc: the twig's geometric centre.
@@ -89,20 +93,22 @@ __device__ void net_store_low(int cur, double nsum, double X0, double X1, double
                               double Sxx, double Syy, double Szz, double Sxy, double Syz,
                               double Szx, double4 gc, double smax0, double theta,
                               const int8_t* __restrict__ node_level, double4* node_c,
-                              const MixedNodes& mx) {
+                              const MixedNodes& mx, bool rec64) {
   const double a0 = X0 - gc.x, a1 = X1 - gc.y, a2 = X2 - gc.z;
   const double dx = sqrt(a0 * a0 + a1 * a1 + a2 * a2);
   const int lev = node_level[cur];
   double smax = smax0;
   for (int l = 0; l < lev; ++l) smax = smax * 0.5;
   node_c[cur] = make_double4(X0, X1, X2, smax / theta + dx);
-  double2* m = mx.m64 + kM64 * (int64_t)cur;
-  m[0] = make_double2(nsum, Q);
-  m[1] = make_double2(Dx, Dy);
-  m[2] = make_double2(Dz, qi);
-  m[3] = make_double2(Sxx, Syy);
-  m[4] = make_double2(Szz, Sxy);
-  m[5] = make_double2(Syz, Szx);
+  if (rec64) {
+    double2* m = mx.m64 + kM64 * (int64_t)cur;
+    m[0] = make_double2(nsum, Q);
+    m[1] = make_double2(Dx, Dy);
+    m[2] = make_double2(Dz, qi);
+    m[3] = make_double2(Sxx, Syy);
+    m[4] = make_double2(Szz, Sxy);
+    m[5] = make_double2(Syz, Szx);
+  }
   const double trS = Sxx + Syy + Szz;
   const double Sxxt = Sxx - trS / 3.0, Syyt = Syy - trS / 3.0, Szzt = Szz - trS / 3.0;
   const double sn = sqrt(Sxxt * Sxxt + Syyt * Syyt + Szzt * Szzt +
@@ -116,10 +122,12 @@ __device__ void net_store_low(int cur, double nsum, double X0, double X1, double
 
 // Third moment T of twig cur (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz):
 // m64[6..10] and the trace-free mom3 with its Frobenius norm.
-__device__ void net_store_T(int cur, const double (&T)[10], const MixedNodes& mx) {
-  double2* m = mx.m64 + kM64 * (int64_t)cur;
+__device__ void net_store_T(int cur, const double (&T)[10], const MixedNodes& mx, bool rec64) {
+  if (rec64) {
+    double2* m = mx.m64 + kM64 * (int64_t)cur;
 #pragma unroll
-  for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+    for (int u = 0; u < 5; ++u) m[6 + u] = make_double2(T[2 * u], T[2 * u + 1]);
+  }
   const double Vx = T[0] + T[5] + T[7], Vy = T[3] + T[1] + T[8], Vz = T[4] + T[6] + T[2];
   double Tt[10];
   Tt[0] = T[0] - 0.6 * Vx;
@@ -145,11 +153,13 @@ __device__ void net_store_T(int cur, const double (&T)[10], const MixedNodes& mx
 // yzzz xxyy xxzz yyzz xxyz xyyz xyzz): m64[11..18] and the 12 components of
 // the trace-free H' = H - sym(delta C)/7 + sym(delta delta) tr C/35 with
 // C_kl = H_mmkl that the walk's hexadecapole reads.
-__device__ void net_store_H(int cur, const double (&H)[15], const MixedNodes& mx) {
-  double2* m = mx.m64 + kM64 * (int64_t)cur;
+__device__ void net_store_H(int cur, const double (&H)[15], const MixedNodes& mx, bool rec64) {
+  if (rec64) {
+    double2* m = mx.m64 + kM64 * (int64_t)cur;
 #pragma unroll
-  for (int u = 0; u < 7; ++u) m[11 + u] = make_double2(H[2 * u], H[2 * u + 1]);
-  m[18] = make_double2(H[14], 0.0);
+    for (int u = 0; u < 7; ++u) m[11 + u] = make_double2(H[2 * u], H[2 * u + 1]);
+    m[18] = make_double2(H[14], 0.0);
+  }
   const double Cxx = H[0] + H[9] + H[10], Cyy = H[9] + H[1] + H[11],
                Czz = H[10] + H[11] + H[2], Cxy = H[3] + H[5] + H[14],
                Cxz = H[4] + H[13] + H[7], Cyz = H[12] + H[6] + H[8];
@@ -189,7 +199,8 @@ __device__ __forceinline__ double group_sum(double v) {
 template <int G>
 __device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double theta,
                         double4* node_c, const int8_t* __restrict__ node_level,
-                        const MixedNodes& mx, const Ensemble& ens) {
+                        const int32_t* __restrict__ node_parent, const MixedNodes& mx,
+                        const Ensemble& ens, bool full) {
   int first = 0, cnt = 0;
   if (t >= 0) {
     first = __ldg(&mx.first[t]);
@@ -259,12 +270,17 @@ __device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double th
   Szx = 0.5 * group_sum<G>(Szx);
 #pragma unroll
   for (int u = 0; u < 10; ++u) T[u] = group_sum<G>(T[u]);
+  bool rec64 = full;
   if (t >= 0 && sub == 0) {
+    if (!rec64) {
+      const int par = __ldg(&node_parent[t]);
+      rec64 = par >= 0 && __ldg(&mx.count[par]) > kMidCount;
+    }
     const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, first) : 0;
     const double4 gc = ldg_d4(&node_c[t]);  // geometric centre (topology)
     net_store_low(t, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx, gc,
-                  geom[seg].smax0, theta, node_level, node_c, mx);
-    net_store_T(t, T, mx);
+                  geom[seg].smax0, theta, node_level, node_c, mx, rec64);
+    net_store_T(t, T, mx, rec64);
   }
   // pass 3: H about the centroid
   double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -291,7 +307,7 @@ __device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double th
   }
 #pragma unroll
   for (int u = 0; u < 15; ++u) H[u] = group_sum<G>(H[u]);
-  if (t >= 0 && sub == 0) net_store_H(t, H, mx);
+  if (t >= 0 && sub == 0) net_store_H(t, H, mx, rec64);
 }
 
 // ---- parallel-axis moments of the twigs above ----
@@ -380,7 +396,7 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
       Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
     }
     net_store_low(cur, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx, gc,
-                  smax0, theta, node_level, node_c, mx);
+                  smax0, theta, node_level, node_c, mx, true);
   }
   // pass 3: third moment
   {
@@ -414,7 +430,7 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     T[8] += Tc[8] + ey * S2zz + ez * S2yz + ez * S2yz + ey * ez * dcz + ey * dcz * ez + dcy * ez * ez + qc * ey * ez * ez;
     T[9] += Tc[9] + ex * S2yz + ey * S2xz + ez * S2xy + ex * ey * dcz + ex * dcy * ez + dcx * ey * ez + qc * ex * ey * ez;
     }
-    net_store_T(cur, T, mx);
+    net_store_T(cur, T, mx, true);
   }
   // pass 4: fourth moment
   {
@@ -455,7 +471,7 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     H[13] += Hc[13] + ex * Tyyz + 2.0 * ey * Txyz + ez * Txyy + 2.0 * ex * ey * S2yz + ex * ez * S2yy + ey * ey * S2xz + 2.0 * ey * ez * S2xy + ey * ey * ez * dcx + 2.0 * ex * ey * ez * dcy + ex * ey * ey * dcz + qc * ex * ey * ey * ez;
     H[14] += Hc[14] + ex * Tyzz + ey * Txzz + 2.0 * ez * Txyz + ex * ey * S2zz + 2.0 * ex * ez * S2yz + 2.0 * ey * ez * S2xz + ez * ez * S2xy + ey * ez * ez * dcx + ex * ez * ez * dcy + 2.0 * ex * ey * ez * dcz + qc * ex * ey * ez * ez;
     }
-    net_store_H(cur, H, mx);
+    net_store_H(cur, H, mx, true);
   }
   return true;
 }
@@ -497,7 +513,12 @@ __device__ __forceinline__ int net_class(int i, int cap, const int32_t* __restri
   return big == 0 ? 6 : -1;
 }
 
-// Pass 1 of the sort into classes: totals per class (tot[0..6]).
+// Pass 1 of the sort into classes: totals per class (tot[0..6]), counted in
+// shared memory per block of kNetNodesPerBlock nodes (one global atomic per
+// class and block).
+constexpr int kNetNodesPerThread = 4;
+constexpr int kNetNodesPerBlock = kNetThreads * kNetNodesPerThread;
+
 __global__ void __launch_bounds__(kNetThreads)
     k_net_mark(const int32_t* __restrict__ bounds, int cap,
                const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
@@ -506,10 +527,13 @@ __global__ void __launch_bounds__(kNetThreads)
   if (threadIdx.x < kNetClasses) h[threadIdx.x] = 0;
   __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m) {
-    const int k = net_class(i, cap, node_pt, mx, node_done, true);
-    if (k >= 0) atomicAdd(&h[k], 1);
+#pragma unroll
+  for (int u = 0; u < kNetNodesPerThread; ++u) {
+    const int i = blockIdx.x * kNetNodesPerBlock + u * kNetThreads + threadIdx.x;
+    if (i < m) {
+      const int k = net_class(i, cap, node_pt, mx, node_done, true);
+      if (k >= 0) atomicAdd(&h[k], 1);
+    }
   }
   __syncthreads();
   if (threadIdx.x < kNetClasses && h[threadIdx.x] > 0) atomicAdd(&tot[threadIdx.x], h[threadIdx.x]);
@@ -517,48 +541,56 @@ __global__ void __launch_bounds__(kNetThreads)
 
 // Pass 2: each twig appended to its class's range of the list (classes in
 // index order; order inside a class is arbitrary -- the arithmetic per twig
-// is not).  cur[0..6]: per-class cursors.
+// is not).  Slots are taken in shared memory per block, then one global
+// atomic per class and block on cur[0..6] places the block's run.
 __global__ void __launch_bounds__(kNetThreads)
     k_net_fill(const int32_t* __restrict__ bounds, int cap,
                const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
                const int32_t* __restrict__ tot, int32_t* cur, int32_t* list) {
+  __shared__ int32_t s_cnt[kNetClasses], s_base[kNetClasses];
+  if (threadIdx.x < kNetClasses) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = i < m ? net_class(i, cap, node_pt, mx, node_done, false) : -1;
-  const int lane = threadIdx.x & 31;
-  int base = 0;
+  int idx[kNetNodesPerThread], cls[kNetNodesPerThread], slot[kNetNodesPerThread];
 #pragma unroll
-  for (int c = 0; c < kNetClasses; ++c) {
-    const unsigned bm = __ballot_sync(0xffffffffu, k == c);
-    if (bm != 0) {
-      const int leader = __ffs(bm) - 1;
-      int off = 0;
-      if (lane == leader) off = atomicAdd(&cur[c], __popc(bm));
-      off = __shfl_sync(0xffffffffu, off, leader);
-      if (k == c) list[base + off + __popc(bm & ((1u << lane) - 1u))] = i;
-    }
-    base += tot[c];
+  for (int u = 0; u < kNetNodesPerThread; ++u) {
+    idx[u] = blockIdx.x * kNetNodesPerBlock + u * kNetThreads + threadIdx.x;
+    cls[u] = idx[u] < m ? net_class(idx[u], cap, node_pt, mx, node_done, false) : -1;
+    slot[u] = cls[u] >= 0 ? atomicAdd(&s_cnt[cls[u]], 1) : 0;
   }
+  __syncthreads();
+  if (threadIdx.x < kNetClasses) {
+    const int c = threadIdx.x;
+    int b = 0;
+    for (int cc = 0; cc < c; ++cc) b += tot[cc];
+    s_base[c] = b + (s_cnt[c] > 0 ? atomicAdd(&cur[c], s_cnt[c]) : 0);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < kNetNodesPerThread; ++u)
+    if (cls[u] >= 0) list[s_base[cls[u]] + slot[u]] = idx[u];
 }
 
 // One thread per twig of classes 0..4 (list[0 .. tot[0] + ... + tot[4])).
 __global__ void __launch_bounds__(kNetThreads)
     k_net_p2m_thread(const Geom* __restrict__ geom, double theta, double4* node_c,
-                     const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
+                     const int8_t* __restrict__ node_level,
+                     const int32_t* __restrict__ node_parent, MixedNodes mx, Ensemble ens,
                      const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
-                     int32_t* err) {
+                     int full, int32_t* err) {
   const int total = tot[0] + tot[1] + tot[2] + tot[3] + tot[4];
   if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
-    net_p2m<1>(list[k], 0, geom, theta, node_c, node_level, mx, ens);
+    net_p2m<1>(list[k], 0, geom, theta, node_c, node_level, node_parent, mx, ens, full != 0);
 }
 
 // One warp per twig of class 5.
 __global__ void __launch_bounds__(kNetThreads)
     k_net_p2m_warp(const Geom* __restrict__ geom, double theta, double4* node_c,
-                   const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
+                   const int8_t* __restrict__ node_level,
+                   const int32_t* __restrict__ node_parent, MixedNodes mx, Ensemble ens,
                    const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
-                   int32_t* err) {
+                   int full, int32_t* err) {
   const int b0 = tot[0] + tot[1] + tot[2] + tot[3] + tot[4];
   const int total = tot[5];
   const int lane = threadIdx.x & 31;
@@ -567,7 +599,8 @@ __global__ void __launch_bounds__(kNetThreads)
   if (__shfl_sync(0xffffffffu, e, 0) & (kErrCapacity | kErrWalk)) return;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < total; k += nw) {
-    net_p2m<32>(list[b0 + k], lane, geom, theta, node_c, node_level, mx, ens);
+    net_p2m<32>(list[b0 + k], lane, geom, theta, node_c, node_level, node_parent, mx, ens,
+                full != 0);
     __syncwarp();
   }
 }
@@ -606,10 +639,10 @@ __global__ void __launch_bounds__(128)
 // The net-charge moments of the combined tree (leaves, sort of the twigs
 // into classes, direct sums, climb).  Returns launches.
 int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double theta,
-                const Ensemble& ens, cudaStream_t st) {
+                const Ensemble& ens, bool full, cudaStream_t st) {
   const int T = kNetThreads;
   const int gb = (n + T - 1) / T;
-  const int gcap = (b.cap + T - 1) / T;
+  const int gcap = (b.cap + kNetNodesPerBlock - 1) / kNetNodesPerBlock;
   int32_t* tot = b.mx.lvl;       // 7 class totals
   int32_t* cur = b.mx.lvl + 8;   // 7 class cursors
   k_net_leaves<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.cap, b.node_c,
@@ -624,13 +657,13 @@ int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double 
   int g1 = (n / 2 + T - 1) / T;  // at most n - 1 twigs
   if (g1 > sms * 8) g1 = sms * 8;
   if (g1 < 1) g1 = 1;
-  k_net_p2m_thread<<<g1, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.mx, ens, tot,
-                                     b.mx.lvl_list, b.err);
+  k_net_p2m_thread<<<g1, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.node_parent,
+                                     b.mx, ens, tot, b.mx.lvl_list, full ? 1 : 0, b.err);
   int g2 = (n / kSmallCount * 32 + T - 1) / T;
   if (g2 > sms * 8) g2 = sms * 8;
   if (g2 < 1) g2 = 1;
-  k_net_p2m_warp<<<g2, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.mx, ens, tot,
-                                   b.mx.lvl_list, b.err);
+  k_net_p2m_warp<<<g2, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.node_parent,
+                                   b.mx, ens, tot, b.mx.lvl_list, full ? 1 : 0, b.err);
   k_net_top<<<sms, 128, 0, st>>>(b.geom, theta, b.cap, b.node_c, b.node_parent, b.node_done,
                                  b.node_level, b.mx, ens, tot, b.mx.lvl_list, b.err);
   return 6;
