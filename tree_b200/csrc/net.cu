@@ -51,7 +51,7 @@ __constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
 // sums them as particles and the parallel-axis pass treats them as point
 // charges.
 constexpr int kMidCount = 2048;   // twigs up to this size: direct sums (P2M)
-constexpr int kSmallCount = 64;   // twigs up to this size: 8 lanes each, else a warp
+constexpr int kSmallCount = 64;   // twigs up to this size: a thread each, else a warp
 
 // Leaves of the combined tree (one per sorted particle): the position with
 // w = -1 (the walk's leaf mark), and the sorted positions the walk and the
@@ -184,18 +184,30 @@ __device__ void net_store_H(int cur, const double (&H)[15], const MixedNodes& mx
 // Sum over the G lanes of an aligned lane group (butterfly: every lane of the
 // group ends with the same total, added in the same order).
 template <int G>
-__device__ __forceinline__ double group_sum(double v) {
+__device__ __forceinline__ double group_sum(double v, unsigned mask = 0xffffffffu) {
 #pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
   return v;
 }
 
+// One sorted particle relative to the centroid: a = x - X, q = +1 ion / -1
+// electron, w = 1 ion / 0 electron.
+struct P2mPt {
+  double ax, ay, az, q, w;
+};
+__device__ __forceinline__ P2mPt p2m_pt(const double4* __restrict__ xs, int j, double X0,
+                                        double X1, double X2) {
+  const double4 p = ldg_d4(&xs[j]);
+  return {p.x - X0, p.y - X1, p.z - X2, p.w > 0.5 ? 1.0 : -1.0, p.w};
+}
+
 // Moments of twig t straight from its particles (the sorted range first ..
-// first + count - 1 of xs): the centroid, then Q, q_ion, D, S and T about it,
-// then H.  G lanes share the twig: lane `sub` takes every G-th particle and
-// the group adds the lanes' sums after each pass; lane 0 of the group stores.
-// Every lane of the warp calls this together (t < 0: a group without a twig,
-// which still takes part in the shuffles).
+// first + count - 1 of xs), one pass per moment order so that few
+// accumulators are live: the centroid; Q, q_ion, D and S about it; T; H.
+// G lanes share the twig: lane `sub` takes every G-th particle and the group
+// adds the lanes' sums after each pass; lane 0 of the group stores.  Every
+// lane of the warp calls this together (t < 0: a group without a twig, which
+// still takes part in the shuffles).
 template <int G>
 __device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double theta,
                         double4* node_c, const int8_t* __restrict__ node_level,
@@ -207,6 +219,7 @@ __device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double th
     cnt = __ldg(&mx.count[t]);
   }
   const double4* __restrict__ xs = mx.xs + first;
+  const bool store = t >= 0 && sub == 0;
   // pass 1: centroid
   double X0 = 0.0, X1 = 0.0, X2 = 0.0;
   for (int j = sub; j < cnt; j += G) {
@@ -224,90 +237,96 @@ __device__ void net_p2m(int t, int sub, const Geom* __restrict__ geom, double th
     X1 /= nsum;
     X2 /= nsum;
   }
-  // pass 2: Q, q_ion, D, 2 S and T about the centroid
-  double Q = 0, qi = 0, Dx = 0, Dy = 0, Dz = 0;
-  double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
-  double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int j = sub; j < cnt; j += G) {
-    const double4 p = ldg_d4(&xs[j]);
-    const double q = p.w > 0.5 ? 1.0 : -1.0;
-    const double ax = p.x - X0, ay = p.y - X1, az = p.z - X2;
-    const double qx = q * ax, qy = q * ay, qz = q * az;
-    const double qxx = qx * ax, qyy = qy * ay, qzz = qz * az;
-    const double qxy = qx * ay, qyz = qy * az, qzx = qz * ax;
-    Q += q;
-    qi += p.w;
-    Dx += qx;
-    Dy += qy;
-    Dz += qz;
-    Sxx += qxx;
-    Syy += qyy;
-    Szz += qzz;
-    Sxy += qxy;
-    Syz += qyz;
-    Szx += qzx;
-    T[0] += qxx * ax;  // xxx
-    T[1] += qyy * ay;  // yyy
-    T[2] += qzz * az;  // zzz
-    T[3] += qxx * ay;  // xxy
-    T[4] += qxx * az;  // xxz
-    T[5] += qyy * ax;  // xyy
-    T[6] += qyy * az;  // yyz
-    T[7] += qzz * ax;  // xzz
-    T[8] += qzz * ay;  // yzz
-    T[9] += qxy * az;  // xyz
-  }
-  Q = group_sum<G>(Q);
-  qi = group_sum<G>(qi);
-  Dx = group_sum<G>(Dx);
-  Dy = group_sum<G>(Dy);
-  Dz = group_sum<G>(Dz);
-  Sxx = 0.5 * group_sum<G>(Sxx);
-  Syy = 0.5 * group_sum<G>(Syy);
-  Szz = 0.5 * group_sum<G>(Szz);
-  Sxy = 0.5 * group_sum<G>(Sxy);
-  Syz = 0.5 * group_sum<G>(Syz);
-  Szx = 0.5 * group_sum<G>(Szx);
-#pragma unroll
-  for (int u = 0; u < 10; ++u) T[u] = group_sum<G>(T[u]);
   bool rec64 = full;
-  if (t >= 0 && sub == 0) {
-    if (!rec64) {
-      const int par = __ldg(&node_parent[t]);
-      rec64 = par >= 0 && __ldg(&mx.count[par]) > kMidCount;
+  if (store && !rec64) {
+    const int par = __ldg(&node_parent[t]);
+    rec64 = par >= 0 && __ldg(&mx.count[par]) > kMidCount;
+  }
+  // pass 2: Q, q_ion, D and S = 1/2 sum q a a^T
+  {
+    double Q = 0, qi = 0, Dx = 0, Dy = 0, Dz = 0;
+    double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
+    for (int j = sub; j < cnt; j += G) {
+      const P2mPt a = p2m_pt(xs, j, X0, X1, X2);
+      const double qx = a.q * a.ax, qy = a.q * a.ay, qz = a.q * a.az;
+      Q += a.q;
+      qi += a.w;
+      Dx += qx;
+      Dy += qy;
+      Dz += qz;
+      Sxx += qx * a.ax;
+      Syy += qy * a.ay;
+      Szz += qz * a.az;
+      Sxy += qx * a.ay;
+      Syz += qy * a.az;
+      Szx += qz * a.ax;
     }
-    const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, first) : 0;
-    const double4 gc = ldg_d4(&node_c[t]);  // geometric centre (topology)
-    net_store_low(t, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx, gc,
-                  geom[seg].smax0, theta, node_level, node_c, mx, rec64);
-    net_store_T(t, T, mx, rec64);
+    Q = group_sum<G>(Q);
+    qi = group_sum<G>(qi);
+    Dx = group_sum<G>(Dx);
+    Dy = group_sum<G>(Dy);
+    Dz = group_sum<G>(Dz);
+    Sxx = 0.5 * group_sum<G>(Sxx);
+    Syy = 0.5 * group_sum<G>(Syy);
+    Szz = 0.5 * group_sum<G>(Szz);
+    Sxy = 0.5 * group_sum<G>(Sxy);
+    Syz = 0.5 * group_sum<G>(Syz);
+    Szx = 0.5 * group_sum<G>(Szx);
+    if (store) {
+      const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, first) : 0;
+      const double4 gc = ldg_d4(&node_c[t]);  // geometric centre (topology)
+      net_store_low(t, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx,
+                    gc, geom[seg].smax0, theta, node_level, node_c, mx, rec64);
+    }
   }
-  // pass 3: H about the centroid
-  double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int j = sub; j < cnt; j += G) {
-    const double4 p = ldg_d4(&xs[j]);
-    const double q = p.w > 0.5 ? 1.0 : -1.0;
-    const double ax = p.x - X0, ay = p.y - X1, az = p.z - X2;
-    const double qxx = q * ax * ax, qyy = q * ay * ay, qzz = q * az * az;
-    H[0] += qxx * ax * ax;   // xxxx
-    H[1] += qyy * ay * ay;   // yyyy
-    H[2] += qzz * az * az;   // zzzz
-    H[3] += qxx * ax * ay;   // xxxy
-    H[4] += qxx * ax * az;   // xxxz
-    H[5] += qyy * ay * ax;   // xyyy
-    H[6] += qyy * ay * az;   // yyyz
-    H[7] += qzz * az * ax;   // xzzz
-    H[8] += qzz * az * ay;   // yzzz
-    H[9] += qxx * ay * ay;   // xxyy
-    H[10] += qxx * az * az;  // xxzz
-    H[11] += qyy * az * az;  // yyzz
-    H[12] += qxx * ay * az;  // xxyz
-    H[13] += qyy * ax * az;  // xyyz
-    H[14] += qzz * ax * ay;  // xyzz
-  }
+  // pass 3: T (order xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz)
+  {
+    double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = sub; j < cnt; j += G) {
+      const P2mPt a = p2m_pt(xs, j, X0, X1, X2);
+      const double qxx = a.q * a.ax * a.ax, qyy = a.q * a.ay * a.ay, qzz = a.q * a.az * a.az;
+      T[0] += qxx * a.ax;
+      T[1] += qyy * a.ay;
+      T[2] += qzz * a.az;
+      T[3] += qxx * a.ay;
+      T[4] += qxx * a.az;
+      T[5] += qyy * a.ax;
+      T[6] += qyy * a.az;
+      T[7] += qzz * a.ax;
+      T[8] += qzz * a.ay;
+      T[9] += a.q * a.ax * a.ay * a.az;
+    }
 #pragma unroll
-  for (int u = 0; u < 15; ++u) H[u] = group_sum<G>(H[u]);
-  if (t >= 0 && sub == 0) net_store_H(t, H, mx, rec64);
+    for (int u = 0; u < 10; ++u) T[u] = group_sum<G>(T[u]);
+    if (store) net_store_T(t, T, mx, rec64);
+  }
+  // pass 4: H (order xxxx yyyy zzzz xxxy xxxz xyyy yyyz xzzz yzzz xxyy xxzz
+  // yyzz xxyz xyyz xyzz)
+  {
+    double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = sub; j < cnt; j += G) {
+      const P2mPt a = p2m_pt(xs, j, X0, X1, X2);
+      const double qxx = a.q * a.ax * a.ax, qyy = a.q * a.ay * a.ay, qzz = a.q * a.az * a.az;
+      H[0] += qxx * a.ax * a.ax;
+      H[1] += qyy * a.ay * a.ay;
+      H[2] += qzz * a.az * a.az;
+      H[3] += qxx * a.ax * a.ay;
+      H[4] += qxx * a.ax * a.az;
+      H[5] += qyy * a.ay * a.ax;
+      H[6] += qyy * a.ay * a.az;
+      H[7] += qzz * a.az * a.ax;
+      H[8] += qzz * a.az * a.ay;
+      H[9] += qxx * a.ay * a.ay;
+      H[10] += qxx * a.az * a.az;
+      H[11] += qyy * a.az * a.az;
+      H[12] += qxx * a.ay * a.az;
+      H[13] += qyy * a.ax * a.az;
+      H[14] += qzz * a.ax * a.ay;
+    }
+#pragma unroll
+    for (int u = 0; u < 15; ++u) H[u] = group_sum<G>(H[u]);
+    if (store) net_store_H(t, H, mx, rec64);
+  }
 }
 
 // ---- parallel-axis moments of the twigs above ----
@@ -329,96 +348,63 @@ __device__ __forceinline__ void child_rec(int c, bool leaf, const MixedNodes& mx
   }
 }
 
-// Net moments of twig `cur` from its children (all final): centroid, then
-// Q, D, S, T and H about it by the parallel-axis rules, each summed over the
-// children in pre-order (ascending octant digit, the order of the child
-// table).  One pass over the children per moment order keeps few
-// accumulators live at a time (the children's records are re-read from
-// L1/L2); the child indices come from one read of the child table, so the
-// loads of all children are independent.
-__device__ bool net_twig(int cur, double smax0, double theta, int cap,
-                         double4* node_c, const int8_t* __restrict__ node_level,
-                         const MixedNodes& mx, int32_t* err) {
+// Net moments of twig `cur` from its children (all final) by the 8 lanes of
+// an aligned lane group (mask gm), lane j taking the child of octant digit j:
+// the centroid, then each child's Q, D, S, T and H translated to it by the
+// parallel-axis rules and summed over the group (butterfly); lane 0 stores.
+// All 8 lanes call this together.
+__device__ bool net_twig8(int cur, int j, unsigned gm, double smax0, double theta, int cap,
+                          double4* node_c, const int8_t* __restrict__ node_level,
+                          const MixedNodes& mx, int32_t* err) {
   const double4 gc = ldcg_d4(&node_c[cur]);  // geometric centre (topology)
-  int kid[8];
-  {
-    const int4* kk = reinterpret_cast<const int4*>(mx.kids + 8 * (int64_t)cur);
-    const int4 k0 = __ldg(kk), k1 = __ldg(kk + 1);
-    kid[0] = k0.x; kid[1] = k0.y; kid[2] = k0.z; kid[3] = k0.w;
-    kid[4] = k1.x; kid[5] = k1.y; kid[6] = k1.z; kid[7] = k1.w;
+  const int c = __ldg(&mx.kids[8 * (int64_t)cur + j]);
+  if (__any_sync(gm, c >= cap || (c >= 0 && c <= cur))) {
+    if (j == 0) set_error(err, kErrWalk);
+    return false;
   }
+  double4 cc = make_double4(0.0, 0.0, 0.0, 0.0);
+  double2 r[19];
 #pragma unroll
-  for (int j = 0; j < 8; ++j)
-    if (kid[j] >= cap || (kid[j] >= 0 && kid[j] <= cur)) {
-      set_error(err, kErrWalk);
-      return false;
+  for (int u = 0; u < 19; ++u) r[u] = make_double2(0.0, 0.0);
+  if (c >= 0) {
+    cc = ldcg_d4(&node_c[c]);
+    child_rec<19>(c, cc.w < 0.0, mx, r);
+  }
+  // centroid: count-weighted child centroids
+  const double nc = r[0].x;
+  const double nsum = group_sum<8>(nc, gm);
+  const double X0 = group_sum<8>(nc * cc.x, gm) / nsum;
+  const double X1 = group_sum<8>(nc * cc.y, gm) / nsum;
+  const double X2 = group_sum<8>(nc * cc.z, gm) / nsum;
+  // this lane's child about the centroid (all zero for an empty octant)
+  const double qc = r[0].y, dcx = r[1].x, dcy = r[1].y, dcz = r[2].x;
+  const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
+  {
+    const double Q = group_sum<8>(qc, gm), qi = group_sum<8>(r[2].y, gm);
+    const double Dx = group_sum<8>(dcx + qc * ex, gm);
+    const double Dy = group_sum<8>(dcy + qc * ey, gm);
+    const double Dz = group_sum<8>(dcz + qc * ez, gm);
+    const double Sxx = group_sum<8>(r[3].x + dcx * ex + 0.5 * qc * ex * ex, gm);
+    const double Syy = group_sum<8>(r[3].y + dcy * ey + 0.5 * qc * ey * ey, gm);
+    const double Szz = group_sum<8>(r[4].x + dcz * ez + 0.5 * qc * ez * ez, gm);
+    const double Sxy = group_sum<8>(r[4].y + 0.5 * (dcx * ey + ex * dcy) + 0.5 * qc * ex * ey, gm);
+    const double Syz = group_sum<8>(r[5].x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez, gm);
+    const double Szx = group_sum<8>(r[5].y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex, gm);
+    if (j == 0)
+      net_store_low(cur, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx,
+                    gc, smax0, theta, node_level, node_c, mx, true);
+  }
+  const double S2xx = 2 * r[3].x, S2yy = 2 * r[3].y, S2zz = 2 * r[4].x, S2xy = 2 * r[4].y,
+               S2yz = 2 * r[5].x, S2xz = 2 * r[5].y;
+  {
+    double Tc[10], T[10];
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+      Tc[2 * u] = r[6 + u].x;
+      Tc[2 * u + 1] = r[6 + u].y;
     }
-  // pass 1: count and centroid
-  double nsum = 0.0, X0 = 0.0, X1 = 0.0, X2 = 0.0;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int c = kid[j];
-    if (c < 0) continue;
-    const double4 cc = ldcg_d4(&node_c[c]);
-    const double nc = cc.w < 0.0 ? 1.0 : __ldcg(mx.m64 + kM64 * (int64_t)c).x;
-    nsum += nc;
-    X0 += nc * cc.x;
-    X1 += nc * cc.y;
-    X2 += nc * cc.z;
-  }
-  X0 /= nsum;
-  X1 /= nsum;
-  X2 /= nsum;
-  // pass 2: net charge, dipole and second moment about the centroid
-  {
-    double Q = 0, Dx = 0, Dy = 0, Dz = 0, qi = 0;
-    double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Syz = 0, Szx = 0;
-#pragma unroll 1
-    for (int j = 0; j < 8; ++j) {
-      const int c = kid[j];
-      if (c < 0) continue;
-      const double4 cc = ldcg_d4(&node_c[c]);
-      double2 r[6];
-      child_rec<6>(c, cc.w < 0.0, mx, r);
-      const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3], a4 = r[4], a5 = r[5];
-      const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
-      const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
-      Q += qc;
-      qi += a2.y;
-      Dx += dcx + qc * ex;
-      Dy += dcy + qc * ey;
-      Dz += dcz + qc * ez;
-      Sxx += a3.x + dcx * ex + 0.5 * qc * ex * ex;
-      Syy += a3.y + dcy * ey + 0.5 * qc * ey * ey;
-      Szz += a4.x + dcz * ez + 0.5 * qc * ez * ez;
-      Sxy += a4.y + 0.5 * (dcx * ey + ex * dcy) + 0.5 * qc * ex * ey;
-      Syz += a5.x + 0.5 * (dcy * ez + ey * dcz) + 0.5 * qc * ey * ez;
-      Szx += a5.y + 0.5 * (dcz * ex + ez * dcx) + 0.5 * qc * ez * ex;
-    }
-    net_store_low(cur, nsum, X0, X1, X2, Q, qi, Dx, Dy, Dz, Sxx, Syy, Szz, Sxy, Syz, Szx, gc,
-                  smax0, theta, node_level, node_c, mx, true);
-  }
-  // pass 3: third moment
-  {
-    double T[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-    for (int j = 0; j < 8; ++j) {
-      const int c = kid[j];
-      if (c < 0) continue;
-      const double4 cc = ldcg_d4(&node_c[c]);
-      double2 r[11];
-      child_rec<11>(c, cc.w < 0.0, mx, r);
-      const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3], a4 = r[4], a5 = r[5];
-      const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
-      const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
-      const double S2xx = 2 * a3.x, S2yy = 2 * a3.y, S2zz = 2 * a4.x, S2xy = 2 * a4.y,
-                   S2yz = 2 * a5.x, S2xz = 2 * a5.y;
-      double Tc[10];
-#pragma unroll
-      for (int u = 0; u < 5; ++u) {
-        Tc[2 * u] = r[6 + u].x;
-        Tc[2 * u + 1] = r[6 + u].y;
-      }
+    for (int u = 0; u < 10; ++u) T[u] = 0.0;
     T[0] += Tc[0] + ex * S2xx + ex * S2xx + ex * S2xx + ex * ex * dcx + ex * dcx * ex + dcx * ex * ex + qc * ex * ex * ex;
     T[1] += Tc[1] + ey * S2yy + ey * S2yy + ey * S2yy + ey * ey * dcy + ey * dcy * ey + dcy * ey * ey + qc * ey * ey * ey;
     T[2] += Tc[2] + ez * S2zz + ez * S2zz + ez * S2zz + ez * ez * dcz + ez * dcz * ez + dcz * ez * ez + qc * ez * ez * ez;
@@ -429,32 +415,21 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     T[7] += Tc[7] + ex * S2zz + ez * S2xz + ez * S2xz + ex * ez * dcz + ex * dcz * ez + dcx * ez * ez + qc * ex * ez * ez;
     T[8] += Tc[8] + ey * S2zz + ez * S2yz + ez * S2yz + ey * ez * dcz + ey * dcz * ez + dcy * ez * ez + qc * ey * ez * ez;
     T[9] += Tc[9] + ex * S2yz + ey * S2xz + ez * S2xy + ex * ey * dcz + ex * dcy * ez + dcx * ey * ez + qc * ex * ey * ez;
-    }
-    net_store_T(cur, T, mx, true);
-  }
-  // pass 4: fourth moment
-  {
-    double H[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-    for (int j = 0; j < 8; ++j) {
-      const int c = kid[j];
-      if (c < 0) continue;
-      const double4 cc = ldcg_d4(&node_c[c]);
-      double2 r[19];
-      child_rec<19>(c, cc.w < 0.0, mx, r);
-      const double2 a0 = r[0], a1 = r[1], a2 = r[2], a3 = r[3], a4 = r[4], a5 = r[5];
-      const double qc = a0.y, dcx = a1.x, dcy = a1.y, dcz = a2.x;
-      const double ex = cc.x - X0, ey = cc.y - X1, ez = cc.z - X2;
-      const double S2xx = 2 * a3.x, S2yy = 2 * a3.y, S2zz = 2 * a4.x, S2xy = 2 * a4.y,
-                   S2yz = 2 * a5.x, S2xz = 2 * a5.y;
-      const double Txxx = r[6].x, Tyyy = r[6].y, Tzzz = r[7].x, Txxy = r[7].y, Txxz = r[8].x,
-                   Txyy = r[8].y, Tyyz = r[9].x, Txzz = r[9].y, Tyzz = r[10].x, Txyz = r[10].y;
-      double Hc[16];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        Hc[2 * u] = r[11 + u].x;
-        Hc[2 * u + 1] = r[11 + u].y;
-      }
+    for (int u = 0; u < 10; ++u) T[u] = group_sum<8>(T[u], gm);
+    if (j == 0) net_store_T(cur, T, mx, true);
+  }
+  {
+    const double Txxx = r[6].x, Tyyy = r[6].y, Tzzz = r[7].x, Txxy = r[7].y, Txxz = r[8].x,
+                 Txyy = r[8].y, Tyyz = r[9].x, Txzz = r[9].y, Tyzz = r[10].x, Txyz = r[10].y;
+    double Hc[16], H[15];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      Hc[2 * u] = r[11 + u].x;
+      Hc[2 * u + 1] = r[11 + u].y;
+    }
+#pragma unroll
+    for (int u = 0; u < 15; ++u) H[u] = 0.0;
     H[0] += Hc[0] + 4.0 * ex * Txxx + 6.0 * ex * ex * S2xx + 4.0 * ex * ex * ex * dcx + qc * ex * ex * ex * ex;
     H[1] += Hc[1] + 4.0 * ey * Tyyy + 6.0 * ey * ey * S2yy + 4.0 * ey * ey * ey * dcy + qc * ey * ey * ey * ey;
     H[2] += Hc[2] + 4.0 * ez * Tzzz + 6.0 * ez * ez * S2zz + 4.0 * ez * ez * ez * dcz + qc * ez * ez * ez * ez;
@@ -470,8 +445,9 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
     H[12] += Hc[12] + 2.0 * ex * Txyz + ey * Txxz + ez * Txxy + ex * ex * S2yz + 2.0 * ex * ey * S2xz + 2.0 * ex * ez * S2xy + ey * ez * S2xx + 2.0 * ex * ey * ez * dcx + ex * ex * ez * dcy + ex * ex * ey * dcz + qc * ex * ex * ey * ez;
     H[13] += Hc[13] + ex * Tyyz + 2.0 * ey * Txyz + ez * Txyy + 2.0 * ex * ey * S2yz + ex * ez * S2yy + ey * ey * S2xz + 2.0 * ey * ez * S2xy + ey * ey * ez * dcx + 2.0 * ex * ey * ez * dcy + ex * ey * ey * dcz + qc * ex * ey * ey * ez;
     H[14] += Hc[14] + ex * Tyzz + ey * Txzz + 2.0 * ez * Txyz + ex * ey * S2zz + 2.0 * ex * ez * S2yz + 2.0 * ey * ez * S2xz + ez * ez * S2xy + ey * ez * ez * dcx + ex * ez * ez * dcy + 2.0 * ex * ey * ez * dcz + qc * ex * ey * ez * ez;
-    }
-    net_store_H(cur, H, mx, true);
+#pragma unroll
+    for (int u = 0; u < 15; ++u) H[u] = group_sum<8>(H[u], gm);
+    if (j == 0) net_store_H(cur, H, mx, true);
   }
   return true;
 }
@@ -482,9 +458,16 @@ __device__ bool net_twig(int cur, double smax0, double theta, int cap,
 // about as many iterations), 65 .. kMidCount (a warp each), and the twigs
 // above kMidCount whose twig children are all below it (where the
 // parallel-axis climb starts).  The other twigs above kMidCount count the
-// children of their own kind that they wait for in node_done.
+// children of their own kind that they wait for in node_done.  The sort is a
+// counting sort over blocks of kNetBlockNodes nodes: per-block class counts
+// (class-major), their exclusive scan, then each block writes its twigs of
+// each class in index order at its offset -- the list holds the classes in
+// order and every class in node order.
 constexpr int kNetClasses = 7;  // class index: 0..4 one thread, 5 a warp, 6 climb start
 constexpr int kNetThreads = 256;
+constexpr int kNetNodesPerThread = 4;
+constexpr int kNetBlockNodes = kNetThreads * kNetNodesPerThread;
+static_assert(kNetBlockNodes == 1024, "net_cls_entries assumes blocks of 1024 nodes");
 
 __device__ __forceinline__ int net_class_of(int c) {
   if (c > kMidCount) return 6;
@@ -513,125 +496,134 @@ __device__ __forceinline__ int net_class(int i, int cap, const int32_t* __restri
   return big == 0 ? 6 : -1;
 }
 
-// Pass 1 of the sort into classes: totals per class (tot[0..6]), counted in
-// shared memory per block of kNetNodesPerBlock nodes (one global atomic per
-// class and block).
-constexpr int kNetNodesPerThread = 4;
-constexpr int kNetNodesPerBlock = kNetThreads * kNetNodesPerThread;
-
+// Pass 1 of the sort: class counts of block b's nodes in cnt[class * nb + b].
 __global__ void __launch_bounds__(kNetThreads)
     k_net_mark(const int32_t* __restrict__ bounds, int cap,
                const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
-               int32_t* tot) {
+               int32_t* cnt) {
   __shared__ int32_t h[kNetClasses];
   if (threadIdx.x < kNetClasses) h[threadIdx.x] = 0;
   __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
 #pragma unroll
   for (int u = 0; u < kNetNodesPerThread; ++u) {
-    const int i = blockIdx.x * kNetNodesPerBlock + u * kNetThreads + threadIdx.x;
+    const int i = blockIdx.x * kNetBlockNodes + u * kNetThreads + threadIdx.x;
     if (i < m) {
       const int k = net_class(i, cap, node_pt, mx, node_done, true);
       if (k >= 0) atomicAdd(&h[k], 1);
     }
   }
   __syncthreads();
-  if (threadIdx.x < kNetClasses && h[threadIdx.x] > 0) atomicAdd(&tot[threadIdx.x], h[threadIdx.x]);
+  if (threadIdx.x < kNetClasses) cnt[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
 }
 
-// Pass 2: each twig appended to its class's range of the list (classes in
-// index order; order inside a class is arbitrary -- the arithmetic per twig
-// is not).  Slots are taken in shared memory per block, then one global
-// atomic per class and block on cur[0..6] places the block's run.
+// Pass 2: block b's twigs of class c written in index order from off[c * nb
+// + b] (the exclusive scan of the counts).
 __global__ void __launch_bounds__(kNetThreads)
     k_net_fill(const int32_t* __restrict__ bounds, int cap,
                const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
-               const int32_t* __restrict__ tot, int32_t* cur, int32_t* list) {
-  __shared__ int32_t s_cnt[kNetClasses], s_base[kNetClasses];
-  if (threadIdx.x < kNetClasses) s_cnt[threadIdx.x] = 0;
+               const int32_t* __restrict__ off, int32_t* list) {
+  __shared__ int32_t s_w[kNetClasses][kNetThreads / 32];  // per-warp starts
+  __shared__ int32_t s_run[kNetClasses];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  if (threadIdx.x < kNetClasses) s_run[threadIdx.x] = off[threadIdx.x * gridDim.x + blockIdx.x];
   __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
-  int idx[kNetNodesPerThread], cls[kNetNodesPerThread], slot[kNetNodesPerThread];
-#pragma unroll
   for (int u = 0; u < kNetNodesPerThread; ++u) {
-    idx[u] = blockIdx.x * kNetNodesPerBlock + u * kNetThreads + threadIdx.x;
-    cls[u] = idx[u] < m ? net_class(idx[u], cap, node_pt, mx, node_done, false) : -1;
-    slot[u] = cls[u] >= 0 ? atomicAdd(&s_cnt[cls[u]], 1) : 0;
-  }
-  __syncthreads();
-  if (threadIdx.x < kNetClasses) {
-    const int c = threadIdx.x;
-    int b = 0;
-    for (int cc = 0; cc < c; ++cc) b += tot[cc];
-    s_base[c] = b + (s_cnt[c] > 0 ? atomicAdd(&cur[c], s_cnt[c]) : 0);
-  }
-  __syncthreads();
+    const int i = blockIdx.x * kNetBlockNodes + u * kNetThreads + threadIdx.x;
+    const int k = i < m ? net_class(i, cap, node_pt, mx, node_done, false) : -1;
+    int rank = 0;
 #pragma unroll
-  for (int u = 0; u < kNetNodesPerThread; ++u)
-    if (cls[u] >= 0) list[s_base[cls[u]] + slot[u]] = idx[u];
+    for (int c = 0; c < kNetClasses; ++c) {
+      const unsigned bm = __ballot_sync(0xffffffffu, k == c);
+      if (k == c) rank = __popc(bm & lt);
+      if (lane == 0) s_w[c][w] = __popc(bm);
+    }
+    __syncthreads();
+    if (threadIdx.x < kNetClasses) {
+      int run = s_run[threadIdx.x];
+#pragma unroll
+      for (int ww = 0; ww < kNetThreads / 32; ++ww) {
+        const int t = s_w[threadIdx.x][ww];
+        s_w[threadIdx.x][ww] = run;
+        run += t;
+      }
+      s_run[threadIdx.x] = run;
+    }
+    __syncthreads();
+    if (k >= 0) list[s_w[k][w] + rank] = i;
+    __syncthreads();
+  }
 }
 
-// One thread per twig of classes 0..4 (list[0 .. tot[0] + ... + tot[4])).
-__global__ void __launch_bounds__(kNetThreads)
+// One thread per twig of classes 0..4: list[off[0] .. off[5 nb]).
+__global__ void __launch_bounds__(kNetThreads, 4)
     k_net_p2m_thread(const Geom* __restrict__ geom, double theta, double4* node_c,
                      const int8_t* __restrict__ node_level,
                      const int32_t* __restrict__ node_parent, MixedNodes mx, Ensemble ens,
-                     const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
-                     int full, int32_t* err) {
-  const int total = tot[0] + tot[1] + tot[2] + tot[3] + tot[4];
+                     const int32_t* __restrict__ off, int nb,
+                     const int32_t* __restrict__ list, int full, int32_t* err) {
+  const int b0 = off[0], b1 = off[5 * nb];
   if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
+  for (int k = b0 + blockIdx.x * blockDim.x + threadIdx.x; k < b1; k += gridDim.x * blockDim.x)
     net_p2m<1>(list[k], 0, geom, theta, node_c, node_level, node_parent, mx, ens, full != 0);
 }
 
-// One warp per twig of class 5.
+// One warp per twig of class 5: list[off[5 nb] .. off[6 nb]).
 __global__ void __launch_bounds__(kNetThreads)
     k_net_p2m_warp(const Geom* __restrict__ geom, double theta, double4* node_c,
                    const int8_t* __restrict__ node_level,
                    const int32_t* __restrict__ node_parent, MixedNodes mx, Ensemble ens,
-                   const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
-                   int full, int32_t* err) {
-  const int b0 = tot[0] + tot[1] + tot[2] + tot[3] + tot[4];
-  const int total = tot[5];
+                   const int32_t* __restrict__ off, int nb,
+                   const int32_t* __restrict__ list, int full, int32_t* err) {
+  const int b0 = off[5 * nb], b1 = off[6 * nb];
   const int lane = threadIdx.x & 31;
   int e = 0;
   if (lane == 0) e = *((volatile int32_t*)err);
   if (__shfl_sync(0xffffffffu, e, 0) & (kErrCapacity | kErrWalk)) return;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < total; k += nw) {
-    net_p2m<32>(list[b0 + k], lane, geom, theta, node_c, node_level, node_parent, mx, ens,
+  for (int k = b0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < b1; k += nw) {
+    net_p2m<32>(list[k], lane, geom, theta, node_c, node_level, node_parent, mx, ens,
                 full != 0);
     __syncwarp();
   }
 }
 
-// The twigs above kMidCount: one thread per climb start computes its twig
-// from the children, then climbs while it is the last child to arrive at the
-// parent (fence, atomic, fence: the children's records are visible to the
-// thread that completes the parent).
+// The twigs above kMidCount: a group of 8 lanes per climb start computes its
+// twig from the children, then climbs while it is the last child to arrive
+// at the parent (fence, atomic, fence: the children's records are visible to
+// the group that completes the parent).  list[off[6 nb] .. off[7 nb]).
 __global__ void __launch_bounds__(128)
     k_net_top(const Geom* __restrict__ geom, double theta, int cap, double4* node_c,
               const int32_t* __restrict__ node_parent, int32_t* node_done,
               const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
-              const int32_t* __restrict__ tot, const int32_t* __restrict__ list,
+              const int32_t* __restrict__ off, int nb, const int32_t* __restrict__ list,
               int32_t* err) {
-  const int b0 = tot[0] + tot[1] + tot[2] + tot[3] + tot[4] + tot[5];
-  const int total = tot[6];
+  const int b0 = off[6 * nb], b1 = off[7 * nb];
+  const int lane = threadIdx.x & 31, j = lane & 7;
+  const unsigned gm = 0xffu << (lane & 24);
   if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
-    int t = list[b0 + k];
+  const int ng = (gridDim.x * blockDim.x) >> 3;
+  for (int k = b0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 3); k < b1; k += ng) {
+    int t = list[k];
     const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, __ldg(&mx.first[t])) : 0;
     const double smax0 = geom[seg].smax0;
-    for (int g = 0; t >= 0; ++g) {
+    for (int g = 0;; ++g) {
       if (g > kMaxLevel + 2) {
-        set_error(err, kErrWalk);
+        if (j == 0) set_error(err, kErrWalk);
         break;
       }
-      if (!net_twig(t, smax0, theta, cap, node_c, node_level, mx, err)) break;
+      if (!net_twig8(t, j, gm, smax0, theta, cap, node_c, node_level, mx, err)) break;
+      const int par = node_parent[t];
+      int last = 0;
+      if (j == 0 && par >= 0) {
+        __threadfence();
+        last = atomicSub(&node_done[par], 1) == 1;
+      }
+      if (!__shfl_sync(gm, last, lane & 24)) break;
       __threadfence();
-      t = node_parent[t];
-      if (t < 0 || atomicSub(&node_done[t], 1) != 1) break;
-      __threadfence();
+      t = par;
     }
   }
 }
@@ -642,15 +634,15 @@ int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double 
                 const Ensemble& ens, bool full, cudaStream_t st) {
   const int T = kNetThreads;
   const int gb = (n + T - 1) / T;
-  const int gcap = (b.cap + kNetNodesPerBlock - 1) / kNetNodesPerBlock;
-  int32_t* tot = b.mx.lvl;       // 7 class totals
-  int32_t* cur = b.mx.lvl + 8;   // 7 class cursors
+  const int nb = (b.cap + kNetBlockNodes - 1) / kNetBlockNodes;
+  int32_t* cnt = b.mx.cls;                        // 7 nb class counts
+  int32_t* off = b.mx.cls + net_cls_entries(b.cap);  // their exclusive scan (+ total)
   k_net_leaves<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.cap, b.node_c,
                                  b.mx, ens, b.err);
-  cudaMemsetAsync(b.mx.lvl, 0, 16 * sizeof(int32_t), st);
-  k_net_mark<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, tot);
-  k_net_fill<<<gcap, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, tot, cur,
-                                 b.mx.lvl_list);
+  k_net_mark<<<nb, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, cnt);
+  int launches = 2 + exclusive_scan(cnt, off, kNetClasses * nb, b.scan_partial, true, st);
+  k_net_fill<<<nb, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, off,
+                               b.mx.lvl_list);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -658,15 +650,15 @@ int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double 
   if (g1 > sms * 8) g1 = sms * 8;
   if (g1 < 1) g1 = 1;
   k_net_p2m_thread<<<g1, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.node_parent,
-                                     b.mx, ens, tot, b.mx.lvl_list, full ? 1 : 0, b.err);
+                                     b.mx, ens, off, nb, b.mx.lvl_list, full ? 1 : 0, b.err);
   int g2 = (n / kSmallCount * 32 + T - 1) / T;
   if (g2 > sms * 8) g2 = sms * 8;
   if (g2 < 1) g2 = 1;
   k_net_p2m_warp<<<g2, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.node_parent,
-                                   b.mx, ens, tot, b.mx.lvl_list, full ? 1 : 0, b.err);
+                                   b.mx, ens, off, nb, b.mx.lvl_list, full ? 1 : 0, b.err);
   k_net_top<<<sms, 128, 0, st>>>(b.geom, theta, b.cap, b.node_c, b.node_parent, b.node_done,
-                                 b.node_level, b.mx, ens, tot, b.mx.lvl_list, b.err);
-  return 6;
+                                 b.node_level, b.mx, ens, off, nb, b.mx.lvl_list, b.err);
+  return launches + 4;
 }
 
 }  // namespace tg

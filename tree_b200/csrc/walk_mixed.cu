@@ -881,6 +881,7 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.geom, (size_t)cap);
   rc |= realloc_dev(&mb.lvl_list, (size_t)cap);
+  rc |= realloc_dev(&mb.cls, 2 * (size_t)net_cls_entries(cap));
   return rc;
 }
 
@@ -902,7 +903,7 @@ int mixed_alloc_particles(MixedBuffers& mb, int n) {
 void mixed_free(MixedBuffers& mb) {
   void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
                   mb.mom3, mb.mom4, mb.geom, mb.xs, mb.groups, mb.stack, mb.control,
-                  mb.lvl_list, mb.lvl};
+                  mb.lvl_list, mb.lvl, mb.cls};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   mb = MixedBuffers();
@@ -924,6 +925,7 @@ MixedNodes mixed_nodes(const MixedBuffers& mb) {
   m.n_groups = mb.control + 2;
   m.lvl_list = mb.lvl_list;
   m.lvl = mb.lvl;
+  m.cls = mb.cls;
   return m;
 }
 

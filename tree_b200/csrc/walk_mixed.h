@@ -25,6 +25,7 @@ struct MixedBuffers {
   int2* groups = nullptr;
   int32_t* lvl_list = nullptr; // per node: twigs by level (upward pass)
   int32_t* lvl = nullptr;      // per level: count, offset, cursor
+  int32_t* cls = nullptr;      // net pass: class counts per node block, then their scan
   int32_t* stack = nullptr;    // per resident warp: kStackCap node indices
   int32_t* control = nullptr;  // [0] group cursor, [1] max stack depth, [2] groups
   int grid_warps = 0;
