@@ -244,13 +244,14 @@ int tree_gpu_tree_dump(tree_gpu_handle* h, int32_t species, int64_t cap,
  * Sxy, Syz, Szx with S = 1/2 sum q a a^T, T[10] in the order xxx yyy zzz xxy
  * xxz xyy yyz xzz yzz xyz, H[15] in the order xxxx yyyy zzzz xxxy xxxz xyyy
  * yyyz xzzz yzzz xxyy xxzz yyzz xxyz xyyz xyzz, 0; all zero for a leaf),
- * first and count (the node's range of sorted particles), level;
+ * first and count (the node's range of sorted particles), level, parent
+ * (-1 for the root);
  * sorted[4 * (n_el + n_ion)]: the sorted particles (x, y, z, 1 for an ion or
  * 0 for an electron).  NULL buffers are skipped; *n_nodes receives the node
  * count (pass all buffers NULL to query it). */
 int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* moments,
-                      int64_t* first, int64_t* count, int32_t* level, double* sorted,
-                      int64_t* n_nodes);
+                      int64_t* first, int64_t* count, int32_t* level, int64_t* parent,
+                      double* sorted, int64_t* n_nodes);
 
 /* Runs all later work of the handle on `stream` (a cudaStream_t; NULL
  * restores the handle's own stream).  No counterpart in the reference (its

@@ -158,11 +158,11 @@ MODULE TREE_GPU_MOD
      END FUNCTION
 
      INTEGER(C_INT) FUNCTION tree_gpu_net_dump(h, cap, centre, moments, first, &
-          count, level, sorted, n_nodes) BIND(C)
+          count, level, parent, sorted, n_nodes) BIND(C)
        IMPORT :: C_INT, C_PTR, C_INT64_T
        TYPE(C_PTR), VALUE :: h
        INTEGER(C_INT64_T), VALUE :: cap
-       TYPE(C_PTR), VALUE :: centre, moments, first, count, level, sorted
+       TYPE(C_PTR), VALUE :: centre, moments, first, count, level, parent, sorted
        INTEGER(C_INT64_T), INTENT(OUT) :: n_nodes
      END FUNCTION
 

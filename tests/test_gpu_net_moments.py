@@ -89,3 +89,55 @@ def test_net_moments_match_their_definition(device_lib, n_half):
         assert err.max() <= 1e-11, (t, cnt[t], err.max())
     print(f"net moments n={2 * n_half}: {len(pick)} twigs checked "
           f"({len(big)} above 64 particles), worst scaled error {worst:.2e}")
+
+
+@pytest.mark.parametrize("colocated", [False, True])
+def test_combined_tree_structure(device_lib, colocated):
+    """The combined tree's nodes, one thread per node: the root holds every
+    particle; each node lies one level below its parent, which precedes it in
+    pre-order; a twig's first child follows it; the children of a twig
+    partition its particle range in index order; the leaves are the sorted
+    particles, one each; and a twig's particles fit the cell of its level
+    (the root box halved per level).  colocated: electrons exactly on their
+    ions, whose pairs share all 42 spatial levels (chains of one-child
+    twigs down to the species bit)."""
+    xe, xi = _cloud(20000, 99)
+    if colocated:
+        xe = xi.copy()
+    cfg = api.Config(theta=0.5, physics=api.PHYS_KELBG, precision=api.PREC_MIXED)
+    with api.TreeForce(len(xe), len(xi), cfg) as tf:
+        tf.force(xe, xi)
+        d = tf.net_dump()
+    n = len(xe) + len(xi)
+    first, cnt, lev, par = d["first"], d["count"], d["level"], d["parent"]
+    m = len(cnt)
+    assert par[0] == -1 and lev[0] == 0 and first[0] == 0 and cnt[0] == n
+    i = np.arange(1, m)
+    assert np.all((par[1:] >= 0) & (par[1:] < i))
+    assert np.all(lev[1:] == lev[par[1:]] + 1)
+    leaf = cnt == 1
+    twig = ~leaf
+    assert leaf.sum() == n
+    assert np.array_equal(np.sort(first[leaf]), np.arange(n))
+    tw = np.flatnonzero(twig)
+    assert np.all(par[tw + 1] == tw)  # pre-order: the first child follows
+    # children partition the parent's range, in index order
+    ch = np.flatnonzero(par >= 0)
+    order = np.lexsort((first[ch], par[ch]))
+    ch = ch[order]
+    p = par[ch]
+    start = np.r_[True, p[1:] != p[:-1]]
+    assert np.all(first[ch[start]] == first[p[start]])
+    nxt = ~start
+    assert np.all(first[ch[nxt]] == first[ch[np.flatnonzero(nxt) - 1]] + cnt[ch[np.flatnonzero(nxt) - 1]])
+    sums = np.bincount(p, weights=cnt[ch], minlength=m)
+    assert np.array_equal(sums[tw], cnt[tw].astype(float))
+    # particles of a twig fit its cell (per axis: root side / 2^level)
+    xs = d["sorted"][:, :3]
+    side = xs.max(0) - xs.min(0)
+    for t in np.random.default_rng(5).choice(tw, min(4000, len(tw)), replace=False):
+        q = xs[first[t]:first[t] + cnt[t]]
+        ext = q.max(0) - q.min(0)
+        assert np.all(ext <= side * 2.0 ** -int(lev[t]) * (1 + 1e-12)), (t, lev[t])
+    if colocated:
+        assert lev.max() >= 42  # e-i pairs separated only by the species bit

@@ -112,7 +112,7 @@ def load_library(path: str = LIB_PATH):
                                      dp, dp, ctypes.POINTER(ctypes.c_int32),
                                      lp, lp, lp]
     L.tree_gpu_net_dump.argtypes = [vp, ctypes.c_int64, dp, dp, lp, lp,
-                                    ctypes.POINTER(ctypes.c_int32), dp, lp]
+                                    ctypes.POINTER(ctypes.c_int32), lp, dp, lp]
     L.tree_gpu_direct.argtypes = [vp, lp, ctypes.c_int64, dp, dp]
     L.tree_gpu_direct_static.argtypes = [vp, ctypes.c_int64, ctypes.c_int64,
                                          ctypes.POINTER(Params), vp,
@@ -371,25 +371,26 @@ class TreeForce:
         """The combined tree of the mixed path, rebuilt from the current device
         positions with every FP64 record written (pre-order):
         centre (m, 3), moments (m, 38) -- n, Q, D[3], q_ion, S[6] (xx yy zz xy
-        yz zx), T[10], H[15], 0 -- first, count, level (m,), and the sorted
-        particles (n, 4): x, y, z, 1 for ions."""
+        yz zx), T[10], H[15], 0 -- first, count, level, parent (m,), and the
+        sorted particles (n, 4): x, y, z, 1 for ions."""
         n = ctypes.c_int64()
         self._check(self.lib.tree_gpu_net_dump(self.h, 0, None, None, None, None, None,
-                                               None, ctypes.byref(n)))
+                                               None, None, ctypes.byref(n)))
         m = n.value
         centre = np.zeros((m, 3))
         mom = np.zeros((m, 38))
         first = np.zeros(m, np.int64)
         count = np.zeros(m, np.int64)
         level = np.zeros(m, np.int32)
+        parent = np.zeros(m, np.int64)
         xs = np.zeros((self.n_el + self.n_ion, 4))
         lp = ctypes.POINTER(ctypes.c_int64)
         self._check(self.lib.tree_gpu_net_dump(
             self.h, m, _dp(centre), _dp(mom), first.ctypes.data_as(lp),
             count.ctypes.data_as(lp), level.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
-            _dp(xs), ctypes.byref(n)))
+            parent.ctypes.data_as(lp), _dp(xs), ctypes.byref(n)))
         return dict(centre=centre, moments=mom, first=first, count=count, level=level,
-                    sorted=xs)
+                    parent=parent, sorted=xs)
 
     def set_stream(self, stream_handle: int | None):
         """Enqueue later work on a caller's cudaStream_t (an integer handle,

@@ -199,7 +199,7 @@ __global__ void k_geom_seg(const uint64_t* bb, const int32_t* __restrict__ start
 // (top = 1 - lsb for the single-cloud layouts).
 __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
                        int lsb, int n_el_charge, const Geom* __restrict__ geom,
-                       Ensemble ens, key128* keys, uint32_t* vals) {
+                       Ensemble ens, key128* keys, uint64_t* hi, uint32_t* vals) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int s = i >= n_el;
@@ -237,7 +237,15 @@ __global__ void k_keys(const double* __restrict__ x, int n, int n_el,
   if (lsb) key |= (key128)(ion ? 1u : 0u);
   if (top > 0) key |= (key128)(uint32_t)seg << (128 - top);
   keys[i] = key;
+  hi[i] = (uint64_t)(key >> 64);
   vals[i] = (uint32_t)i;
+}
+
+// Full keys in the order of the sorted high words.
+__global__ void k_gather_keys(const key128* __restrict__ keys_in,
+                              const uint32_t* __restrict__ vals, int n, key128* keys_out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) keys_out[p] = keys_in[vals[p]];
 }
 
 // ---------------------------------------------------------------- scan ----
@@ -805,6 +813,104 @@ __global__ void k_topology(const key128* __restrict__ keys,
                               : twig_index_before(keys, L, off, sb, p, depth - 1, top);
 }
 
+// ------------------------------------------- combined-tree topology ----
+// The combined tree of the mixed path is written one thread per node rather
+// than one per particle: no lane waits on another's emission loop.  Node i
+// belongs to the sorted particle that emits it (owner[i]); its slot among
+// that particle's nodes gives its level.  Twig centres are the closed form
+// of the key's digits, c_k = c0_k + lx0_k ((B_k + 1/2) 2^-d - 1/2), B_k the
+// d bits of axis k (within a rounding of the level-by-level descent; the
+// mixed walk reads them only through |centroid - centre|).  Leaves also
+// write their position (w = -1, the walk's leaf mark) and the sorted copy
+// xs (w = 1 for ions).  The child table is cleared here and filled by
+// k_link_children; per-node skip and child counts are not needed.
+__global__ void k_owner(const int32_t* __restrict__ off, int n, int cap, int32_t* owner) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int e = off[p + 1] < cap ? off[p + 1] : cap;
+  for (int i = off[p]; i < e; ++i) owner[i] = p;
+}
+
+__global__ void k_topology_mixed(const key128* __restrict__ keys,
+                                 const uint32_t* __restrict__ vals,
+                                 const int8_t* __restrict__ L,
+                                 const int32_t* __restrict__ off,
+                                 const int32_t* __restrict__ owner,
+                                 const int32_t* __restrict__ bounds, int n,
+                                 int n_el_charge, const double* __restrict__ x,
+                                 const Geom* __restrict__ geom, int cap, double4* node_c,
+                                 int32_t* node_pt, int32_t* node_parent, int32_t* node_done,
+                                 int8_t* node_level, MixedNodes mx, Ensemble ens) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int p = owner[i];
+  const int slot = i - off[p];
+  int lo, hi;
+  lo_hi(L, p, lo, hi);
+  const int ntw = hi > lo ? hi - lo : 0;
+  int s = 0, sb = 0, se = n, top = 0, nlev = kMaxLevel;  // single cloud: top = 1 - lsb = 0
+  if (ens.nseg > 0) {
+    s = seg_of(ens.start, ens.nseg, p);
+    sb = ens.start[s];
+    se = ens.start[s + 1];
+    top = ens.top;
+    nlev = ens.nlev;
+  }
+  const key128 key = keys[p];
+  node_done[i] = 0;
+  mx.first[i] = p;
+  if (slot < ntw) {
+    const int d = lo + 1 + slot;
+    // axis bits of the first d digits (digit l at bits 127 - 3l .. 125 - 3l of key << top)
+    uint64_t B[3] = {0, 0, 0};
+    key128 kk = key << top;
+    for (int l = 0; l < d; ++l) {
+      const uint32_t dig = (uint32_t)(kk >> 125) & 7u;
+      B[0] = 2 * B[0] + (dig & 1u);
+      B[1] = 2 * B[1] + ((dig >> 1) & 1u);
+      B[2] = 2 * B[2] + (dig >> 2);
+      kk <<= 3;
+    }
+    const Geom& G = geom[s];
+    double c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double f = ldexp((double)B[k] + 0.5, -d) - 0.5;  // exact
+      c[k] = G.c0[k] + G.lx0[k] * f;
+    }
+    node_c[i] = make_double4(c[0], c[1], c[2], 0.0);
+    node_level[i] = (int8_t)d;
+    node_pt[i] = -1;
+    int q_end = se;
+    if (d > 0) {
+      const int sh = shift_for_level(d, top);
+      q_end = range_end(keys, L, p, se, d, sh, key >> sh);
+    }
+    mx.count[i] = q_end - p;
+    mx.digit[i] = d == 0 ? (int8_t)0 : (int8_t)((key >> (128 - top - 3 * d)) & 7);
+    int4* kk4 = reinterpret_cast<int4*>(mx.kids + 8 * (int64_t)i);
+    kk4[0] = make_int4(-1, -1, -1, -1);
+    kk4[1] = make_int4(-1, -1, -1, -1);
+    node_parent[i] = d == 0 ? -1
+                     : slot > 0 ? i - 1
+                                : twig_index_before(keys, L, off, sb, p, d - 1, top);
+  } else {
+    const int depth = (lo > hi ? lo : hi) + 1;
+    const uint32_t o = vals[p];
+    node_level[i] = (int8_t)depth;
+    node_pt[i] = (int32_t)o;
+    mx.count[i] = 1;
+    mx.digit[i] = depth <= nlev ? (int8_t)((key >> (128 - top - 3 * depth)) & 7)
+                                : (int8_t)(key & 1);
+    node_parent[i] = ntw > 0 ? i - 1 : twig_index_before(keys, L, off, sb, p, depth - 1, top);
+    const bool ion = (int)o >= (ens.nseg > 0 ? __ldg(&ens.elec_end[s]) : n_el_charge);
+    const double px = x[3 * (int64_t)o], py = x[3 * (int64_t)o + 1], pz = x[3 * (int64_t)o + 2];
+    node_c[i] = make_double4(px, py, pz, -1.0);
+    mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
+  }
+}
+
 // Counts children per twig (separate launch so the zeroing in k_topology is
 // complete).
 __global__ void k_link_children(const int32_t* __restrict__ node_parent,
@@ -815,7 +921,7 @@ __global__ void k_link_children(const int32_t* __restrict__ node_parent,
   if (i >= m) return;
   int par = node_parent[i];
   if (par >= 0) {
-    atomicAdd(&node_nchild[par], 1);
+    if (node_nchild) atomicAdd(&node_nchild[par], 1);
     mx.kids[8 * (int64_t)par + mx.digit[i]] = i;  // siblings have distinct digits
   }
 }
@@ -1079,12 +1185,16 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   const int lsb = mode == 0 ? 0 : 1;
   const int top = ens.nseg > 0 ? ens.top : 1 - lsb;
   const int nlev = ens.nseg > 0 ? ens.nlev : kMaxLevel;
-  k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, ens, b.keys, b.vals);
+  // full keys into keys_alt, their high words into the two halves of keys
+  uint64_t* hi = reinterpret_cast<uint64_t*>(b.keys);
+  k_keys<<<gb, T, 0, st>>>(x, n, split, lsb, n_el, b.geom, ens, b.keys_alt, hi, b.vals);
   launches += 3;
-  // sort on the high 64 bits (8 passes), then order the rare ties fully;
+  // sort the high 64 bits (8 passes over 12-byte pairs), gather the full
+  // keys in that order, then order the rare ties fully;
   // a long tie run switches on the one-block full sort (which exits otherwise)
-  launches += radix_sort(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
-                         b.sort_hist, b.scan_partial, st, 8);
+  launches += radix_sort(hi, b.vals, hi + n, b.vals_alt, n, b.sort_hist, b.scan_partial, st);
+  k_gather_keys<<<gb, T, 0, st>>>(b.keys_alt, b.vals, n, b.keys);
+  launches += 1;
   cudaMemsetAsync(b.bounds + 4, 0, sizeof(int32_t), st);
   k_tie_fix<<<gb, T, 0, st>>>(b.keys, b.vals, n, b.bounds + 4);
   k_sort_block<<<1, kSbThreads, 0, st>>>(b.keys, b.vals, b.keys_alt, b.vals_alt, n,
@@ -1094,14 +1204,24 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);
   k_bounds<<<1, 32, 0, st>>>(b.off, n, split, b.cap, b.bounds, b.err);
-  k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, split, lsb, b.geom,
-                               b.cap, b.node_c, b.node_skip, b.node_pt,
-                               b.node_parent, b.node_nchild, b.node_done,
-                               b.node_level, b.mx, ens, b.err);
   int gcap = (b.cap + T - 1) / T;
-  k_link_children<<<gcap, T, 0, st>>>(b.node_parent, b.bounds, b.cap,
-                                      b.node_nchild, b.mx);
-  launches += 3;
+  if (mode == 0) {
+    k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, split, lsb, b.geom,
+                                 b.cap, b.node_c, b.node_skip, b.node_pt,
+                                 b.node_parent, b.node_nchild, b.node_done,
+                                 b.node_level, b.mx, ens, b.err);
+    k_link_children<<<gcap, T, 0, st>>>(b.node_parent, b.bounds, b.cap,
+                                        b.node_nchild, b.mx);
+    launches += 3;
+  } else {
+    // node_nchild serves as the owner array (the combined tree counts no children)
+    k_owner<<<gb, T, 0, st>>>(b.off, n, b.cap, b.node_nchild);
+    k_topology_mixed<<<gcap, T, 0, st>>>(b.keys, b.vals, b.L, b.off, b.node_nchild, b.bounds,
+                                         n, n_el, x, b.geom, b.cap, b.node_c, b.node_pt,
+                                         b.node_parent, b.node_done, b.node_level, b.mx, ens);
+    k_link_children<<<gcap, T, 0, st>>>(b.node_parent, b.bounds, b.cap, nullptr, b.mx);
+    launches += 4;
+  }
   if (mode == 0) {
     k_upward<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, split, b.geom, theta,
                                b.cap, b.bounds, b.node_c, b.node_m,
@@ -1109,7 +1229,7 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
                                b.node_done, b.node_level, b.err);
     return launches + 1;
   }
-  launches += net_moments(b, x, n, n_el, theta, ens, full_records, st);
+  launches += net_moments(b, n, theta, ens, full_records, st);
   // the level lists of the upward pass are free again: a single cloud keeps
   // its group-level histogram there, an ensemble has one row per cloud
   const int nsg = ens.nseg > 0 ? ens.nseg : 1;

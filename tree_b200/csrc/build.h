@@ -119,7 +119,7 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
                 double theta, int mode, cudaStream_t st, bool full_records = false);
 // The net-charge moments of the combined tree (mode 1) once its topology and
 // child tables exist.
-int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double theta,
-                const Ensemble& ens, bool full_records, cudaStream_t st);
+int net_moments(const BuildBuffers& b, int n, double theta, const Ensemble& ens,
+                bool full_records, cudaStream_t st);
 
 }  // namespace tg

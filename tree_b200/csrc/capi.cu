@@ -963,8 +963,8 @@ static int build_full_records(tree_gpu_handle* h) {
 }
 
 int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* moments,
-                      int64_t* first, int64_t* count, int32_t* level, double* sorted,
-                      int64_t* n_nodes) {
+                      int64_t* first, int64_t* count, int32_t* level, int64_t* parent,
+                      double* sorted, int64_t* n_nodes) {
   if (!h) return TREE_GPU_ERR_ARG;
   if (h->b.ens.nseg > 0)
     return fail(h, TREE_GPU_ERR_ARG, "ensemble handle: no combined-tree dump");
@@ -976,11 +976,12 @@ int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* m
   CK(cudaMemcpy(bnd, h->b.bounds, sizeof(bnd), cudaMemcpyDeviceToHost));
   const int m = std::min(bnd[2], h->b.cap);
   if (n_nodes) *n_nodes = m;
-  if (!centre && !moments && !first && !count && !level && !sorted) return TREE_GPU_OK;
+  if (!centre && !moments && !first && !count && !level && !parent && !sorted)
+    return TREE_GPU_OK;
   if (cap < m) return fail(h, TREE_GPU_ERR_ARG, "dump buffer too small");
   std::vector<double4> c(m);
   std::vector<double2> mm((size_t)tg::kM64 * m);
-  std::vector<int32_t> fi(m), co(m), pt(m);
+  std::vector<int32_t> fi(m), co(m), pt(m), pa(m);
   std::vector<int8_t> lv(m);
   if (m) {
     CK(cudaMemcpy(c.data(), h->b.node_c, m * sizeof(double4), cudaMemcpyDeviceToHost));
@@ -989,9 +990,11 @@ int tree_gpu_net_dump(tree_gpu_handle* h, int64_t cap, double* centre, double* m
     CK(cudaMemcpy(fi.data(), h->b.mx.first, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(co.data(), h->b.mx.count, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(pt.data(), h->b.node_pt, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pa.data(), h->b.node_parent, m * sizeof(int32_t), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(lv.data(), h->b.node_level, m * sizeof(int8_t), cudaMemcpyDeviceToHost));
   }
   for (int i = 0; i < m; ++i) {
+    if (parent) parent[i] = pa[i];
     if (centre) {
       centre[3 * (size_t)i] = c[i].x;
       centre[3 * (size_t)i + 1] = c[i].y;

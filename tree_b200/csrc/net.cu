@@ -53,33 +53,6 @@ __constant__ double kTMult[10] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 6};
 constexpr int kMidCount = 2048;   // twigs up to this size: direct sums (P2M)
 constexpr int kSmallCount = 64;   // twigs up to this size: a thread each, else a warp
 
-// Leaves of the combined tree (one per sorted particle): the position with
-// w = -1 (the walk's leaf mark), and the sorted positions the walk and the
-// direct sums read (w = 1 for ions).
-__global__ void k_net_leaves(const double* __restrict__ x,
-                             const uint32_t* __restrict__ vals,
-                             const int8_t* __restrict__ L,
-                             const int32_t* __restrict__ off, int n,
-                             int n_el_charge, int cap, double4* node_c,
-                             MixedNodes mx, Ensemble ens, int32_t* err) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  if (*((volatile int32_t*)err) & kErrCapacity) return;
-  int lo, hi;
-  lo_hi(L, p, lo, hi);
-  int ntw = hi > lo ? hi - lo : 0;
-  int leaf = off[p] + ntw;
-  if (leaf >= cap) return;
-  uint32_t o = vals[p];
-  // sorting keeps each cloud's index range, so p and o share the cloud
-  const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, p) : 0;
-  const bool ion = (int)o >= (ens.nseg > 0 ? __ldg(&ens.elec_end[seg]) : n_el_charge);
-  const double px = x[3 * (int64_t)o], py = x[3 * (int64_t)o + 1],
-               pz = x[3 * (int64_t)o + 2];
-  node_c[leaf] = make_double4(px, py, pz, -1.0);
-  mx.xs[p] = make_double4(px, py, pz, ion ? 1.0 : 0.0);
-}
-
 // ---- the records of one twig ----
 // The FP32 records and node_c are always written; the FP64 record m64 only
 // where it is read: by the parallel-axis pass (children of the large twigs,
@@ -628,19 +601,17 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// The net-charge moments of the combined tree (leaves, sort of the twigs
-// into classes, direct sums, climb).  Returns launches.
-int net_moments(const BuildBuffers& b, const double* x, int n, int n_el, double theta,
-                const Ensemble& ens, bool full, cudaStream_t st) {
+// The net-charge moments of the combined tree (sort of the twigs into
+// classes, direct sums, climb) once the topology (with the leaves' positions
+// and the sorted copy xs) and the child tables exist.  Returns launches.
+int net_moments(const BuildBuffers& b, int n, double theta, const Ensemble& ens, bool full,
+                cudaStream_t st) {
   const int T = kNetThreads;
-  const int gb = (n + T - 1) / T;
   const int nb = (b.cap + kNetBlockNodes - 1) / kNetBlockNodes;
   int32_t* cnt = b.mx.cls;                        // 7 nb class counts
   int32_t* off = b.mx.cls + net_cls_entries(b.cap);  // their exclusive scan (+ total)
-  k_net_leaves<<<gb, T, 0, st>>>(x, b.vals, b.L, b.off, n, n_el, b.cap, b.node_c,
-                                 b.mx, ens, b.err);
   k_net_mark<<<nb, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, cnt);
-  int launches = 2 + exclusive_scan(cnt, off, kNetClasses * nb, b.scan_partial, true, st);
+  int launches = 1 + exclusive_scan(cnt, off, kNetClasses * nb, b.scan_partial, true, st);
   k_net_fill<<<nb, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, off,
                                b.mx.lvl_list);
   int dev = 0, sms = 148;
