@@ -831,19 +831,12 @@ __global__ void k_owner(const int32_t* __restrict__ off, int n, int cap, int32_t
   for (int i = off[p]; i < e; ++i) owner[i] = p;
 }
 
-__global__ void k_topology_mixed(const key128* __restrict__ keys,
-                                 const uint32_t* __restrict__ vals,
-                                 const int8_t* __restrict__ L,
-                                 const int32_t* __restrict__ off,
-                                 const int32_t* __restrict__ owner,
-                                 const int32_t* __restrict__ bounds, int n,
-                                 int n_el_charge, const double* __restrict__ x,
-                                 const Geom* __restrict__ geom, int cap, double4* node_c,
-                                 int32_t* node_pt, int32_t* node_parent, int32_t* node_done,
-                                 int8_t* node_level, MixedNodes mx, Ensemble ens) {
-  const int m = bounds[2] < cap ? bounds[2] : cap;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+__device__ __forceinline__ void topology_node(
+    int i, const key128* __restrict__ keys, const uint32_t* __restrict__ vals,
+    const int8_t* __restrict__ L, const int32_t* __restrict__ off,
+    const int32_t* __restrict__ owner, int n, int n_el_charge, const double* __restrict__ x,
+    const Geom* __restrict__ geom, double4* node_c, int32_t* node_pt, int32_t* node_parent,
+    int32_t* node_done, int8_t* node_level, const MixedNodes& mx, const Ensemble& ens) {
   const int p = owner[i];
   const int slot = i - off[p];
   int lo, hi;
@@ -911,18 +904,34 @@ __global__ void k_topology_mixed(const key128* __restrict__ keys,
   }
 }
 
+__global__ void k_topology_mixed(const key128* __restrict__ keys,
+                                 const uint32_t* __restrict__ vals,
+                                 const int8_t* __restrict__ L,
+                                 const int32_t* __restrict__ off,
+                                 const int32_t* __restrict__ owner,
+                                 const int32_t* __restrict__ bounds, int n,
+                                 int n_el_charge, const double* __restrict__ x,
+                                 const Geom* __restrict__ geom, int cap, double4* node_c,
+                                 int32_t* node_pt, int32_t* node_parent, int32_t* node_done,
+                                 int8_t* node_level, MixedNodes mx, Ensemble ens) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    topology_node(i, keys, vals, L, off, owner, n, n_el_charge, x, geom, node_c, node_pt,
+                  node_parent, node_done, node_level, mx, ens);
+}
+
 // Counts children per twig (separate launch so the zeroing in k_topology is
 // complete).
 __global__ void k_link_children(const int32_t* __restrict__ node_parent,
                                 const int32_t* __restrict__ bounds, int cap,
                                 int32_t* node_nchild, MixedNodes mx) {
-  int m = bounds[2] < cap ? bounds[2] : cap;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  int par = node_parent[i];
-  if (par >= 0) {
-    if (node_nchild) atomicAdd(&node_nchild[par], 1);
-    mx.kids[8 * (int64_t)par + mx.digit[i]] = i;  // siblings have distinct digits
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const int par = node_parent[i];
+    if (par >= 0) {
+      if (node_nchild) atomicAdd(&node_nchild[par], 1);
+      mx.kids[8 * (int64_t)par + mx.digit[i]] = i;  // siblings have distinct digits
+    }
   }
 }
 
@@ -1072,21 +1081,24 @@ __global__ void k_group_levels(const int32_t* __restrict__ bounds, int cap,
                                const int8_t* __restrict__ node_level, MixedNodes mx,
                                Ensemble ens, int32_t* glvl) {
   const int m = bounds[2] < cap ? bounds[2] : cap;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int slot = -1, w = 0;
-  if (t < m) {
-    const int cnt = mx.count[t];
-    const int par = node_parent[t];
-    if (cnt <= kGroupMax && (par < 0 || mx.count[par] > kGroupMax)) {
-      const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[t]) : 0;
-      slot = seg * kLevelSlots + node_level[t];
-      w = cnt;
+  // warp-uniform loop: every lane reaches the collectives of each round
+  for (int base = blockIdx.x * blockDim.x; base < m; base += gridDim.x * blockDim.x) {
+    const int t = base + threadIdx.x;
+    int slot = -1, w = 0;
+    if (t < m) {
+      const int cnt = mx.count[t];
+      const int par = node_parent[t];
+      if (cnt <= kGroupMax && (par < 0 || mx.count[par] > kGroupMax)) {
+        const int seg = ens.nseg > 0 ? seg_of(ens.start, ens.nseg, mx.first[t]) : 0;
+        slot = seg * kLevelSlots + node_level[t];
+        w = cnt;
+      }
     }
+    // one atomic per distinct slot per warp
+    const unsigned peers = __match_any_sync(0xffffffffu, slot);
+    const int sum = __reduce_add_sync(peers, w);
+    if (slot >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&glvl[slot], sum);
   }
-  // one atomic per distinct slot per warp (all lanes reach this point)
-  const unsigned peers = __match_any_sync(0xffffffffu, slot);
-  const int sum = __reduce_add_sync(peers, w);
-  if (slot >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&glvl[slot], sum);
 }
 
 // Per cloud: the lowest level at which siblings may be packed, stored in the
@@ -1109,14 +1121,11 @@ __global__ void k_group_cut(int32_t* glvl, int nseg) {
   h[kLevelSlots - 1] = med > kGroupSlack ? med - kGroupSlack : 0;
 }
 
-__global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
-                         const int32_t* __restrict__ node_parent,
-                         const int8_t* __restrict__ node_level, MixedNodes mx,
-                         Ensemble ens, const int32_t* __restrict__ glvl,
-                         int2* groups, int32_t* n_groups) {
-  int m = bounds[2] < cap ? bounds[2] : cap;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= m) return;
+__device__ __forceinline__ void groups_of_node(int t, const int32_t* __restrict__ node_parent,
+                                               const int8_t* __restrict__ node_level,
+                                               const MixedNodes& mx, const Ensemble& ens,
+                                               const int32_t* __restrict__ glvl,
+                                               int2* groups, int32_t* n_groups) {
   const int cnt = mx.count[t];
   if (node_parent[t] < 0 && cnt <= kGroupMax) {  // a whole tree fits one group
     int g = atomicAdd(n_groups, 1);
@@ -1157,6 +1166,16 @@ __global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
     run_cnt += cc;
   }
   close_run();
+}
+
+__global__ void k_groups(const int32_t* __restrict__ bounds, int cap,
+                         const int32_t* __restrict__ node_parent,
+                         const int8_t* __restrict__ node_level, MixedNodes mx,
+                         Ensemble ens, const int32_t* __restrict__ glvl,
+                         int2* groups, int32_t* n_groups) {
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x)
+    groups_of_node(t, node_parent, node_level, mx, ens, glvl, groups, n_groups);
 }
 
 // ------------------------------------------------------------- driver ----
@@ -1204,7 +1223,12 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);
   k_bounds<<<1, 32, 0, st>>>(b.off, n, split, b.cap, b.bounds, b.err);
+  // per-node passes: a fixed grid striding over the device's node count
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int gcap = (b.cap + T - 1) / T;
+  if (gcap > 8 * sms) gcap = 8 * sms;
   if (mode == 0) {
     k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, split, lsb, b.geom,
                                  b.cap, b.node_c, b.node_skip, b.node_pt,

@@ -25,11 +25,11 @@ struct MixedNodes {
   int32_t* lvl_list; // per node: twigs grouped by level (upward pass)
   int32_t* lvl;      // kLevelSlots x 3: count, offset, cursor per level
   int32_t* cls;      // net pass: class counts per block of 1024 nodes (class-major),
-                     // then their exclusive scan (net_cls_entries(cap) each)
+                     // then their exclusive scan (net_cls_entries(cap) in all)
 };
 
-// Entries of each half of MixedNodes::cls for node capacity cap.
-inline int net_cls_entries(int cap) { return 7 * ((cap + 1023) / 1024) + 1; }
+// Entries of MixedNodes::cls for node capacity cap.
+inline int net_cls_entries(int cap) { return 2 * 7 * ((cap + 1023) / 1024); }
 
 constexpr int kLevelSlots = 64;  // > deepest twig level
 

@@ -469,88 +469,144 @@ __device__ __forceinline__ int net_class(int i, int cap, const int32_t* __restri
   return big == 0 ? 6 : -1;
 }
 
-// Pass 1 of the sort: class counts of block b's nodes in cnt[class * nb + b].
+// Pass 1 of the sort: class counts of node block b (nodes b kNetBlockNodes
+// .. + kNetBlockNodes - 1) in cnt[class * NB + b], for the blocks that hold
+// nodes (the grid strides over them; NB: the blocks of the node capacity).
 __global__ void __launch_bounds__(kNetThreads)
-    k_net_mark(const int32_t* __restrict__ bounds, int cap,
+    k_net_mark(const int32_t* __restrict__ bounds, int cap, int NB,
                const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
                int32_t* cnt) {
   __shared__ int32_t h[kNetClasses];
-  if (threadIdx.x < kNetClasses) h[threadIdx.x] = 0;
-  __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int nblk = (m + kNetBlockNodes - 1) / kNetBlockNodes;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    if (threadIdx.x < kNetClasses) h[threadIdx.x] = 0;
+    __syncthreads();
 #pragma unroll
-  for (int u = 0; u < kNetNodesPerThread; ++u) {
-    const int i = blockIdx.x * kNetBlockNodes + u * kNetThreads + threadIdx.x;
-    if (i < m) {
-      const int k = net_class(i, cap, node_pt, mx, node_done, true);
-      if (k >= 0) atomicAdd(&h[k], 1);
+    for (int u = 0; u < kNetNodesPerThread; ++u) {
+      const int i = blk * kNetBlockNodes + u * kNetThreads + threadIdx.x;
+      if (i < m) {
+        const int k = net_class(i, cap, node_pt, mx, node_done, true);
+        if (k >= 0) atomicAdd(&h[k], 1);
+      }
     }
+    __syncthreads();
+    if (threadIdx.x < kNetClasses) cnt[threadIdx.x * NB + blk] = h[threadIdx.x];
+    __syncthreads();
   }
-  __syncthreads();
-  if (threadIdx.x < kNetClasses) cnt[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
 }
 
-// Pass 2: block b's twigs of class c written in index order from off[c * nb
-// + b] (the exclusive scan of the counts).
+// The exclusive scan of the counts in class-major order, one block: off[c *
+// NB + b] = where block b's twigs of class c start; start[c] = where class c
+// starts (start[7] = all twigs listed).
+__global__ void __launch_bounds__(1024)
+    k_net_scan(const int32_t* __restrict__ bounds, int cap, int NB,
+               const int32_t* __restrict__ cnt, int32_t* off, int32_t* start) {
+  __shared__ int32_t ws[32];
+  __shared__ int32_t carry;
+  const int m = bounds[2] < cap ? bounds[2] : cap;
+  const int nblk = (m + kNetBlockNodes - 1) / kNetBlockNodes;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int c = 0; c < kNetClasses; ++c) {
+    if (threadIdx.x == 0) start[c] = carry;
+    for (int b0 = 0; b0 < nblk; b0 += 1024) {
+      const int b = b0 + threadIdx.x;
+      const int v = b < nblk ? cnt[c * NB + b] : 0;
+      int inc = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+      }
+      if (lane == 31) ws[w] = inc;
+      __syncthreads();
+      if (w == 0) {
+        const int x = ws[lane];
+        int wi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, wi, o);
+          if (lane >= o) wi += t;
+        }
+        ws[lane] = wi - x;
+      }
+      __syncthreads();
+      const int base = carry;
+      if (b < nblk) off[c * NB + b] = base + ws[w] + inc - v;
+      __syncthreads();
+      if (threadIdx.x == 1023) carry = base + ws[w] + inc;
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) start[kNetClasses] = carry;
+}
+
+// Pass 2: block b's twigs of class c written in index order from off[c * NB
+// + b].
 __global__ void __launch_bounds__(kNetThreads)
-    k_net_fill(const int32_t* __restrict__ bounds, int cap,
+    k_net_fill(const int32_t* __restrict__ bounds, int cap, int NB,
                const int32_t* __restrict__ node_pt, int32_t* node_done, MixedNodes mx,
                const int32_t* __restrict__ off, int32_t* list) {
   __shared__ int32_t s_w[kNetClasses][kNetThreads / 32];  // per-warp starts
   __shared__ int32_t s_run[kNetClasses];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  if (threadIdx.x < kNetClasses) s_run[threadIdx.x] = off[threadIdx.x * gridDim.x + blockIdx.x];
-  __syncthreads();
   const int m = bounds[2] < cap ? bounds[2] : cap;
-  for (int u = 0; u < kNetNodesPerThread; ++u) {
-    const int i = blockIdx.x * kNetBlockNodes + u * kNetThreads + threadIdx.x;
-    const int k = i < m ? net_class(i, cap, node_pt, mx, node_done, false) : -1;
-    int rank = 0;
-#pragma unroll
-    for (int c = 0; c < kNetClasses; ++c) {
-      const unsigned bm = __ballot_sync(0xffffffffu, k == c);
-      if (k == c) rank = __popc(bm & lt);
-      if (lane == 0) s_w[c][w] = __popc(bm);
-    }
+  const int nblk = (m + kNetBlockNodes - 1) / kNetBlockNodes;
+  for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    if (threadIdx.x < kNetClasses) s_run[threadIdx.x] = off[threadIdx.x * NB + blk];
     __syncthreads();
-    if (threadIdx.x < kNetClasses) {
-      int run = s_run[threadIdx.x];
+    for (int u = 0; u < kNetNodesPerThread; ++u) {
+      const int i = blk * kNetBlockNodes + u * kNetThreads + threadIdx.x;
+      const int k = i < m ? net_class(i, cap, node_pt, mx, node_done, false) : -1;
+      int rank = 0;
 #pragma unroll
-      for (int ww = 0; ww < kNetThreads / 32; ++ww) {
-        const int t = s_w[threadIdx.x][ww];
-        s_w[threadIdx.x][ww] = run;
-        run += t;
+      for (int c = 0; c < kNetClasses; ++c) {
+        const unsigned bm = __ballot_sync(0xffffffffu, k == c);
+        if (k == c) rank = __popc(bm & lt);
+        if (lane == 0) s_w[c][w] = __popc(bm);
       }
-      s_run[threadIdx.x] = run;
+      __syncthreads();
+      if (threadIdx.x < kNetClasses) {
+        int run = s_run[threadIdx.x];
+#pragma unroll
+        for (int ww = 0; ww < kNetThreads / 32; ++ww) {
+          const int t = s_w[threadIdx.x][ww];
+          s_w[threadIdx.x][ww] = run;
+          run += t;
+        }
+        s_run[threadIdx.x] = run;
+      }
+      __syncthreads();
+      if (k >= 0) list[s_w[k][w] + rank] = i;
+      __syncthreads();
     }
-    __syncthreads();
-    if (k >= 0) list[s_w[k][w] + rank] = i;
-    __syncthreads();
   }
 }
 
-// One thread per twig of classes 0..4: list[off[0] .. off[5 nb]).
+// One thread per twig of classes 0..4: list[start[0] .. start[5]).
 __global__ void __launch_bounds__(kNetThreads, 4)
     k_net_p2m_thread(const Geom* __restrict__ geom, double theta, double4* node_c,
                      const int8_t* __restrict__ node_level,
                      const int32_t* __restrict__ node_parent, MixedNodes mx, Ensemble ens,
-                     const int32_t* __restrict__ off, int nb,
+                     const int32_t* __restrict__ start,
                      const int32_t* __restrict__ list, int full, int32_t* err) {
-  const int b0 = off[0], b1 = off[5 * nb];
+  const int b0 = start[0], b1 = start[5];
   if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
   for (int k = b0 + blockIdx.x * blockDim.x + threadIdx.x; k < b1; k += gridDim.x * blockDim.x)
     net_p2m<1>(list[k], 0, geom, theta, node_c, node_level, node_parent, mx, ens, full != 0);
 }
 
-// One warp per twig of class 5: list[off[5 nb] .. off[6 nb]).
+// One warp per twig of class 5: list[start[5] .. start[6]).
 __global__ void __launch_bounds__(kNetThreads)
     k_net_p2m_warp(const Geom* __restrict__ geom, double theta, double4* node_c,
                    const int8_t* __restrict__ node_level,
                    const int32_t* __restrict__ node_parent, MixedNodes mx, Ensemble ens,
-                   const int32_t* __restrict__ off, int nb,
+                   const int32_t* __restrict__ start,
                    const int32_t* __restrict__ list, int full, int32_t* err) {
-  const int b0 = off[5 * nb], b1 = off[6 * nb];
+  const int b0 = start[5], b1 = start[6];
   const int lane = threadIdx.x & 31;
   int e = 0;
   if (lane == 0) e = *((volatile int32_t*)err);
@@ -566,14 +622,14 @@ __global__ void __launch_bounds__(kNetThreads)
 // The twigs above kMidCount: a group of 8 lanes per climb start computes its
 // twig from the children, then climbs while it is the last child to arrive
 // at the parent (fence, atomic, fence: the children's records are visible to
-// the group that completes the parent).  list[off[6 nb] .. off[7 nb]).
+// the group that completes the parent).  list[start[6] .. start[7]).
 __global__ void __launch_bounds__(128)
     k_net_top(const Geom* __restrict__ geom, double theta, int cap, double4* node_c,
               const int32_t* __restrict__ node_parent, int32_t* node_done,
               const int8_t* __restrict__ node_level, MixedNodes mx, Ensemble ens,
-              const int32_t* __restrict__ off, int nb, const int32_t* __restrict__ list,
+              const int32_t* __restrict__ start, const int32_t* __restrict__ list,
               int32_t* err) {
-  const int b0 = off[6 * nb], b1 = off[7 * nb];
+  const int b0 = start[6], b1 = start[7];
   const int lane = threadIdx.x & 31, j = lane & 7;
   const unsigned gm = 0xffu << (lane & 24);
   if (*((volatile int32_t*)err) & (kErrCapacity | kErrWalk)) return;
@@ -607,29 +663,31 @@ __global__ void __launch_bounds__(128)
 int net_moments(const BuildBuffers& b, int n, double theta, const Ensemble& ens, bool full,
                 cudaStream_t st) {
   const int T = kNetThreads;
-  const int nb = (b.cap + kNetBlockNodes - 1) / kNetBlockNodes;
-  int32_t* cnt = b.mx.cls;                        // 7 nb class counts
-  int32_t* off = b.mx.cls + net_cls_entries(b.cap);  // their exclusive scan (+ total)
-  k_net_mark<<<nb, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, cnt);
-  int launches = 1 + exclusive_scan(cnt, off, kNetClasses * nb, b.scan_partial, true, st);
-  k_net_fill<<<nb, T, 0, st>>>(b.bounds, b.cap, b.node_pt, b.node_done, b.mx, off,
-                               b.mx.lvl_list);
+  const int NB = (b.cap + kNetBlockNodes - 1) / kNetBlockNodes;
+  int32_t* cnt = b.mx.cls;                  // 7 NB class counts
+  int32_t* off = b.mx.cls + 7 * NB;         // their exclusive scan
+  int32_t* start = b.mx.lvl + 16;           // 8 class starts
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int gblk = NB < 4 * sms ? NB : 4 * sms;
+  k_net_mark<<<gblk, T, 0, st>>>(b.bounds, b.cap, NB, b.node_pt, b.node_done, b.mx, cnt);
+  k_net_scan<<<1, 1024, 0, st>>>(b.bounds, b.cap, NB, cnt, off, start);
+  k_net_fill<<<gblk, T, 0, st>>>(b.bounds, b.cap, NB, b.node_pt, b.node_done, b.mx, off,
+                                 b.mx.lvl_list);
   int g1 = (n / 2 + T - 1) / T;  // at most n - 1 twigs
   if (g1 > sms * 8) g1 = sms * 8;
   if (g1 < 1) g1 = 1;
   k_net_p2m_thread<<<g1, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.node_parent,
-                                     b.mx, ens, off, nb, b.mx.lvl_list, full ? 1 : 0, b.err);
+                                     b.mx, ens, start, b.mx.lvl_list, full ? 1 : 0, b.err);
   int g2 = (n / kSmallCount * 32 + T - 1) / T;
   if (g2 > sms * 8) g2 = sms * 8;
   if (g2 < 1) g2 = 1;
   k_net_p2m_warp<<<g2, T, 0, st>>>(b.geom, theta, b.node_c, b.node_level, b.node_parent,
-                                   b.mx, ens, off, nb, b.mx.lvl_list, full ? 1 : 0, b.err);
+                                   b.mx, ens, start, b.mx.lvl_list, full ? 1 : 0, b.err);
   k_net_top<<<sms, 128, 0, st>>>(b.geom, theta, b.cap, b.node_c, b.node_parent, b.node_done,
-                                 b.node_level, b.mx, ens, off, nb, b.mx.lvl_list, b.err);
-  return launches + 4;
+                                 b.node_level, b.mx, ens, start, b.mx.lvl_list, b.err);
+  return 6;
 }
 
 }  // namespace tg

@@ -881,7 +881,7 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.geom, (size_t)cap);
   rc |= realloc_dev(&mb.lvl_list, (size_t)cap);
-  rc |= realloc_dev(&mb.cls, 2 * (size_t)net_cls_entries(cap));
+  rc |= realloc_dev(&mb.cls, (size_t)net_cls_entries(cap));
   return rc;
 }
 
