@@ -362,8 +362,8 @@ int exclusive_scan(const int32_t* in, int32_t* out, int n, int32_t* partial,
 // ---------------------------------------------------------- radix sort ----
 constexpr int kRsThreads = 256;
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsIters = 16;                       // items per lane
-constexpr int kRsTile = kRsThreads * kRsIters;     // 4096 items per block
+constexpr int kRsIters = 8;                        // items per lane
+constexpr int kRsTile = kRsThreads * kRsIters;     // 2048 items per block
 constexpr int kRsBins = 256;
 
 int radix_blocks(int n) { return (n + kRsTile - 1) / kRsTile; }
@@ -385,7 +385,7 @@ __global__ void k_rs_hist(const K* __restrict__ keys, int n, int shift,
 }
 
 // Stable scatter: tile order is warp-major (warp w owns items
-// [w*512, w*512+512) of the tile), then iteration, then lane.
+// [w*32*kRsIters, (w+1)*32*kRsIters) of the tile), then iteration, then lane.
 template <class K>
 __global__ void __launch_bounds__(kRsThreads)
     k_rs_scatter(const K* __restrict__ keys_in,
@@ -1223,12 +1223,15 @@ int build_trees(const BuildBuffers& b, const double* x, int n, int n_el,
   k_counts<<<gb, T, 0, st>>>(b.L, n, b.cnt);
   launches += 2 + exclusive_scan(b.cnt, b.off, n, b.scan_partial, true, st);
   k_bounds<<<1, 32, 0, st>>>(b.off, n, split, b.cap, b.bounds, b.err);
-  // per-node passes: a fixed grid striding over the device's node count
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int gcap = (b.cap + T - 1) / T;
-  if (gcap > 8 * sms) gcap = 8 * sms;
+  // per-node passes: a grid of one thread per node for trees of up to 2n
+  // nodes (the usual size), striding over the device's node count beyond
+  // (the capacity can be many times the tree after a co-located start).
+  // Blocks run in about index order, so the atomic appends of k_groups come
+  // out in about pre-order: the walk takes target groups in that order, and
+  // neighbouring warps then share the cells they open.
+  const int64_t per_node = b.cap < 2 * (int64_t)n ? b.cap : 2 * (int64_t)n;
+  int gcap = (int)((per_node + T - 1) / T);
+  if (gcap < 1) gcap = 1;
   if (mode == 0) {
     k_topology<<<gb, T, 0, st>>>(b.keys, b.vals, b.L, b.off, n, split, lsb, b.geom,
                                  b.cap, b.node_c, b.node_skip, b.node_pt,
