@@ -275,8 +275,12 @@ def equal_accuracy(points, target=1e-4):
     the opening angle where rms reaches `target` and the time per step there,
     by power laws in theta fitted to the points (an extrapolation when the
     target lies outside them)."""
-    pts = [p for p in points if p[1] and p[1] > 0 and p[2] > 0]
+    pts = sorted(p for p in points if p[1] and p[1] > 0 and p[2] > 0)
     if len(pts) < 2:
+        return None
+    # the fit means something only where the error falls as theta shrinks
+    # over every measured arm
+    if any(b[1] <= a[1] for a, b in zip(pts, pts[1:])):
         return None
     th = [p[0] for p in pts]
     a_e, b_e = power_law(th, [p[1] for p in pts])
@@ -284,6 +288,8 @@ def equal_accuracy(points, target=1e-4):
     if b_e <= 0:
         return None
     theta_t = float(np.exp((np.log(target) - a_e) / b_e))
+    if theta_t < 0.5 * min(th) or theta_t > 2.0 * max(th):
+        return None  # too far outside the measured arms to report
     ms_t = float(np.exp(a_t + b_t * np.log(theta_t)))
     return {"target_rms": target, "theta": theta_t, "ms_per_step": ms_t,
             "rms_exponent": b_e, "time_exponent": b_t,
@@ -576,6 +582,19 @@ def run_ours(args, rank, world, dist):
                     for k, v in compare.items()
                     if k.startswith("fp64_plain_theta") and isinstance(v, dict)]
         eq = equal_accuracy(fp64_pts, 1e-4)
+        if eq is None and fp64_pts:
+            # the plain path does not reach the bar on any arm it can run in
+            # a bench (nor along a usable trend): its most accurate arm gives
+            # a lower bound of the equal-accuracy speed-up
+            best = min((p for p in fp64_pts if p[1]), key=lambda p: p[1], default=None)
+            if best is not None:
+                compare["fp64_plain_most_accurate_arm"] = {
+                    "theta": best[0], "rms_rel_err": best[1], "ms_per_step": best[2],
+                    "headline_over": best[2] / ours_ms,
+                    "note": ("no plain FP64 arm reaches rms 1e-4 and its error does not fall "
+                             "steadily with theta, so no equal-accuracy point is fitted; "
+                             "this arm is still less accurate than the headline, so the "
+                             "ratio is a lower bound")}
         if eq:
             eq["headline_over_fp64_at_equal_accuracy"] = eq["ms_per_step"] / ours_ms
             eq["note"] = ("plain FP64 fixed-theta path: rms error and time per step fitted as "

@@ -28,6 +28,15 @@ def test_equal_accuracy_needs_two_usable_points():
     assert bench.equal_accuracy([(0.5, 1e-3, 100.0), (0.3, 1e-2, 300.0)]) is None
 
 
+def test_equal_accuracy_refuses_nonmonotone_or_far_fits():
+    # the error rises between two of the arms: no trend to follow
+    pts = [(0.5, 1.0e-2, 295.0), (0.35, 1.6e-2, 606.0), (0.25, 5.1e-3, 1293.0)]
+    assert bench.equal_accuracy(pts, 1e-4) is None
+    # a steady trend whose crossing lies far below the smallest arm
+    pts = [(0.5, 1.0e-2, 100.0), (0.25, 9.0e-3, 400.0)]
+    assert bench.equal_accuracy(pts, 1e-4) is None
+
+
 def test_both_arms_describe_the_same_workload():
     import argparse
     args = argparse.Namespace(te=50.0, theta=0.3, physics="kelbg", no_rdf=False, nsamp=10)
