@@ -46,6 +46,10 @@ FLOPS_P2P_REF = 30     # leaf laws of tree.f90 / erf-Kelbg with the x^2>40 short
 FLOPS_M2P_MIXED = {2: 50, 3: 100, 4: 195}  # FP32 trace-free far field to order 2 / 3 / 4
 FLOPS_P2P_MIXED = 24   # FP32 erf-Kelbg pair with hi/lo offsets
 FLOPS_MLP = 2 * (16 * 64 + 64 * 64 + 64)  # one learned-MAC evaluation (BF16 mma + FP32)
+# One far cell summed into a target group's local expansion (local.cuh at
+# order 4: potential and its first to fourth derivatives, ~700 operations of
+# which most are FMA), evaluated once per group instead of once per target.
+FLOPS_LOCAL = 1250
 RDF_BYTES = 2 * 10001 * 8  # the two 64-bit RDF histograms read back per call
 SAMPLE_BYTES = 48          # one TEMPORAL record
 
@@ -54,7 +58,7 @@ SAMPLE_BYTES = 48          # one TEMPORAL record
 # FP64 direct sum stays below 1e-4 at this workload with a margin (7.2e-5 at
 # the state after 25 steps in the tuning sweep; the accuracy audit below,
 # which every run reports, measures it again).
-HEADLINE = dict(theta=0.42, eta=3e-5, order=4, bucket=8)
+HEADLINE = dict(theta=0.42, eta=3e-5, order=4, bucket=8, loc=0.08)
 # Fixed-theta arms beside the learned criterion, per far-field order: the
 # opening angles around the one that meets 1e-4 without the learned test.
 FIXED_ARMS = {2: (0.20, 0.22, 0.25), 3: (0.30, 0.32, 0.35), 4: (0.40, 0.42, 0.45)}
@@ -81,6 +85,9 @@ def parse():
     ap.add_argument("--eta", type=float, default=HEADLINE["eta"])
     ap.add_argument("--order", type=int, default=HEADLINE["order"])
     ap.add_argument("--bucket", type=int, default=HEADLINE["bucket"])
+    ap.add_argument("--loc", type=float, default=HEADLINE["loc"],
+                    help="local expansion of far cells: largest group half-diagonal "
+                         "over cell distance (0 = off)")
     ap.add_argument("--nsamp", type=int, default=10,
                     help="TEMPORAL cadence of the timed loop (Nloop %% nsamp == 0)")
     ap.add_argument("--no-rdf", action="store_true",
@@ -443,6 +450,7 @@ def run_ours(args, rank, world, dist):
     tf.set_stream(stream.cuda_stream)
     if prec == api.PREC_MIXED:
         tf.set_tuning(args.bucket, 4, args.order)
+        tf.set_local_expansion(args.loc)
         if mac == api.MAC_LEARNED:
             from tree_b200 import learned_mac
             params, stats, _ = learned_mac.load_model(order=args.order)
@@ -472,6 +480,7 @@ def run_ours(args, rank, world, dist):
     d_m2p = t_after.n_m2p_total - t_before.n_m2p_total
     d_p2p = t_after.n_p2p_total - t_before.n_p2p_total
     d_net = t_after.n_mac_net_total - t_before.n_mac_net_total
+    d_loc = t_after.n_local_total - t_before.n_local_total
 
     # ---- accuracy audit of the last timed step: FP64 direct sum ----
     audit_idx = None
@@ -513,7 +522,7 @@ def run_ours(args, rank, world, dist):
     fp64 = prec == api.PREC_FP64
     fm2p = FLOPS_M2P_REF if fp64 else FLOPS_M2P_MIXED[args.order]
     fp2p = FLOPS_P2P_REF if fp64 else FLOPS_P2P_MIXED
-    flops = d_m2p * fm2p + d_p2p * fp2p
+    flops = d_m2p * fm2p + d_p2p * fp2p + (0 if fp64 else d_loc * FLOPS_LOCAL)
     achieved = flops / (walk_ms_sum / 1e3) / 1e12 if walk_ms_sum > 0 else 0.0
     sm_mhz = clk.get("sm_mhz") or 1965.0
     peak = fp_peak_tflops(sm_mhz, fp64)
@@ -529,7 +538,8 @@ def run_ours(args, rank, world, dist):
                 "flops_per_launch": flops / args.steps, "walk_ms": walk_ms,
                 "n_m2p_per_launch": d_m2p / args.steps, "n_p2p_per_launch": d_p2p / args.steps,
                 "counts": f"interactions summed over the {args.steps} timed walks",
-                "flops_per_m2p": fm2p, "flops_per_p2p": fp2p,
+                "n_local_cells_per_launch": d_loc / args.steps,
+                "flops_per_m2p": fm2p, "flops_per_p2p": fp2p, "flops_per_local_cell": FLOPS_LOCAL,
                 "learned_mac_evals_per_launch": d_net / args.steps,
                 "learned_mac_tensor_tflops": d_net * FLOPS_MLP / (walk_ms_sum / 1e3) / 1e12
                 if walk_ms_sum > 0 else 0.0}
@@ -561,6 +571,7 @@ def run_ours(args, rank, world, dist):
                 tc.set_stream(stream.cuda_stream)
                 if aprec == api.PREC_MIXED:
                     tc.set_tuning(args.bucket, 4, args.order)
+                    tc.set_local_expansion(args.loc)
                 tc.load_state(st_warm["x_el"], st_warm["v_el"], st_warm["f_el"],
                               st_warm["x_ion"], st_warm["v_ion"], st_warm["f_ion"])
                 tb = tc.timings()
@@ -574,6 +585,7 @@ def run_ours(args, rank, world, dist):
                                  "rms_rel_err": acc_c and acc_c["rms_rel_err"],
                                  "max_rel_err": acc_c and acc_c["max_rel_err"],
                                  "n_m2p_per_step": (ta.n_m2p_total - tb.n_m2p_total) / ksteps,
+                                 "n_local_cells_per_step": (ta.n_local_total - tb.n_local_total) / ksteps,
                                  "n_p2p_per_step": (ta.n_p2p_total - tb.n_p2p_total) / ksteps}
         ours_ms = ms / args.steps
         compare["headline_over_fp64_plain_theta0.5"] = (
@@ -638,6 +650,7 @@ def run_ours(args, rank, world, dist):
                    "mac": "learned" if mac == api.MAC_LEARNED else "fixed",
                    "eta": args.eta if mac == api.MAC_LEARNED else None,
                    "order": args.order, "bucket": args.bucket,
+                   "local_expansion": args.loc if not fp64 else None,
                    "loop": "tree_gpu_run: CUDA-graph replay of the step body"},
         "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "clocks": clk, "e2e": e2e, "gpu_launches": launches,

@@ -96,6 +96,8 @@ typedef struct tree_gpu_timing {
   int64_t n_m2p_total;     /* accepted cells summed over every walk of the handle */
   int64_t n_p2p_total;     /* pair evaluations summed over every walk */
   int64_t n_mac_net_total; /* learned-MAC evaluations summed over every walk */
+  int64_t n_local;         /* cells summed into target groups' local expansions, last call */
+  int64_t n_local_total;   /* the same, summed over every walk */
 } tree_gpu_timing;
 
 typedef struct tree_gpu_handle tree_gpu_handle;
@@ -268,6 +270,19 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
  * No counterpart in the reference; chosen by the autotuner (tree_b200/tune.py). */
 int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
                         int32_t blocks_per_sm, int32_t order);
+
+/* Local expansions of far cells in the mixed-precision walk.  An accepted
+ * cell far from a target group (32 targets at most) is expanded once about
+ * the group's centre to second order in the force (value, gradient, second
+ * and third derivatives of its potential) instead of being evaluated at every
+ * target; the group sums these expansions and each target evaluates the sum
+ * once.  A cell is far when h/d <= max_ratio, h the group's half-diagonal and
+ * d the distance from the group's centre to the cell's centroid; the added
+ * force error is of order (h/d)^3 of that cell's field.  Default 0.08;
+ * 0 evaluates every accepted cell at every target; at most 0.5.  No
+ * counterpart in the reference, whose walks evaluate every accepted cell per
+ * target (tree.f90:744-779). */
+int tree_gpu_set_local_expansion(tree_gpu_handle* h, double max_ratio);
 
 /* ---- learned multipole acceptance criterion (no counterpart in the
  * reference, whose criterion is the fixed s/theta + dx < r of tree.f90:743).

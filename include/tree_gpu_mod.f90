@@ -51,7 +51,7 @@ MODULE TREE_GPU_MOD
      REAL(C_DOUBLE) :: ms_build, ms_walk, ms_kdk, ms_total
      INTEGER(C_INT64_T) :: n_m2p, n_p2p, n_nodes, calls, launches, &
           n_mac_net, n_mac_fallback, n_m2p_total, n_p2p_total, &
-          n_mac_net_total
+          n_mac_net_total, n_local, n_local_total
   END TYPE tree_gpu_timing
 
   INTERFACE
@@ -175,6 +175,12 @@ MODULE TREE_GPU_MOD
        IMPORT :: C_INT, C_PTR, C_INT32_T
        TYPE(C_PTR), VALUE :: h
        INTEGER(C_INT32_T), VALUE :: bucket, blocks_per_sm, order
+     END FUNCTION
+
+     INTEGER(C_INT) FUNCTION tree_gpu_set_local_expansion(h, max_ratio) BIND(C)
+       IMPORT :: C_INT, C_PTR, C_DOUBLE
+       TYPE(C_PTR), VALUE :: h
+       REAL(C_DOUBLE), VALUE :: max_ratio
      END FUNCTION
 
      INTEGER(C_INT) FUNCTION tree_gpu_mac_collect(h, theta_lo, theta_hi, rho_lo, &

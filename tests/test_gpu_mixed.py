@@ -207,3 +207,38 @@ def test_hexadecapole_more_accurate_than_octupole(device_lib, theta):
             fd, _ = tf.direct(t)
         rms[order] = float(np.sqrt(np.mean(_rel(np.vstack([f_el, f_ion])[t], fd) ** 2)))
     assert rms[4] < 0.7 * rms[3], rms
+
+
+def test_local_expansion_of_far_cells(device_lib):
+    """Accepted cells far from a target group are summed into the group's
+    local expansion instead of being evaluated per target: a large share of
+    the far field moves there while the error against the direct sum, the
+    forces and the potential energy stay where they were."""
+    n = 262144
+    xe, xi = _displaced(n, 21, shift=1.0)
+    rng = np.random.default_rng(4)
+    t = np.sort(rng.choice(n, 8192, replace=False))
+    out = {}
+    fd = None
+    for eps in (0.0, 0.08):
+        with api.TreeForce(len(xe), len(xi), _mixed(0.42)) as tf:
+            tf.set_tuning(8, 4, 4)
+            tf.set_local_expansion(eps)
+            f_el, f_ion, ee, ei = tf.force(xe, xi)
+            tm = tf.timings()
+            if fd is None:
+                fd, _ = tf.direct(t)
+        f = np.vstack([f_el, f_ion])
+        out[eps] = (f, ee + ei, tm.n_m2p, tm.n_local, np.sqrt(np.mean(_rel(f[t], fd) ** 2)))
+    f0, e0, m2p0, loc0, rms0 = out[0.0]
+    f1, e1, m2p1, loc1, rms1 = out[0.08]
+    assert loc0 == 0 and loc1 > 0
+    # per-target far-field evaluations fall by a fifth or more
+    assert m2p1 < 0.8 * m2p0
+    assert rms1 < 1.1 * rms0 + 2e-6 and rms1 < 1e-4, (rms0, rms1)
+    d = _rel(f1, f0)
+    assert np.sqrt(np.mean(d**2)) < 3e-5 and d.max() < 2e-3
+    assert e1 == pytest.approx(e0, rel=1e-5)
+    with api.TreeForce(8, 8, _mixed(0.5)) as tf:
+        with pytest.raises(api.TreeGpuError):
+            tf.set_local_expansion(0.6)

@@ -33,6 +33,7 @@ EXPORTS = ("tree_gpu_create", "tree_gpu_set_params", "tree_gpu_force",
            "tree_gpu_run", "tree_gpu_set_graphs", "tree_gpu_get_nloop",
            "tree_gpu_get_state", "tree_gpu_direct", "tree_gpu_direct_static",
            "tree_gpu_tree_dump", "tree_gpu_net_dump", "tree_gpu_set_stream", "tree_gpu_set_tuning",
+           "tree_gpu_set_local_expansion",
            "tree_gpu_mac_collect", "tree_gpu_mac_samples", "tree_gpu_mac_clear",
            "tree_gpu_mac_train", "tree_gpu_mac_set_model",
            "tree_gpu_mac_get_model", "tree_gpu_mac_config", "tree_gpu_mlp_grad",
@@ -73,7 +74,8 @@ class Timing(ctypes.Structure):
                 ("n_nodes", ctypes.c_int64), ("calls", ctypes.c_int64),
                 ("launches", ctypes.c_int64), ("n_mac_net", ctypes.c_int64),
                 ("n_mac_fallback", ctypes.c_int64), ("n_m2p_total", ctypes.c_int64),
-                ("n_p2p_total", ctypes.c_int64), ("n_mac_net_total", ctypes.c_int64)]
+                ("n_p2p_total", ctypes.c_int64), ("n_mac_net_total", ctypes.c_int64),
+                ("n_local", ctypes.c_int64), ("n_local_total", ctypes.c_int64)]
 
 
 class TreeGpuError(RuntimeError):
@@ -119,6 +121,7 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.c_int64, vp, vp, vp]
     L.tree_gpu_set_stream.argtypes = [vp, vp]
     L.tree_gpu_set_tuning.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    L.tree_gpu_set_local_expansion.argtypes = [vp, ctypes.c_double]
     fp = ctypes.POINTER(ctypes.c_float)
     L.tree_gpu_mac_collect.argtypes = [vp, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_double,
@@ -400,6 +403,12 @@ class TreeForce:
 
     def set_tuning(self, bucket: int = 8, blocks_per_sm: int = 4, order: int = 3):
         self._check(self.lib.tree_gpu_set_tuning(self.h, bucket, blocks_per_sm, order))
+
+    def set_local_expansion(self, max_ratio: float = 0.08):
+        """Accepted cells with (group half-diagonal) / (distance to the cell's
+        centroid) <= max_ratio are summed into each target group's local
+        expansion instead of being evaluated per target; 0 turns it off."""
+        self._check(self.lib.tree_gpu_set_local_expansion(self.h, max_ratio))
 
     # ---- learned MAC ----
     def mac_collect(self, theta_lo=0.2, theta_hi=0.9, rho_lo=0.05, rho_hi=0.9,

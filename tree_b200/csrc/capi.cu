@@ -204,9 +204,10 @@ int alloc_all(tree_gpu_handle* h) {
   if ((rc = dalloc(h, &b.bounds, 5))) return rc;
   if ((rc = dalloc(h, &b.err, 1))) return rc;
   if ((rc = dalloc(h, &h->rdf, 2 * (size_t)tg::kRdfBins))) return rc;
-  if ((rc = dalloc(h, &h->counters, 8))) return rc;
-  // [0..3] this step's walk counts, [4..7] running totals of the handle
-  if (cudaMemset(h->counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess)
+  if ((rc = dalloc(h, &h->counters, 16))) return rc;
+  // [0..3] this step's walk counts, [4..7] running totals of the handle,
+  // [8] this step's cells in local expansions, [9] their running total
+  if (cudaMemset(h->counters, 0, 16 * sizeof(unsigned long long)) != cudaSuccess)
     return fail(h, TREE_GPU_ERR_CUDA, "counter initialisation failed");
   if ((rc = dalloc(h, &h->partial, 4 * (size_t)tg::kdk_partials_needed(n) + 4)))
     return rc;
@@ -284,6 +285,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
       tg::build_trees(h->b, h->x, h->n, (int)h->n_el, h->prm.theta, mode, st);
   if (ev) record(h, ev->e[1]);
   cudaMemsetAsync(h->counters, 0, 4 * sizeof(unsigned long long), st);
+  cudaMemsetAsync(h->counters + 8, 0, sizeof(unsigned long long), st);
   if (with_rdf)
     cudaMemsetAsync(h->rdf, 0, 2 * sizeof(uint32_t) * tg::kRdfBins, st);
   tg::TreeView tv = tree_view(h);
@@ -349,7 +351,7 @@ int grow_nodes(tree_gpu_handle* h) {
 }
 
 void read_counters(tree_gpu_handle* h) {
-  unsigned long long c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long c[16] = {};
   cudaMemcpy(c, h->counters, sizeof(c), cudaMemcpyDeviceToHost);
   h->timing.n_m2p = (int64_t)c[0];
   h->timing.n_p2p = (int64_t)c[1];
@@ -358,6 +360,8 @@ void read_counters(tree_gpu_handle* h) {
   h->timing.n_m2p_total = (int64_t)c[4];
   h->timing.n_p2p_total = (int64_t)c[5];
   h->timing.n_mac_net_total = (int64_t)c[6];
+  h->timing.n_local = (int64_t)c[8];
+  h->timing.n_local_total = (int64_t)c[9];
 }
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
@@ -1035,6 +1039,15 @@ int tree_gpu_set_tuning(tree_gpu_handle* h, int32_t bucket,
   h->tune.bucket = bucket;
   h->tune.blocks_per_sm = blocks_per_sm;
   h->tune.order = order;
+  ++h->epoch;
+  return TREE_GPU_OK;
+}
+
+int tree_gpu_set_local_expansion(tree_gpu_handle* h, double max_ratio) {
+  if (!h) return TREE_GPU_ERR_ARG;
+  if (!(max_ratio >= 0.0 && max_ratio <= 0.5))
+    return fail(h, TREE_GPU_ERR_ARG, "max_ratio must be in [0, 0.5]");
+  h->tune.loc_eps = (float)max_ratio;
   ++h->epoch;
   return TREE_GPU_OK;
 }

@@ -104,8 +104,8 @@ __global__ void __launch_bounds__(kKdkThreads)
 }
 
 // Sums rows of `partial` (nb x 4) in fixed order into out[0..3].  With cnt
-// (the walk's interaction counters of this step in cnt[0..3]), also adds
-// them to the running totals cnt[4..7].
+// (the walk's interaction counters of this step in cnt[0..3] and cnt[8]),
+// also adds them to the running totals cnt[4..7] and cnt[9].
 __global__ void k_sum_partials4(const double* __restrict__ partial, int nb,
                                 double* out, unsigned long long* cnt = nullptr) {
   __shared__ double sh[kKdkThreads];
@@ -122,6 +122,7 @@ __global__ void k_sum_partials4(const double* __restrict__ partial, int nb,
     __syncthreads();
   }
   if (cnt && threadIdx.x < 4) cnt[4 + threadIdx.x] += cnt[threadIdx.x];
+  if (cnt && threadIdx.x == 4) cnt[9] += cnt[8];
 }
 
 // Potential energy: epot_part[i] = (contribution to Epot_e, to Epot_i).

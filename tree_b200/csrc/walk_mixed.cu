@@ -27,6 +27,7 @@
 // charge nearly cancels.  Near field: erf-Kelbg (or the reference laws) for
 // every particle pair.
 #include <cstdio>
+#include "local.cuh"
 #include "mac.cuh"
 #include "walk_mixed.h"
 
@@ -36,6 +37,8 @@ constexpr int kMxWarps = 8;
 constexpr int kMxThreads = 32 * kMxWarps;
 constexpr int kStackCap = 8192;   // node indices per warp
 constexpr int kM2pRing = 64;      // power of two, > 31 + 32
+constexpr int kLocRing = 64;      // power of two, > 31 + 32
+constexpr int kLocStride = kLocCoef | 1;  // odd row stride of the coefficient rows
 constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
 constexpr int kMaxBucket = 8;
 constexpr int kMaxBlocksPerSm = 4;
@@ -51,6 +54,7 @@ constexpr int kPartF4 = 5;        // float4 per staged source pair (4 used + pad
 
 struct WarpSmem {
   int m2p[kM2pRing];
+  int loc[kLocRing];       // far cells summed into the group's local expansion
   int p2p[kP2pRing];
   int cq_node[kCandRing];  // learned-MAC candidates waiting for a full batch
   float cq_d[kCandRing];
@@ -69,10 +73,14 @@ struct WarpSmem {
     // (nlz nlz' idx idx'): negated hi / lo offsets from the group centre,
     // charge, sorted index bits
     float4 part[16 * kPartF4];
+    // local-expansion coefficients of up to 32 cells, one row per lane
+    // (odd stride: conflict-free rows and columns)
+    float loc_rows[32 * kLocStride];
   };
   // pair constants of the group's cloud: 1/lambda^2 (ee, ei, ii), 1/rs,
   // 1/lambda (ee, ei, ii)
   float pk[8];
+  double hl2;  // the group's squared half-diagonal (local-expansion test)
 };
 
 struct MixedArgs {
@@ -91,6 +99,10 @@ struct MixedArgs {
   int32_t* stack;
   int bucket;
   int p2p_max;  // accepted cells with at most this many particles go to P2P
+  // accepted cells far from the group go to its local expansion: h / d <=
+  // loc_eps, h the group's half-diagonal, d the distance from its centre to
+  // the cell's centroid; loc_eps = 0: never
+  double loc_eps2;
   int physics;
   float inv_lam2_ee, inv_lam2_ei, inv_lam2_ii;
   float inv_lam_ee, inv_lam_ei, inv_lam_ii;
@@ -294,6 +306,53 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
   kahan_add(acc.sz, acc.cz, fz);
   acc.phi_all += (double)pa;
   acc.phi_ion += (double)pi;
+}
+
+// -------------------------------------------------------------- local ----
+// Up to 32 far cells, one per lane: each lane expands its cell's field about
+// the group centre G (local.cuh) into its row of `loc_rows`; lanes 0..28 then
+// add one coefficient each over the rows to their running sum `lsum`.  The
+// group's targets evaluate the summed expansion once, after the walk.
+template <int ORDER>
+__device__ __forceinline__ void eval_local(WarpSmem& sm, int head, int cnt,
+                                           const MixedArgs& a, double Gx, double Gy,
+                                           double Gz, int lane, float& lsum) {
+  constexpr int kStride = kLocStride;
+  if (lane < cnt) {
+    const int node = sm.loc[(head + lane) & (kLocRing - 1)];
+    const double4 c = ldg_d4(&a.node_c[node]);
+    CellMoments m;
+    const float4* mp = a.mom + 3 * (int64_t)node;
+    const float4 m0 = __ldg(mp), m1 = __ldg(mp + 1), m2 = __ldg(mp + 2);
+    m.q = m0.x;
+    m.d[0] = m0.y; m.d[1] = m0.z; m.d[2] = m0.w;
+    m.s[0] = m1.x; m.s[1] = m1.y; m.s[2] = m1.z; m.s[3] = m1.w;
+    m.s[4] = m2.x; m.s[5] = m2.y;
+    m.q_ion = m2.w;
+    if (ORDER >= 3) {
+      const float4* tp = a.mom3 + 3 * (int64_t)node;
+      const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+      m.t[0] = t0.x; m.t[1] = t0.y; m.t[2] = t0.z; m.t[3] = t0.w;
+      m.t[4] = t1.x; m.t[5] = t1.y; m.t[6] = t1.z; m.t[7] = t1.w;
+      m.t[8] = t2.x; m.t[9] = t2.y;
+    }
+    if (ORDER >= 4) {
+      const float4* hp = a.mom4 + 3 * (int64_t)node;
+      const float4 h0 = __ldg(hp), h1 = __ldg(hp + 1), h2 = __ldg(hp + 2);
+      m.h[0] = h0.x; m.h[1] = h0.y; m.h[2] = h0.z; m.h[3] = h0.w;
+      m.h[4] = h1.x; m.h[5] = h1.y; m.h[6] = h1.z; m.h[7] = h1.w;
+      m.h[8] = h2.x; m.h[9] = h2.y; m.h[10] = h2.z; m.h[11] = h2.w;
+    }
+    local_coefs<ORDER>((float)(Gx - c.x), (float)(Gy - c.y), (float)(Gz - c.z), m,
+                       sm.loc_rows + kStride * lane);
+  }
+  __syncwarp();
+  if (lane < kLocCoef) {
+    float t = 0.f;
+    for (int k = 0; k < cnt; ++k) t += sm.loc_rows[kStride * k + lane];
+    lsum += t;
+  }
+  __syncwarp();
 }
 
 // ---------------------------------------------------------------- P2P ----
@@ -590,7 +649,9 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
                 tlz = (float)(rtz - (double)thz);
     // pairs closer than h / sqrt(32) (h the group's half-diagonal) take the
     // exact offsets (eval_p2p)
-    const float close2 = (float)((hx * hx + hy * hy + hz * hz) * (1.0 / 32.0));
+    const double hl2 = hx * hx + hy * hy + hz * hz;
+    const float close2 = (float)(hl2 * (1.0 / 32.0));
+    if (lane == 0) sm.hl2 = hl2;
     Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
     // error budget of the learned MAC: eta * min |F_prev| / eps over the group
     float budget = 0.f, hlen = 0.f;
@@ -632,7 +693,8 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
     if (lane == 0) stack[0] = root;
     __syncwarp();
     int m2h = 0, m2t = 0, p2h = 0, p2t = 0;  // ring heads/tails (warp-uniform)
-    long long n_m2p = 0, n_p2p = 0;
+    int lch = 0, lct = 0;                    // local-expansion ring
+    float lsum = 0.f;  // lanes 0..19: one summed coefficient of the local expansion
     unsigned n_mlp = 0, n_fallback = 0;  // per lane: cells this lane sent to the MLP
     bool overflow = false;
     int cqh = 0, cqt = 0;  // learned-MAC candidate ring (warp-uniform)
@@ -736,6 +798,12 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
               pcnt = cnt;
             } else if (accept) {
               action = 1;
+              if (a.loc_eps2 > 0.0) {
+                // far from the group: summed into its local expansion
+                const double ux = c.x - Gx, uy = c.y - Gy, uz = c.z - Gz;
+                const double dc2 = ux * ux + uy * uy + uz * uz;
+                if (sm.hl2 <= a.loc_eps2 * dc2) action = 4;
+              }
             } else if (!cand) {
               if (cnt <= a.bucket) {
                 action = 2;
@@ -762,6 +830,10 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       const unsigned bm = __ballot_sync(0xffffffffu, action == 1);
       if (action == 1) sm.m2p[(m2t + __popc(bm & lt)) & (kM2pRing - 1)] = node;
       m2t += __popc(bm);
+      // local-expansion entries
+      const unsigned lm = __ballot_sync(0xffffffffu, action == 4);
+      if (action == 4) sm.loc[(lct + __popc(lm & lt)) & (kLocRing - 1)] = node;
+      lct += __popc(lm);
       // particle entries
       int ptot;
       const int pex = warp_excl_scan(action == 2 ? pcnt : 0, lane, &ptot);
@@ -799,12 +871,14 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
         eval_p2p<PHYS, RDF>(sm, p2h, 32, a, Gx, Gy, Gz, thx, thy, thz, tlx, tly,
                             tlz, close2, pt, tsp, act, lane, hist, acc);
         p2h += 32;
-        n_p2p += 32;
       }
       while (m2t - m2h >= 32) {
         eval_m2p<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
         m2h += 32;
-        n_m2p += 32;
+      }
+      while (lct - lch >= 32) {
+        eval_local<ORDER>(sm, lch, 32, a, Gx, Gy, Gz, lane, lsum);
+        lch += 32;
       }
     }
     if (overflow) {
@@ -814,11 +888,25 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
     if (p2t > p2h) {
       eval_p2p<PHYS, RDF>(sm, p2h, p2t - p2h, a, Gx, Gy, Gz, thx, thy, thz, tlx,
                           tly, tlz, close2, pt, tsp, act, lane, hist, acc);
-      n_p2p += p2t - p2h;
     }
     if (m2t > m2h) {
       eval_m2p<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
-      n_m2p += m2t - m2h;
+    }
+    if (lct > lch) {
+      eval_local<ORDER>(sm, lch, lct - lch, a, Gx, Gy, Gz, lane, lsum);
+    }
+    if (lct > 0) {
+      // every target evaluates the group's summed local expansion
+      if (lane < kLocCoef) sm.loc_rows[lane] = lsum;
+      __syncwarp();
+      float lfx, lfy, lfz, lph, lpi;
+      local_eval(sm.loc_rows, thx, thy, thz, lfx, lfy, lfz, lph, lpi);
+      __syncwarp();
+      kahan_add(acc.sx, acc.cx, lfx);
+      kahan_add(acc.sy, acc.cy, lfy);
+      kahan_add(acc.sz, acc.cz, lfz);
+      acc.phi_all += (double)lph;
+      acc.phi_ion += (double)lpi;
     }
     if (act) {
       const double sc = tsp ? kEps : -kEps;  // eps * target charge
@@ -833,8 +921,10 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
                            : make_double2(all, 0.0);
     }
     if (lane == 0) {
-      atomicAdd(&a.counters[0], (unsigned long long)(n_m2p * n_act));
-      atomicAdd(&a.counters[1], (unsigned long long)(n_p2p * n_act));
+      // every queued entry was evaluated: the ring tails are the counts
+      atomicAdd(&a.counters[0], (unsigned long long)m2t * n_act);
+      atomicAdd(&a.counters[1], (unsigned long long)p2t * n_act);
+      if (lct > 0) atomicAdd(&a.counters[8], (unsigned long long)lct);
     }
     if (LEARNED) {
       unsigned long long m = n_mlp, fb = n_fallback;
@@ -957,6 +1047,7 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   // an octupole M2P costs ~110 flop, a quadrupole one ~60, a pair ~24
   a.p2p_max = tune.order >= 3 ? 4 : 2;
   if (a.p2p_max > a.bucket) a.p2p_max = a.bucket;
+  a.loc_eps2 = (double)tune.loc_eps * tune.loc_eps;
   a.physics = wp.physics;
   a.inv_lam2_ee = (float)(1.0 / (wp.lam_ee * wp.lam_ee));
   a.inv_lam2_ei = (float)(1.0 / (wp.lam_ei * wp.lam_ei));
