@@ -308,6 +308,191 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
   acc.phi_ion += (double)pi;
 }
 
+// The same far field two cells at a time on the packed FP32 (f32x2) pipeline:
+// cells 2b and 2b+1 are staged side by side, so one 16-byte shared load gives
+// two float2 operands and every multiply-add serves both cells.  Used where
+// the walk runs with 128 registers per thread (the RDF layout: one 16-warp
+// block per SM), which holds the doubled live state without spills.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+template <int ORDER>
+__device__ __forceinline__ void eval_m2p_x2(WarpSmem& sm, int head, int cnt,
+                                            const MixedArgs& a, double Gx, double Gy,
+                                            double Gz, float tx, float ty, float tz,
+                                            int lane, Acc& acc) {
+  constexpr int kRows = ORDER >= 4 ? 9 : (ORDER == 3 ? 6 : 4);
+  {
+    // this lane's cell as kRows float4 rows (the layout of eval_m2p), or a
+    // chargeless dummy far away past cnt
+    float4 r[kRows];
+    if (lane < cnt) {
+      const int node = sm.m2p[(head + lane) & (kM2pRing - 1)];
+      const double4 c = ldg_d4(&a.node_c[node]);
+      const float4* mp = a.mom + 3 * (int64_t)node;
+      const float4 m0 = __ldg(mp), m1 = __ldg(mp + 1), m2 = __ldg(mp + 2);
+      r[0] = make_float4((float)(c.x - Gx), (float)(c.y - Gy), (float)(c.z - Gz), m0.x);
+      r[1] = make_float4(m0.y, m0.z, m0.w, m2.w);
+      r[2] = m1;
+      if (ORDER >= 3) {
+        const float4* tp = a.mom3 + 3 * (int64_t)node;
+        const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+        r[3] = make_float4(m2.x, m2.y, t0.x, t0.y);
+        r[4] = make_float4(t0.z, t0.w, t1.x, t1.y);
+        r[5] = make_float4(t1.z, t1.w, t2.x, t2.y);
+      } else {
+        r[3] = make_float4(m2.x, m2.y, 0.f, 0.f);
+      }
+      if (ORDER >= 4) {
+        const float4* hp = a.mom4 + 3 * (int64_t)node;
+        r[6] = __ldg(hp);
+        r[7] = __ldg(hp + 1);
+        r[8] = __ldg(hp + 2);
+      }
+    } else {
+      r[0] = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);
+#pragma unroll
+      for (int j = 1; j < kRows; ++j) r[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // pair block b = lane / 2: row j of both cells as (x x' y y') (z z' w w');
+    // the even lane writes the first float4, the odd lane the second
+    const bool odd = lane & 1;
+    float4* blk = sm.cell + 2 * kCellF4 * (lane >> 1);
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      const float s0 = odd ? r[j].x : r[j].z, s1 = odd ? r[j].y : r[j].w;
+      const float p0 = __shfl_xor_sync(0xffffffffu, s0, 1);
+      const float p1 = __shfl_xor_sync(0xffffffffu, s1, 1);
+      blk[2 * j + (odd ? 1 : 0)] = odd ? make_float4(p0, r[j].z, p1, r[j].w)
+                                       : make_float4(r[j].x, p0, r[j].y, p1);
+    }
+  }
+  __syncwarp();
+  const float2 tx2 = f2(tx), ty2 = f2(ty), tz2 = f2(tz);
+  float2 fx = f2(0.f), fy = fx, fz = fx, pa = fx, pi = fx;
+  const int npair = (cnt + 1) >> 1;
+#pragma unroll 1
+  for (int b = 0; b < npair; ++b) {
+    const float4* bl = sm.cell + 2 * kCellF4 * b;
+    float4 q = bl[0];
+    const float2 Ax = make_float2(q.x, q.y), Ay = make_float2(q.z, q.w);
+    q = bl[1];
+    const float2 Az = make_float2(q.x, q.y), Q = make_float2(q.z, q.w);
+    q = bl[2];
+    const float2 Dx = make_float2(q.x, q.y), Dy = make_float2(q.z, q.w);
+    q = bl[3];
+    const float2 Dz = make_float2(q.x, q.y), Qi = make_float2(q.z, q.w);
+    q = bl[4];
+    const float2 Sxx = make_float2(q.x, q.y), Syy = make_float2(q.z, q.w);
+    q = bl[5];
+    const float2 Szz = make_float2(q.x, q.y), Sxy = make_float2(q.z, q.w);
+    q = bl[6];
+    const float2 Syz = make_float2(q.x, q.y), Szx = make_float2(q.z, q.w);
+    const float2 dx = add2(tx2, make_float2(-Ax.x, -Ax.y));
+    const float2 dy = add2(ty2, make_float2(-Ay.x, -Ay.y));
+    const float2 dz = add2(tz2, make_float2(-Az.x, -Az.y));
+    const float2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, f2(1e-30f))));
+    const float2 s = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 s2 = mul2(s, s);
+    const float2 nx = mul2(dx, s), ny = mul2(dy, s), nz = mul2(dz, s);
+    const float2 Sx = fma2(Sxx, nx, fma2(Sxy, ny, mul2(Szx, nz)));
+    const float2 Sy = fma2(Sxy, nx, fma2(Syy, ny, mul2(Syz, nz)));
+    const float2 Sz = fma2(Szx, nx, fma2(Syz, ny, mul2(Szz, nz)));
+    const float2 u = fma2(nx, Sx, fma2(ny, Sy, mul2(nz, Sz)));
+    const float2 Dn = fma2(Dx, nx, fma2(Dy, ny, mul2(Dz, nz)));
+    const float2 su = mul2(s, u);
+    float2 gp = fma2(s, fma2(f2(15.f), su, mul2(f2(3.f), Dn)), Q);
+    float2 php = fma2(s, fma2(f2(3.f), su, Dn), Q);
+    const float2 c5 = mul2(f2(-6.f), s2);
+    const float2 ms = make_float2(-s.x, -s.y);
+    float2 gx = fma2(c5, Sx, mul2(ms, Dx));
+    float2 gy = fma2(c5, Sy, mul2(ms, Dy));
+    float2 gz = fma2(c5, Sz, mul2(ms, Dz));
+    if (ORDER >= 3) {
+      // (Syz Szx Txxx Tyyy) (Tzzz Txxy Txxz Txyy) (Tyyz Txzz Tyzz Txyz)
+      q = bl[7];
+      const float2 Txxx = make_float2(q.x, q.y), Tyyy = make_float2(q.z, q.w);
+      q = bl[8];
+      const float2 Txxy = make_float2(q.z, q.w);
+      q = bl[9];
+      const float2 Txxz = make_float2(q.x, q.y), Txyy = make_float2(q.z, q.w);
+      q = bl[10];
+      const float2 Tyyz = make_float2(q.x, q.y), Txzz = make_float2(q.z, q.w);
+      q = bl[11];
+      const float2 Tyzz = make_float2(q.x, q.y), Txyz = make_float2(q.z, q.w);
+      const float2 zz = mul2(nz, nz);
+      const float2 mzz = make_float2(-zz.x, -zz.y);
+      const float2 a2 = fma2(nx, nx, mzz), b2 = fma2(ny, ny, mzz);
+      const float2 x2 = add2(nx, nx), y2 = add2(ny, ny);
+      const float2 xy2 = mul2(x2, ny), xz2 = mul2(x2, nz), yz2 = mul2(y2, nz);
+      const float2 Tx = fma2(Txxx, a2, fma2(Txyy, b2, fma2(Txxy, xy2, fma2(Txxz, xz2, mul2(Txyz, yz2)))));
+      const float2 Ty = fma2(Txxy, a2, fma2(Tyyy, b2, fma2(Txyy, xy2, fma2(Txyz, xz2, mul2(Tyyz, yz2)))));
+      const float2 Tz = fma2(Txxz, a2, fma2(Tyyz, b2, fma2(Txyz, xy2, fma2(Txzz, xz2, mul2(Tyzz, yz2)))));
+      const float2 T3 = fma2(nx, Tx, fma2(ny, Ty, mul2(nz, Tz)));
+      const float2 s3T3 = mul2(mul2(s2, s), T3);
+      gp = fma2(f2(17.5f), s3T3, gp);
+      php = fma2(f2(2.5f), s3T3, php);
+      const float2 c7 = mul2(f2(-7.5f), mul2(s2, s));
+      gx = fma2(c7, Tx, gx);
+      gy = fma2(c7, Ty, gy);
+      gz = fma2(c7, Tz, gz);
+    }
+    if (ORDER >= 4) {
+      // (xxxx xxxy xxxz xxyy) (xxyz xyyy xyyz yyyy) (yyyz xxzz xyzz yyzz)
+      q = bl[12];
+      const float2 H0 = make_float2(q.x, q.y), H1 = make_float2(q.z, q.w);
+      q = bl[13];
+      const float2 H2 = make_float2(q.x, q.y), H3 = make_float2(q.z, q.w);
+      q = bl[14];
+      const float2 H4 = make_float2(q.x, q.y), H5 = make_float2(q.z, q.w);
+      q = bl[15];
+      const float2 H6 = make_float2(q.x, q.y), H7 = make_float2(q.z, q.w);
+      q = bl[16];
+      const float2 H8 = make_float2(q.x, q.y), H9 = make_float2(q.z, q.w);
+      q = bl[17];
+      const float2 H10 = make_float2(q.x, q.y), H11 = make_float2(q.z, q.w);
+      const float2 xx = mul2(nx, nx), yy = mul2(ny, ny);
+      const float2 zz3 = mul2(f2(3.f), mul2(nz, nz));
+      const float2 mnz = make_float2(-nz.x, -nz.y);
+      const float2 P1 = mul2(nx, add2(xx, make_float2(-zz3.x, -zz3.y)));
+      const float2 P6 = mul2(ny, add2(yy, make_float2(-zz3.x, -zz3.y)));
+      const float2 P2 = mul2(mul2(f2(3.f), ny), fma2(nz, mnz, xx));
+      const float2 P4 = mul2(mul2(f2(3.f), nx), fma2(nz, mnz, yy));
+      const float2 P3 = mul2(nz, fma2(f2(3.f), xx, mul2(mnz, nz)));
+      const float2 P7 = mul2(nz, fma2(f2(3.f), yy, mul2(mnz, nz)));
+      const float2 P5 = mul2(mul2(f2(6.f), nx), mul2(ny, nz));
+      const float2 Vx = fma2(H0, P1, fma2(H1, P2, fma2(H2, P3, fma2(H3, P4,
+                        fma2(H4, P5, fma2(H5, P6, mul2(H6, P7)))))));
+      const float2 Vy = fma2(H1, P1, fma2(H3, P2, fma2(H4, P3, fma2(H5, P4,
+                        fma2(H6, P5, fma2(H7, P6, mul2(H8, P7)))))));
+      const float2 Vz = fma2(H2, P1, fma2(H4, P2, fma2(H9, P3, fma2(H6, P4,
+                        fma2(H10, P5, fma2(H8, P6, mul2(H11, P7)))))));
+      const float2 H4n = fma2(nx, Vx, fma2(ny, Vy, mul2(nz, Vz)));
+      const float2 s4 = mul2(s2, s2);
+      const float2 s4H = mul2(s4, H4n);
+      gp = fma2(f2(39.375f), s4H, gp);
+      php = fma2(f2(4.375f), s4H, php);
+      const float2 c9 = mul2(f2(-17.5f), s4);
+      gx = fma2(c9, Vx, gx);
+      gy = fma2(c9, Vy, gy);
+      gz = fma2(c9, Vz, gz);
+    }
+    fx = fma2(s2, fma2(gp, nx, gx), fx);
+    fy = fma2(s2, fma2(gp, ny, gy), fy);
+    fz = fma2(s2, fma2(gp, nz, gz), fz);
+    pa = fma2(s, php, pa);
+    pi = fma2(Qi, s, pi);
+  }
+  __syncwarp();
+  kahan_add(acc.sx, acc.cx, fx.x + fx.y);
+  kahan_add(acc.sy, acc.cy, fy.x + fy.y);
+  kahan_add(acc.sz, acc.cz, fz.x + fz.y);
+  acc.phi_all += (double)pa.x + (double)pa.y;
+  acc.phi_ion += (double)pi.x + (double)pi.y;
+}
+
 // -------------------------------------------------------------- local ----
 // Up to 32 far cells, one per lane: each lane expands its cell's field about
 // the group centre G (local.cuh) into its row of `loc_rows`; lanes 0..28 then
@@ -873,7 +1058,8 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
         p2h += 32;
       }
       while (m2t - m2h >= 32) {
-        eval_m2p<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+        if (RDF) eval_m2p_x2<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+        else eval_m2p<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
         m2h += 32;
       }
       while (lct - lch >= 32) {
@@ -890,7 +1076,8 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
                           tly, tlz, close2, pt, tsp, act, lane, hist, acc);
     }
     if (m2t > m2h) {
-      eval_m2p<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+      if (RDF) eval_m2p_x2<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+      else eval_m2p<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
     }
     if (lct > lch) {
       eval_local<ORDER>(sm, lch, lct - lch, a, Gx, Gy, Gz, lane, lsum);
