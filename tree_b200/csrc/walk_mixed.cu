@@ -1231,8 +1231,11 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.control = mb.control;
   a.stack = mb.stack;
   a.bucket = tune.bucket < 1 ? 1 : (tune.bucket > kMaxBucket ? kMaxBucket : tune.bucket);
-  // an octupole M2P costs ~110 flop, a quadrupole one ~60, a pair ~24
-  a.p2p_max = tune.order >= 3 ? 4 : 2;
+  // an accepted cell of at most p2p_max particles is summed as pairs: with
+  // the hexadecapole far field (measured at N = 1M, learned criterion) one
+  // far-field evaluation costs about two pair interactions, at order 3 about
+  // four
+  a.p2p_max = tune.order >= 4 ? 2 : (tune.order == 3 ? 4 : 2);
   if (a.p2p_max > a.bucket) a.p2p_max = a.bucket;
   a.loc_eps2 = (double)tune.loc_eps * tune.loc_eps;
   a.physics = wp.physics;
