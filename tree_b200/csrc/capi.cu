@@ -294,6 +294,7 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
     tg::walk64(h->x, h->n, (int)h->n_el, h->b.vals, tv, wp, h->f,
                h->epot_part, with_rdf ? h->rdf : nullptr, h->counters,
                h->b.err, st);
+    h->timing.launches += h->n > 0 ? 1 : 0;
   } else {
     tg::LearnedMac lm;
     const bool use_learned = h->prm.mac == TREE_GPU_MAC_LEARNED && h->has_model &&
@@ -308,13 +309,14 @@ void enqueue_force(tree_gpu_handle* h, bool with_rdf, EventSet* ev) {
       lm.rho_lo = h->mac_rho_lo;
       lm.rho_hi = h->mac_rho_hi;
     }
-    tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp, h->tune,
-                   use_learned ? &lm : nullptr, h->b.ens, h->cloud_pk, h->f, h->epot_part,
-                   with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
+    // the walk, and with the learned criterion its per-cell pre-filter pass
+    h->timing.launches +=
+        tg::walk_mixed(h->mb, h->b, h->x, h->n, (int)h->n_el, tv, wp, h->tune,
+                       use_learned ? &lm : nullptr, h->b.ens, h->cloud_pk, h->f, h->epot_part,
+                       with_rdf ? h->rdf : nullptr, h->counters, h->b.err, st);
   }
   if (ev) record(h, ev->e[2]);
-  h->timing.launches += (h->n > 0 ? 1 : 0) + 2;  // walk + epot partial/sum
-  // (the mixed walk is one kernel as well)
+  h->timing.launches += 2;  // epot partial/sum
   tg::epot_sum(h->epot_part, h->n, h->partial, h->diag, h->counters, st);
 }
 

@@ -54,12 +54,18 @@ __device__ __forceinline__ float mac_f7(float tnorm, float n, float s) {
 }
 __device__ __forceinline__ float mac_f14(float s, float d) { return log10f(s / d); }
 
-__device__ __forceinline__ float mac_prefilter(const float4 g4, float tnorm, float d,
-                                               const float* c) {
+// The walk evaluates the estimate split into a part of the cell alone and a
+// part of the distance.  With B = log10(budget d^2 / n) the budget in the label's units,
+//   est - B = K - log10(budget) - (2 + c0) log10(d),
+//   K = c0 log10(s) + c1 f3 + c2 f7 + c3 f6 + c4 + log10(n),
+// so K is computed once per cell and build (k_mac_node_terms) and the walk
+// compares est + m with B by one logarithm of d.
+__device__ __forceinline__ float mac_node_term(const float4 g4, float tnorm, const float* c) {
   const float s = g4.x, n = g4.z;
-  return fmaf(c[0], mac_f14(s, d),
+  return fmaf(c[0], log10f(s),
               fmaf(c[1], mac_f3(n),
-                   fmaf(c[2], mac_f7(tnorm, n, s), fmaf(c[3], mac_f6(g4.w, n, s), c[4]))));
+                   fmaf(c[2], mac_f7(tnorm, n, s),
+                        fmaf(c[3], mac_f6(g4.w, n, s), c[4] + log10f(n)))));
 }
 
 __device__ __forceinline__ void mac_features(

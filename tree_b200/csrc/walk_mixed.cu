@@ -80,7 +80,16 @@ struct WarpSmem {
   // pair constants of the group's cloud: 1/lambda^2 (ee, ei, ii), 1/rs,
   // 1/lambda (ee, ei, ii)
   float pk[8];
+  // the group's box: centre and half extents (read where used, so that they
+  // hold no registers across the walk loop)
+  double gx, gy, gz, bx, by, bz;
   double hl2;  // the group's squared half-diagonal (local-expansion test)
+  // learned criterion, per group: log10 of the error budget (-inf: none),
+  // and the cells sent to the network / kept on the fixed decision.  Kept
+  // here rather than in registers, which the walk loop needs for its
+  // evaluations.
+  float lbud;
+  unsigned n_mlp, n_fallback;
 };
 
 struct MixedArgs {
@@ -120,6 +129,10 @@ struct MixedArgs {
   const float4* geom;
   const float4* mom3;
   const float4* mom4;
+  // per cell: its part K of the pre-filter (mac.cuh) and the distance
+  // s / rho_hi + dx below which its acceptance ratio s / (d - dx) exceeds
+  // rho_hi (the learned criterion's band)
+  const float2* mac_k;
   const float* margins;  // m_lo, m_hi, pre-filter coefficients c0..c4
   const double* f_prev;
   float eta_over_eps;
@@ -753,6 +766,65 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
   acc.phi_ion += 0.5 * (pad + pqd);  // ion sources: (all + charge-weighted) / 2
 }
 
+// ------------------------------------------------------ learned MAC ----
+// One batch of queued candidates (lane < nb holds one) through the network.
+// Returns 1 (accept) or 3 (open) for a candidate, 0 otherwise, plus 4 when
+// its features fell outside the training range (the fixed decision, open,
+// stands).  Out of line: it runs once per 32 candidates, and the network's
+// fragments then take no registers from the walk loop around the call.
+__device__ __noinline__ int mac_batch(const double4* __restrict__ node_c,
+                                      const float4* __restrict__ geom,
+                                      const float4* __restrict__ mom,
+                                      const float4* __restrict__ mom3, float* feat_tile,
+                                      const MlpPacked* mlp, const float* frange, int node,
+                                      bool cand, float cand_d, float cand_B, double Gx,
+                                      double Gy, double Gz, float hlen, float n_act,
+                                      int lane) {
+  float* feat = feat_tile + lane * kMacFeatures;
+  if (cand) {
+    const double4 c = ldg_d4(&node_c[node]);
+    const float4* mp = mom + 3 * (int64_t)node;
+    const float4* tp = mom3 + 3 * (int64_t)node;
+    mac_features(c.x, c.y, c.z, __ldg(&geom[node]), __ldg(mp), __ldg(mp + 1), __ldg(mp + 2),
+                 __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), Gx, Gy, Gz, hlen, cand_d, n_act,
+                 feat);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kMacFeatures; ++k) feat[k] = 0.f;
+  }
+  // range check on the raw features before the network normalises them
+  bool in_range = true;
+#pragma unroll
+  for (int k = 0; k < kMacFeatures; ++k)
+    in_range = in_range && feat[k] >= frange[k] && feat[k] <= frange[kMacFeatures + k];
+  __syncwarp();
+  const float y = mlp_forward_warp(feat_tile, *mlp, lane);
+  if (!cand) return 0;
+  // predicted |dF| = 10^y * n / d^2 against the group's budget; out of the
+  // training range the fixed-theta decision (open) stands
+  return ((in_range && y <= cand_B) ? 1 : 3) | (in_range ? 0 : 4);
+}
+
+// Per cell, for the nodes [0, bounds[2]) of this build: its part K of the
+// learned pre-filter (mac_node_term) and the distance s / rho_hi + dx inside
+// which it lies outside the criterion's band.  Leaves are never tested; their
+// records are not read.
+__global__ void k_mac_node_terms(const float4* __restrict__ geom,
+                                 const float4* __restrict__ mom3,
+                                 const int32_t* __restrict__ bounds,
+                                 const float* __restrict__ margins, float inv_rho_hi,
+                                 float2* __restrict__ mac_k) {
+  const int end = bounds[2];
+  float c[kEstCoef];
+#pragma unroll
+  for (int k = 0; k < kEstCoef; ++k) c[k] = __ldg(&margins[2 + k]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+    const float4 g4 = __ldg(&geom[i]);
+    mac_k[i] = make_float2(mac_node_term(g4, __ldg(&mom3[3 * (int64_t)i + 2]).z, c),
+                           fmaf(g4.x, inv_rho_hi, g4.y));
+  }
+}
+
 // --------------------------------------------------------------- walk ----
 // Dynamic shared memory: WarpSmem per warp, then (learned MAC only) the
 // packed network and the features' training range, then (RDF only) the two
@@ -836,17 +908,28 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
     // exact offsets (eval_p2p)
     const double hl2 = hx * hx + hy * hy + hz * hz;
     const float close2 = (float)(hl2 * (1.0 / 32.0));
-    if (lane == 0) sm.hl2 = hl2;
+    if (lane == 0) {
+      sm.hl2 = hl2;
+      sm.gx = Gx;
+      sm.gy = Gy;
+      sm.gz = Gz;
+      sm.bx = hx;
+      sm.by = hy;
+      sm.bz = hz;
+    }
     Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
     // error budget of the learned MAC: eta * min |F_prev| / eps over the group
-    float budget = 0.f, hlen = 0.f;
     if (LEARNED) {
       const int64_t o = a.order[pt];
       const double fx = a.f_prev[3 * o], fy = a.f_prev[3 * o + 1], fz = a.f_prev[3 * o + 2];
       float fm = act ? (float)sqrt(fx * fx + fy * fy + fz * fz) : 3.0e38f;
       for (int o2 = 16; o2 > 0; o2 >>= 1) fm = fminf(fm, __shfl_xor_sync(0xffffffffu, fm, o2));
-      budget = a.eta_over_eps * fm;
-      hlen = (float)sqrt(hx * hx + hy * hy + hz * hz);
+      const float budget = a.eta_over_eps * fm;
+      if (lane == 0) {
+        sm.lbud = budget > 0.f ? log10f(budget) : -INFINITY;
+        sm.n_mlp = 0u;
+        sm.n_fallback = 0u;
+      }
     }
     int ssize = 1;
     // the group's tree: its cloud's root and pair constants
@@ -880,7 +963,6 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
     int m2h = 0, m2t = 0, p2h = 0, p2t = 0;  // ring heads/tails (warp-uniform)
     int lch = 0, lct = 0;                    // local-expansion ring
     float lsum = 0.f;  // lanes 0..19: one summed coefficient of the local expansion
-    unsigned n_mlp = 0, n_fallback = 0;  // per lane: cells this lane sent to the MLP
     bool overflow = false;
     int cqh = 0, cqt = 0;  // learned-MAC candidate ring (warp-uniform)
     while (ssize > 0 || cqt > cqh) {
@@ -889,7 +971,7 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       if (LEARNED && (cqt - cqh >= 32 || (ssize == 0 && cqt > cqh))) {
         // ---- a batch of queued candidates goes through the network ----
         const int nb = min(32, cqt - cqh);
-        bool cand = lane < nb;
+        const bool cand = lane < nb;
         float cand_d = 0.f, cand_B = 0.f;
         if (cand) {
           const int q = (cqh + lane) & (kCandRing - 1);
@@ -899,31 +981,14 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
         }
         cqh += nb;
         __syncwarp();
-        float* feat = reinterpret_cast<float*>(sm.cell) + lane * kMacFeatures;
-        if (cand) {
-          const double4 c = ldg_d4(&a.node_c[node]);
-          const float4* mp = a.mom + 3 * (int64_t)node;
-          const float4* tp = a.mom3 + 3 * (int64_t)node;
-          mac_features(c.x, c.y, c.z, __ldg(&a.geom[node]), __ldg(mp), __ldg(mp + 1),
-                       __ldg(mp + 2), __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), Gx,
-                       Gy, Gz, hlen, cand_d, (float)n_act, feat);
-        } else {
-#pragma unroll
-          for (int k = 0; k < kMacFeatures; ++k) feat[k] = 0.f;
-        }
-        // range check on the raw features before the network normalises them
-        bool in_range = true;
-#pragma unroll
-        for (int k = 0; k < kMacFeatures; ++k)
-          in_range = in_range && feat[k] >= frange[k] && feat[k] <= frange[kMacFeatures + k];
-        __syncwarp();
-        const float y = mlp_forward_warp(reinterpret_cast<float*>(sm.cell), *mlp, lane);
-        if (cand) {
-          // predicted |dF| = 10^y * n / d^2 against the group's budget; out
-          // of the training range the fixed-theta decision (open) stands
-          action = (in_range && y <= cand_B) ? 1 : 3;  // candidates exceed a bucket
-          n_mlp += 1;
-          n_fallback += in_range ? 0 : 1;
+        const int r = mac_batch(a.node_c, a.geom, a.mom, a.mom3, reinterpret_cast<float*>(sm.cell),
+                                mlp, frange, node, cand, cand_d, cand_B, sm.gx, sm.gy, sm.gz,
+                                (float)sqrt(sm.hl2), (float)n_act, lane);
+        if (cand) action = r & 3;  // candidates exceed a bucket: accept or open
+        const unsigned fbm = __ballot_sync(0xffffffffu, (r & 4) != 0);
+        if (lane == 0) {
+          sm.n_mlp += (unsigned)nb;
+          sm.n_fallback += (unsigned)__popc(fbm);
         }
       } else {
         // ---- a batch of nodes from the stack ----
@@ -934,19 +999,25 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
         bool cand = false;  // queued for the learned MAC
         float cand_d = 0.f, cand_B = 0.f;
         if (node >= 0) {
+          // the particle range and (learned criterion) the cell geometry
+          // depend on the node index alone: issued with node_c, so a batch
+          // waits for one round of loads instead of two or three
           const double4 c = ldg_d4(&a.node_c[node]);
+          const int cnt = __ldg(&a.count[node]);
+          const int fst = __ldg(&a.first[node]);
+          const float2 kr = LEARNED ? __ldg(&a.mac_k[node]) : make_float2(0.f, 0.f);
           if (c.w < 0.0) {
             action = 2;
-            pfirst = __ldg(&a.first[node]);
+            pfirst = fst;
             pcnt = 1;
           } else {
             // group MAC: rcrit below the distance from the centroid to the box
-            const double ex = fmax(fabs(c.x - Gx) - hx, 0.0);
-            const double ey = fmax(fabs(c.y - Gy) - hy, 0.0);
-            const double ez = fmax(fabs(c.z - Gz) - hz, 0.0);
+            const double ex = fmax(fabs(c.x - sm.gx) - sm.bx, 0.0);
+            const double ey = fmax(fabs(c.y - sm.gy) - sm.by, 0.0);
+            const double ez = fmax(fabs(c.z - sm.gz) - sm.bz, 0.0);
             const double d2 = ex * ex + ey * ey + ez * ez;
             bool accept = c.w * c.w < d2;  // the fixed-theta test
-            if (LEARNED && !accept && budget > 0.f) {
+            if (LEARNED && !accept) {
               // learned criterion, on top of the fixed test: a cell the fixed
               // test opens is accepted anyway when its predicted acceptance
               // error is within the group's budget.  rho = s / (d - dx) places
@@ -957,42 +1028,41 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
               // once; the rest are queued for the network.  Only cells that
               // would otherwise open into more than a bucket of particle
               // pairs are worth a far-field evaluation.
-              const float4 g4 = __ldg(&a.geom[node]);
-              const float ddf = sqrtf((float)d2);
-              const float margin = ddf - g4.y;
-              const float rho = margin > 0.f ? g4.x / margin : 3.0e38f;
-              if (rho <= a.rho_hi && g4.z > (float)a.bucket) {
-                const float tn = __ldg(&a.mom3[3 * (int64_t)node + 2]).z;
-                const float est = mac_prefilter(g4, tn, ddf, fmodel + 2);
-                const float B = log10f(budget * ddf * ddf / g4.z);
-                if (est + fmodel[1] <= B) {
+              // rho = s / (d - dx) <= rho_hi  <=>  d >= s / rho_hi + dx
+              const float d2f = (float)d2;
+              if (d2f >= kr.y * kr.y && cnt > a.bucket) {
+                const float ddf = sqrtf(d2f);
+                // est - B = K - log10(budget) - (2 + c0) log10(d); no
+                // budget: log10(budget) = -inf, never accepted or queued
+                const float lb = sm.lbud, l10d = __log10f(ddf);
+                const float eb = fmaf(-(2.f + fmodel[2]), l10d, kr.x - lb);
+                if (eb + fmodel[1] <= 0.f) {
                   accept = true;
-                } else if (est + fmodel[0] <= B) {
+                } else if (eb + fmodel[0] <= 0.f) {
                   cand = true;
                   cand_d = ddf;
-                  cand_B = B;
+                  cand_B = lb + 2.f * l10d - log10f((float)cnt);
                 }
               }
             }
             // a small accepted cell is cheaper and exact as particle pairs: an
             // M2P costs about as much as p2p_max pair interactions
-            const int cnt = __ldg(&a.count[node]);
             if (accept && cnt <= a.p2p_max) {
               action = 2;
-              pfirst = __ldg(&a.first[node]);
+              pfirst = fst;
               pcnt = cnt;
             } else if (accept) {
               action = 1;
               if (a.loc_eps2 > 0.0) {
                 // far from the group: summed into its local expansion
-                const double ux = c.x - Gx, uy = c.y - Gy, uz = c.z - Gz;
+                const double ux = c.x - sm.gx, uy = c.y - sm.gy, uz = c.z - sm.gz;
                 const double dc2 = ux * ux + uy * uy + uz * uz;
                 if (sm.hl2 <= a.loc_eps2 * dc2) action = 4;
               }
             } else if (!cand) {
               if (cnt <= a.bucket) {
                 action = 2;
-                pfirst = __ldg(&a.first[node]);
+                pfirst = fst;
                 pcnt = cnt;
               } else {
                 action = 3;
@@ -1053,17 +1123,17 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       max_stack = max(max_stack, ssize);
       __syncwarp();
       while (p2t - p2h >= 32) {
-        eval_p2p<PHYS, RDF>(sm, p2h, 32, a, Gx, Gy, Gz, thx, thy, thz, tlx, tly,
+        eval_p2p<PHYS, RDF>(sm, p2h, 32, a, sm.gx, sm.gy, sm.gz, thx, thy, thz, tlx, tly,
                             tlz, close2, pt, tsp, act, lane, hist, acc);
         p2h += 32;
       }
       while (m2t - m2h >= 32) {
-        if (RDF) eval_m2p_x2<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
-        else eval_m2p<ORDER>(sm, m2h, 32, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+        if (RDF) eval_m2p_x2<ORDER>(sm, m2h, 32, a, sm.gx, sm.gy, sm.gz, thx, thy, thz, lane, acc);
+        else eval_m2p<ORDER>(sm, m2h, 32, a, sm.gx, sm.gy, sm.gz, thx, thy, thz, lane, acc);
         m2h += 32;
       }
       while (lct - lch >= 32) {
-        eval_local<ORDER>(sm, lch, 32, a, Gx, Gy, Gz, lane, lsum);
+        eval_local<ORDER>(sm, lch, 32, a, sm.gx, sm.gy, sm.gz, lane, lsum);
         lch += 32;
       }
     }
@@ -1072,15 +1142,15 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       continue;
     }
     if (p2t > p2h) {
-      eval_p2p<PHYS, RDF>(sm, p2h, p2t - p2h, a, Gx, Gy, Gz, thx, thy, thz, tlx,
+      eval_p2p<PHYS, RDF>(sm, p2h, p2t - p2h, a, sm.gx, sm.gy, sm.gz, thx, thy, thz, tlx,
                           tly, tlz, close2, pt, tsp, act, lane, hist, acc);
     }
     if (m2t > m2h) {
-      if (RDF) eval_m2p_x2<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
-      else eval_m2p<ORDER>(sm, m2h, m2t - m2h, a, Gx, Gy, Gz, thx, thy, thz, lane, acc);
+      if (RDF) eval_m2p_x2<ORDER>(sm, m2h, m2t - m2h, a, sm.gx, sm.gy, sm.gz, thx, thy, thz, lane, acc);
+      else eval_m2p<ORDER>(sm, m2h, m2t - m2h, a, sm.gx, sm.gy, sm.gz, thx, thy, thz, lane, acc);
     }
     if (lct > lch) {
-      eval_local<ORDER>(sm, lch, lct - lch, a, Gx, Gy, Gz, lane, lsum);
+      eval_local<ORDER>(sm, lch, lct - lch, a, sm.gx, sm.gy, sm.gz, lane, lsum);
     }
     if (lct > 0) {
       // every target evaluates the group's summed local expansion
@@ -1114,14 +1184,9 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       if (lct > 0) atomicAdd(&a.counters[8], (unsigned long long)lct);
     }
     if (LEARNED) {
-      unsigned long long m = n_mlp, fb = n_fallback;
-      for (int o2 = 16; o2 > 0; o2 >>= 1) {
-        m += __shfl_xor_sync(0xffffffffu, m, o2);
-        fb += __shfl_xor_sync(0xffffffffu, fb, o2);
-      }
       if (lane == 0) {
-        atomicAdd(&a.counters[2], m);
-        atomicAdd(&a.counters[3], fb);
+        atomicAdd(&a.counters[2], (unsigned long long)sm.n_mlp);
+        atomicAdd(&a.counters[3], (unsigned long long)sm.n_fallback);
       }
     }
   }
@@ -1157,6 +1222,7 @@ int mixed_alloc_nodes(MixedBuffers& mb, int cap) {
   rc |= realloc_dev(&mb.mom4, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.mom, 3 * (size_t)cap);
   rc |= realloc_dev(&mb.geom, (size_t)cap);
+  rc |= realloc_dev(&mb.mac_k, (size_t)cap);
   rc |= realloc_dev(&mb.lvl_list, (size_t)cap);
   rc |= realloc_dev(&mb.cls, (size_t)net_cls_entries(cap));
   return rc;
@@ -1179,7 +1245,7 @@ int mixed_alloc_particles(MixedBuffers& mb, int n) {
 
 void mixed_free(MixedBuffers& mb) {
   void* ptrs[] = {mb.kids, mb.first, mb.count, mb.digit, mb.m64, mb.mom,
-                  mb.mom3, mb.mom4, mb.geom, mb.xs, mb.groups, mb.stack, mb.control,
+                  mb.mom3, mb.mom4, mb.geom, mb.mac_k, mb.xs, mb.groups, mb.stack, mb.control,
                   mb.lvl_list, mb.lvl, mb.cls};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1265,6 +1331,7 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.mom3 = mb.mom3;
   a.mom4 = mb.mom4;
   a.margins = L ? learned->margins : nullptr;
+  a.mac_k = mb.mac_k;
   a.f_prev = L ? learned->f_prev : nullptr;
   a.eta_over_eps = L ? (float)(learned->eta / kEps) : 0.f;
   a.rho_lo = L ? learned->rho_lo : 0.f;
@@ -1278,6 +1345,9 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   const int sms_grid = mb.grid_warps / (kMaxBlocksPerSm * kMxWarps);
   int grid = sms_grid * bps;
   const bool r = rdf != nullptr;
+  if (L) k_mac_node_terms<<<sms_grid * 4, 256, 0, st>>>(mb.geom, mb.mom3, tv.tree_bounds,
+                                                       learned->margins, 1.f / learned->rho_hi,
+                                                       mb.mac_k);
   int dev = 0;
   cudaGetDevice(&dev);
 #define TG_LAUNCH(P, R, LL, O)                                                \
@@ -1307,7 +1377,7 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   }
 #undef TG_LAUNCH_O
 #undef TG_LAUNCH
-  return 1;
+  return L ? 2 : 1;
 }
 
 }  // namespace tg

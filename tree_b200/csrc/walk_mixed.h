@@ -21,6 +21,7 @@ struct MixedBuffers {
   float4* mom3 = nullptr;
   float4* mom4 = nullptr;
   float4* geom = nullptr;
+  float2* mac_k = nullptr;     // learned MAC: the cell's pre-filter record
   double4* xs = nullptr;
   int2* groups = nullptr;
   int32_t* lvl_list = nullptr; // per node: twigs by level (upward pass)
