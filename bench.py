@@ -65,9 +65,15 @@ FIXED_ARMS = {2: (0.20, 0.22, 0.25), 3: (0.30, 0.32, 0.35), 4: (0.40, 0.42, 0.45
 # Opening angles the ensemble autotuner tries, per far-field order.
 TUNE_THETAS = {2: (0.14, 0.16, 0.18, 0.20, 0.22), 3: (0.20, 0.22, 0.24, 0.26, 0.28, 0.30),
                4: (0.30, 0.33, 0.36, 0.39, 0.42, 0.45)}
-# Ensemble of 64 clouds: the autotuner's pick on that workload (learned MAC at
-# theta = 0.26, eta = 3e-5), fixed here so that the bench does no tuning.
-ENSEMBLE_TUNED = dict(theta=0.26, eta=3e-5, bucket=8, order=3, blocks_per_sm=4)
+# Ensemble of 64 clouds, fixed here so that the bench does no tuning: the
+# learned criterion on the hexadecapole far field at theta = 0.36, eta = 3e-5
+# (worst cloud rms 5.7e-5 on 4,096 targets each, 10 steps after the 13-step
+# warm-up; the tuner's fastest order-4 pick, fixed theta = 0.39, reached
+# 1.09e-4 on one cloud at that audit), two blocks per SM (the learned build's
+# register budget).
+ENSEMBLE_TUNED = dict(theta=0.36, eta=3e-5, bucket=8, order=4, blocks_per_sm=2)
+# The fixed test's own grid (its 80-register build holds three blocks per SM).
+ENSEMBLE_FIXED_BPS = 3
 
 
 def parse():
@@ -665,6 +671,20 @@ def run_ours(args, rank, world, dist):
 
 
 # ------------------------------------------------------------- ensemble ----
+def ensemble_rms(ens, nclouds):
+    """Per-cloud rms relative force error of the last forces against each
+    cloud's own FP64 direct sum on 4,096 seeded targets."""
+    f = ens.get_state()["f"]
+    rms = []
+    for cc in range(nclouds):
+        a, b = int(ens.offsets[cc]), int(ens.offsets[cc + 1])
+        t = np.sort(np.random.default_rng(cc).choice(b - a, min(4096, b - a), replace=False))
+        fd, _ = ens.direct(cc, t)
+        err = np.linalg.norm(f[a:b][t] - fd, axis=1) / np.linalg.norm(fd, axis=1)
+        rms.append(float(np.sqrt(np.mean(err ** 2))))
+    return rms
+
+
 def ensemble_record(args, stream, dist, world, tune_it=False, compare_separate=False):
     """Independent clouds of uneven N (log-uniform in [8192, 131072]), peak
     densities log-uniform in [1e14, 1e16] m^-3, T_e uniform in [10, 200] K, in
@@ -701,7 +721,7 @@ def ensemble_record(args, stream, dist, world, tune_it=False, compare_separate=F
         ens.set_tuning(setting["bucket"], setting["blocks_per_sm"], order)
         ens.mac_set_model(params, stats)
         space = [tune.Candidate(t, e, 8, order, g) for t in TUNE_THETAS.get(order, TUNE_THETAS[3])
-                 for e in (0.0, 1e-5, 3e-5) for g in (3, 4)]
+                 for e in (0.0, 1e-5, 3e-5) for g in (2, 3)]
         best, trials = tune.autotune(ens, dt, space=space, target=1e-4, margin=0.8,
                                      audit=1024 * args.clouds, physics=phys,
                                      model=(params, stats))
@@ -726,15 +746,7 @@ def ensemble_record(args, stream, dist, world, tune_it=False, compare_separate=F
     ms = max_over_ranks(e0.elapsed_time(e1), dist)
     t_after = ens.timings()
     value = whole_job_rate(n, world, args.steps, ms)
-    # per-cloud accuracy against each cloud's own FP64 direct sum
-    f = ens.get_state()["f"]
-    rms = []
-    for cc in range(args.clouds):
-        a, b = int(ens.offsets[cc]), int(ens.offsets[cc + 1])
-        t = np.sort(np.random.default_rng(cc).choice(b - a, min(4096, b - a), replace=False))
-        fd, _ = ens.direct(cc, t)
-        err = np.linalg.norm(f[a:b][t] - fd, axis=1) / np.linalg.norm(fd, axis=1)
-        rms.append(float(np.sqrt(np.mean(err ** 2))))
+    rms = ensemble_rms(ens, args.clouds)
     # end to end: cloud-major state host -> device, one step, state back
     pin = {k: torch.from_numpy(np.ascontiguousarray(warm[k])).pin_memory() for k in ("x", "v", "f")}
     k2 = max(1, min(args.steps, 5))
@@ -748,6 +760,31 @@ def ensemble_record(args, stream, dist, world, tune_it=False, compare_separate=F
     a1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(a0.elapsed_time(a1), dist) / k2
+    fixed_arm = None
+    if setting["eta"] > 0:
+        # the same opening angle and order with the fixed test alone, from the
+        # same warm state
+        cand = tune.Candidate(setting["theta"], 0.0, setting["bucket"], setting["order"],
+                              ENSEMBLE_FIXED_BPS)
+        tune._apply(ens, cand, phys, 50.0, None)
+        ens.load_state(warm["x"], warm["v"], warm["f"])
+        ens.step(dt, 1)  # graph capture of this variant, untimed
+        ens.load_state(warm["x"], warm["v"], warm["f"])
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        ens.step(dt, args.steps)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fms = max_over_ranks(f0.elapsed_time(f1), dist) / args.steps
+        frms = ensemble_rms(ens, args.clouds)
+        fixed_arm = {"theta": setting["theta"], "eta": 0.0, "blocks_per_sm": ENSEMBLE_FIXED_BPS,
+                     "ms_per_step": fms, "value": whole_job_rate(n, world, 1, fms),
+                     "rms_rel_err_max_cloud": max(frms),
+                     "rms_rel_err_median_cloud": float(np.median(frms))}
     sep_ms = None
     if compare_separate:
         sep_ms = 0.0
@@ -794,6 +831,7 @@ def ensemble_record(args, stream, dist, world, tune_it=False, compare_separate=F
                                     "rms": rms[cc]} for cc in range(args.clouds)]},
         "e2e": {"value": whole_job_rate(n, world, 1, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": 72 * n, "d2h_bytes_per_step": 72 * n},
+        "fixed_theta_same_setting": fixed_arm,
         "separate_handles_ms_per_step": sep_ms,
         "one_launch_speedup": (sep_ms / (ms / args.steps)) if sep_ms else None,
     }

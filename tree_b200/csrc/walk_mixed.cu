@@ -42,7 +42,13 @@ constexpr int kLocStride = kLocCoef | 1;  // odd row stride of the coefficient r
 constexpr int kP2pRing = 512;     // power of two, > 31 + 32 * kMaxBucket
 constexpr int kMaxBucket = 8;
 constexpr int kMaxBlocksPerSm = 4;
-constexpr int kMinBlocksPerSm = 3;  // 80 registers: 24 resident warps per SM
+// Blocks per SM the walk without RDF counts is compiled for: the fixed test
+// at 3 (80 registers, 24 resident warps), the learned criterion at 2 (128
+// registers, 16 warps): its candidate ring and budget make the 80-register
+// build spill, which cost 13 % of its walk at N = 1M (23.1 against 20.4 ms),
+// while the fixed test runs 5 % faster at 80 registers than at 128.
+constexpr int kMinBlocksPerSm = 3;
+constexpr int kMinBlocksPerSmLearned = 2;
 // With RDF counts the walk runs one block of kRdfWarps per SM that keeps both
 // histograms (2 x 10001 u32) in shared memory and adds them to the global
 // bins once, when the block ends.
@@ -57,8 +63,6 @@ struct WarpSmem {
   int loc[kLocRing];       // far cells summed into the group's local expansion
   int p2p[kP2pRing];
   int cq_node[kCandRing];  // learned-MAC candidates waiting for a full batch
-  float cq_d[kCandRing];
-  float cq_b[kCandRing];
   // The far-field and pair staging areas (and the learned MAC's feature
   // rows, in `cell`) are used one at a time by the warp: one buffer.
   union {
@@ -90,7 +94,15 @@ struct WarpSmem {
   // evaluations.
   float lbud;
   unsigned n_mlp, n_fallback;
+  double2 phi[32];  // per lane: unscaled potential (all sources, ion part)
 };
+
+__device__ __forceinline__ void phi_add(WarpSmem& sm, int lane, double all, double ion) {
+  double2 p = sm.phi[lane];
+  p.x += all;
+  p.y += ion;
+  sm.phi[lane] = p;
+}
 
 struct MixedArgs {
   const double4* __restrict__ node_c;
@@ -147,7 +159,9 @@ struct MixedArgs {
 
 struct Acc {
   float sx, sy, sz, cx, cy, cz;  // Kahan sums of the unscaled force
-  double phi_all, phi_ion;       // unscaled potential: all sources, ion part
+  // The unscaled potential (all sources, ion part) is summed in FP64 in the
+  // warp's shared memory, one slot per lane (WarpSmem::phi): it is touched
+  // once per batch of 32 entries and need not hold registers in between.
 };
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
@@ -317,8 +331,7 @@ __device__ __forceinline__ void eval_m2p(WarpSmem& sm, int head, int cnt,
   kahan_add(acc.sx, acc.cx, fx);
   kahan_add(acc.sy, acc.cy, fy);
   kahan_add(acc.sz, acc.cz, fz);
-  acc.phi_all += (double)pa;
-  acc.phi_ion += (double)pi;
+  phi_add(sm, lane, (double)pa, (double)pi);
 }
 
 // The same far field two cells at a time on the packed FP32 (f32x2) pipeline:
@@ -502,8 +515,7 @@ __device__ __forceinline__ void eval_m2p_x2(WarpSmem& sm, int head, int cnt,
   kahan_add(acc.sx, acc.cx, fx.x + fx.y);
   kahan_add(acc.sy, acc.cy, fy.x + fy.y);
   kahan_add(acc.sz, acc.cz, fz.x + fz.y);
-  acc.phi_all += (double)pa.x + (double)pa.y;
-  acc.phi_ion += (double)pi.x + (double)pi.y;
+  phi_add(sm, lane, (double)pa.x + (double)pa.y, (double)pi.x + (double)pi.y);
 }
 
 // -------------------------------------------------------------- local ----
@@ -762,8 +774,17 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
   kahan_add(acc.sy, acc.cy, fy.x + fy.y);
   kahan_add(acc.sz, acc.cz, fz.x + fz.y);
   const double pad = (double)pa.x + (double)pa.y, pqd = (double)pq.x + (double)pq.y;
-  acc.phi_all += pad;
-  acc.phi_ion += 0.5 * (pad + pqd);  // ion sources: (all + charge-weighted) / 2
+  phi_add(sm, lane, pad, 0.5 * (pad + pqd));  // ion sources: (all + charge-weighted) / 2
+}
+
+// Squared distance from a cell's centroid to the group's box, in an
+// operation order pinned against contraction: the network batch recomputes
+// it for its candidates and must see the value the walk's test saw.
+__device__ __forceinline__ double box_dist2(const double4& c, const WarpSmem& sm) {
+  const double ex = fmax(fabs(c.x - sm.gx) - sm.bx, 0.0);
+  const double ey = fmax(fabs(c.y - sm.gy) - sm.by, 0.0);
+  const double ez = fmax(fabs(c.z - sm.gz) - sm.bz, 0.0);
+  return __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
 }
 
 // ------------------------------------------------------ learned MAC ----
@@ -772,22 +793,26 @@ __device__ __forceinline__ void eval_p2p(WarpSmem& sm, int head, int cnt,
 // its features fell outside the training range (the fixed decision, open,
 // stands).  Out of line: it runs once per 32 candidates, and the network's
 // fragments then take no registers from the walk loop around the call.
+// A candidate's distance d and budget B = log10(budget d^2 / n) (the label's
+// units) are recomputed here as the walk's test formed them.
 __device__ __noinline__ int mac_batch(const double4* __restrict__ node_c,
                                       const float4* __restrict__ geom,
                                       const float4* __restrict__ mom,
-                                      const float4* __restrict__ mom3, float* feat_tile,
+                                      const float4* __restrict__ mom3, WarpSmem& sm,
                                       const MlpPacked* mlp, const float* frange, int node,
-                                      bool cand, float cand_d, float cand_B, double Gx,
-                                      double Gy, double Gz, float hlen, float n_act,
-                                      int lane) {
-  float* feat = feat_tile + lane * kMacFeatures;
+                                      bool cand, float n_act, int lane) {
+  float* feat = reinterpret_cast<float*>(sm.cell) + lane * kMacFeatures;
+  float cand_B = 0.f;
   if (cand) {
     const double4 c = ldg_d4(&node_c[node]);
+    const float4 g4 = __ldg(&geom[node]);
+    const float ddf = sqrtf((float)box_dist2(c, sm));
+    cand_B = sm.lbud + 2.f * __log10f(ddf) - log10f(g4.z);
     const float4* mp = mom + 3 * (int64_t)node;
     const float4* tp = mom3 + 3 * (int64_t)node;
-    mac_features(c.x, c.y, c.z, __ldg(&geom[node]), __ldg(mp), __ldg(mp + 1), __ldg(mp + 2),
-                 __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), Gx, Gy, Gz, hlen, cand_d, n_act,
-                 feat);
+    mac_features(c.x, c.y, c.z, g4, __ldg(mp), __ldg(mp + 1), __ldg(mp + 2), __ldg(tp),
+                 __ldg(tp + 1), __ldg(tp + 2), sm.gx, sm.gy, sm.gz, (float)sqrt(sm.hl2), ddf,
+                 n_act, feat);
   } else {
 #pragma unroll
     for (int k = 0; k < kMacFeatures; ++k) feat[k] = 0.f;
@@ -798,7 +823,7 @@ __device__ __noinline__ int mac_batch(const double4* __restrict__ node_c,
   for (int k = 0; k < kMacFeatures; ++k)
     in_range = in_range && feat[k] >= frange[k] && feat[k] <= frange[kMacFeatures + k];
   __syncwarp();
-  const float y = mlp_forward_warp(feat_tile, *mlp, lane);
+  const float y = mlp_forward_warp(reinterpret_cast<float*>(sm.cell), *mlp, lane);
   if (!cand) return 0;
   // predicted |dF| = 10^y * n / d^2 against the group's budget; out of the
   // training range the fixed-theta decision (open) stands
@@ -844,7 +869,8 @@ static_assert(walk_smem_bytes<true, false>() * kMinBlocksPerSm <= 233472 - 3 * 1
               "three walk blocks no longer fit one SM");
 
 template <int PHYS, bool RDF, bool LEARNED, int ORDER>
-__global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : kMinBlocksPerSm)
+__global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads,
+                                  RDF ? 1 : (LEARNED ? kMinBlocksPerSmLearned : kMinBlocksPerSm))
     k_walk_mixed(MixedArgs a) {
   constexpr int kW = RDF ? kRdfWarps : kMxWarps;
   extern __shared__ float4 dyn_smem[];
@@ -917,7 +943,8 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       sm.by = hy;
       sm.bz = hz;
     }
-    Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.0, 0.0};
+    Acc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    sm.phi[lane] = make_double2(0.0, 0.0);
     // error budget of the learned MAC: eta * min |F_prev| / eps over the group
     if (LEARNED) {
       const int64_t o = a.order[pt];
@@ -972,18 +999,11 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
         // ---- a batch of queued candidates goes through the network ----
         const int nb = min(32, cqt - cqh);
         const bool cand = lane < nb;
-        float cand_d = 0.f, cand_B = 0.f;
-        if (cand) {
-          const int q = (cqh + lane) & (kCandRing - 1);
-          node = sm.cq_node[q];
-          cand_d = sm.cq_d[q];
-          cand_B = sm.cq_b[q];
-        }
+        if (cand) node = sm.cq_node[(cqh + lane) & (kCandRing - 1)];
         cqh += nb;
         __syncwarp();
-        const int r = mac_batch(a.node_c, a.geom, a.mom, a.mom3, reinterpret_cast<float*>(sm.cell),
-                                mlp, frange, node, cand, cand_d, cand_B, sm.gx, sm.gy, sm.gz,
-                                (float)sqrt(sm.hl2), (float)n_act, lane);
+        const int r = mac_batch(a.node_c, a.geom, a.mom, a.mom3, sm, mlp, frange, node, cand,
+                                (float)n_act, lane);
         if (cand) action = r & 3;  // candidates exceed a bucket: accept or open
         const unsigned fbm = __ballot_sync(0xffffffffu, (r & 4) != 0);
         if (lane == 0) {
@@ -997,7 +1017,6 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
         ssize -= nb;
         __syncwarp();
         bool cand = false;  // queued for the learned MAC
-        float cand_d = 0.f, cand_B = 0.f;
         if (node >= 0) {
           // the particle range and (learned criterion) the cell geometry
           // depend on the node index alone: issued with node_c, so a batch
@@ -1012,10 +1031,7 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
             pcnt = 1;
           } else {
             // group MAC: rcrit below the distance from the centroid to the box
-            const double ex = fmax(fabs(c.x - sm.gx) - sm.bx, 0.0);
-            const double ey = fmax(fabs(c.y - sm.gy) - sm.by, 0.0);
-            const double ez = fmax(fabs(c.z - sm.gz) - sm.bz, 0.0);
-            const double d2 = ex * ex + ey * ey + ez * ez;
+            const double d2 = box_dist2(c, sm);
             bool accept = c.w * c.w < d2;  // the fixed-theta test
             if (LEARNED && !accept) {
               // learned criterion, on top of the fixed test: a cell the fixed
@@ -1040,8 +1056,6 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
                   accept = true;
                 } else if (eb + fmodel[0] <= 0.f) {
                   cand = true;
-                  cand_d = ddf;
-                  cand_B = lb + 2.f * l10d - log10f((float)cnt);
                 }
               }
             }
@@ -1075,8 +1089,6 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
           if (cand) {
             const int q = (cqt + __popc(cm & lt)) & (kCandRing - 1);
             sm.cq_node[q] = node;
-            sm.cq_d[q] = cand_d;
-            sm.cq_b[q] = cand_B;
           }
           cqt += __popc(cm);
         }
@@ -1162,8 +1174,7 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       kahan_add(acc.sx, acc.cx, lfx);
       kahan_add(acc.sy, acc.cy, lfy);
       kahan_add(acc.sz, acc.cz, lfz);
-      acc.phi_all += (double)lph;
-      acc.phi_ion += (double)lpi;
+      phi_add(sm, lane, (double)lph, (double)lpi);
     }
     if (act) {
       const double sc = tsp ? kEps : -kEps;  // eps * target charge
@@ -1171,8 +1182,9 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads, RDF ? 1 : k
       a.f[3 * o] = sc * ((double)acc.sx - (double)acc.cx);
       a.f[3 * o + 1] = sc * ((double)acc.sy - (double)acc.cy);
       a.f[3 * o + 2] = sc * ((double)acc.sz - (double)acc.cz);
-      const double all = 0.5 * sc * acc.phi_all;
-      const double from_i = 0.5 * sc * acc.phi_ion;
+      const double2 phi = sm.phi[lane];
+      const double all = 0.5 * sc * phi.x;
+      const double from_i = 0.5 * sc * phi.y;
       // Epot_e = ee + ie + ei, Epot_i = ii (tree.f90:674-715)
       a.epot_part[o] = tsp ? make_double2(all - from_i, from_i)
                            : make_double2(all, 0.0);
@@ -1342,6 +1354,9 @@ int walk_mixed(MixedBuffers& mb, const BuildBuffers& b, const double* x,
   a.roots = ens.roots;
   a.cloud_pk = cloud_pk;
   int bps = tune.blocks_per_sm < 1 ? 1 : (tune.blocks_per_sm > kMaxBlocksPerSm ? kMaxBlocksPerSm : tune.blocks_per_sm);
+  // the learned build holds at most kMinBlocksPerSmLearned blocks per SM:
+  // more would only queue behind them
+  if (L && bps > kMinBlocksPerSmLearned) bps = kMinBlocksPerSmLearned;
   const int sms_grid = mb.grid_warps / (kMaxBlocksPerSm * kMxWarps);
   int grid = sms_grid * bps;
   const bool r = rdf != nullptr;
