@@ -263,7 +263,9 @@ int tree_gpu_set_stream(tree_gpu_handle* h, void* stream);
 
 /* Tunables of the mixed-precision walk: twigs holding at most `bucket`
  * particles (1..8) are summed particle by particle instead of being opened;
- * `blocks_per_sm` (1..4) sets the persistent grid; `order` (2..4) is the
+ * `blocks_per_sm` (1..4) sets the persistent grid of the walk without RDF
+ * counts (the learned criterion's walk holds at most 2 blocks per SM and is
+ * clamped there; with RDF counts the walk runs one block per SM); `order` (2..4) is the
  * far-field expansion order (quadrupole; octupole as well, the default 3; or
  * hexadecapole as well, 4).  A learned acceptance model predicts the error of
  * one order: load one trained at the order in use.
