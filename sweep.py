@@ -5,16 +5,17 @@
     python sweep.py learned [--n 4194304] [--steps 500]
 
 precision: the precision form -- seeded clouds at T_e in {10, 50, 200} K,
-    each run with the mixed-precision walk at opening angles {0.3, 0.5, 0.7}
-    for `steps` steps; at steps 1, 10, 100 and the last, the rms and max
+    each run with the mixed-precision walk (fixed test, far-field order
+    --order, default 3) at opening angles {0.3, 0.5, 0.7} for `steps` steps; at steps 1, 10, 100 and the last, the rms and max
     relative force error against the FP64 O(N^2) direct sum on 16,384 seeded
     targets, and the time per step.
 drift: the total energy 1/2 (mv2_el + mv2_ion) + Epot_e + Epot_i, sampled every
     10 steps over `steps` steps from the same seeded cloud, for the
     mixed-precision walk with the learned criterion (--order, --theta, --eta;
     default 3, 0.30, 3e-5) and
-    for the plain FP64 fixed-theta path (theta 0.5); reports the largest
-    excursion |E - E_0| relative to the mean kinetic energy for both.
+    for the plain FP64 fixed-theta path (theta 0.5), or only those named by
+    --arms; reports the largest excursion |E - E_0| relative to the mean
+    kinetic energy for each.
 learned: the learned-MAC form -- the mixed walk with the learned criterion
     (--order, --theta, --eta) for `steps` steps from a seeded cloud at T_e = 50 K;
     at steps 1, 10, 100 and the last, the rms and max relative force error on
@@ -46,7 +47,7 @@ def _audit(tf, idx):
     return float(np.sqrt(np.mean(err ** 2))), float(err.max())
 
 
-def precision(n, steps, seed, tes=(10.0, 50.0, 200.0), thetas=(0.3, 0.5, 0.7)):
+def precision(n, steps, seed, tes=(10.0, 50.0, 200.0), thetas=(0.3, 0.5, 0.7), order=3):
     dt = units.dt_code(1e-11)
     rng = np.random.default_rng(seed + 17)
     idx = np.sort(rng.choice(n, min(16384, n), replace=False))
@@ -56,6 +57,7 @@ def precision(n, steps, seed, tes=(10.0, 50.0, 200.0), thetas=(0.3, 0.5, 0.7)):
         for th in thetas:
             cfg = api.Config(theta=th, te=te, physics=api.PHYS_KELBG, precision=api.PREC_MIXED)
             with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
+                tf.set_tuning(8, 4, order)
                 tf.set_state(c.x_el, c.v_el, c.x_ion, c.v_ion)
                 done, rows = 0, []
                 t0 = tf.timings()
@@ -68,12 +70,13 @@ def precision(n, steps, seed, tes=(10.0, 50.0, 200.0), thetas=(0.3, 0.5, 0.7)):
                     rms, mx = _audit(tf, idx)
                     rows.append({"step": m, "rms": rms, "max": mx})
                 t1 = tf.timings()
-            print(json.dumps({"mode": "precision", "n": n, "te_k": te, "theta": th,
+            print(json.dumps({"mode": "precision", "n": n, "order": order, "te_k": te, "theta": th,
                               "steps": steps, "audits": rows,
                               "ms_per_step": (t1.ms_total - t0.ms_total) / steps}), flush=True)
 
 
-def drift(n, steps, seed, nsamp=10, order=3, theta=0.30, eta=3e-5):
+def drift(n, steps, seed, nsamp=10, order=3, theta=0.30, eta=3e-5,
+          arms_wanted=("mixed_learned", "fp64_plain")):
     dt = units.dt_code(1e-11)
     c = cloud.make_cloud(n, seed=seed)
     params, stats, _ = learned_mac.load_model(order=order)
@@ -83,6 +86,8 @@ def drift(n, steps, seed, nsamp=10, order=3, theta=0.30, eta=3e-5):
             ("fp64_plain", api.Config(theta=0.5, physics=api.PHYS_KELBG,
                                       precision=api.PREC_FP64)))
     for name, cfg in arms:
+        if name not in arms_wanted:
+            continue
         with api.TreeForce(len(c.x_el), len(c.x_ion), cfg) as tf:
             if cfg.precision == api.PREC_MIXED:
                 tf.set_tuning(8, 4, order)
@@ -97,7 +102,9 @@ def drift(n, steps, seed, nsamp=10, order=3, theta=0.30, eta=3e-5):
         out[name] = {"excursion_over_mean_ke": float(np.max(np.abs(e - e[0])) / np.mean(ke)),
                      "e_first": float(e[0]), "e_last": float(e[-1]),
                      "ms_per_step": (t1.ms_total - t0.ms_total) / steps}
-    out["ratio"] = out["mixed_learned"]["excursion_over_mean_ke"] / out["fp64_plain"]["excursion_over_mean_ke"]
+    if "mixed_learned" in out and "fp64_plain" in out:
+        out["ratio"] = (out["mixed_learned"]["excursion_over_mean_ke"] /
+                        out["fp64_plain"]["excursion_over_mean_ke"])
     print(json.dumps({"mode": "drift", "n": n, "steps": steps, "nsamp": nsamp, **out}),
           flush=True)
 
@@ -164,15 +171,19 @@ def main():
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--order", type=int, default=3, help="far-field order (drift, learned)")
+    ap.add_argument("--order", type=int, default=3,
+                    help="far-field order (precision, drift, learned)")
+    ap.add_argument("--arms", default="mixed_learned,fp64_plain",
+                    help="drift: the arms to run (the plain FP64 arm does not depend "
+                         "on the mixed path's settings)")
     ap.add_argument("--theta", type=float, default=0.30, help="opening angle (drift, learned)")
     ap.add_argument("--eta", type=float, default=3e-5, help="learned budget (drift, learned)")
     args = ap.parse_args()
     if args.mode == "precision":
-        precision(args.n or 1048576, args.steps or 1000, args.seed)
+        precision(args.n or 1048576, args.steps or 1000, args.seed, order=args.order)
     elif args.mode == "drift":
         drift(args.n or 1048576, args.steps or 1000, args.seed, order=args.order,
-              theta=args.theta, eta=args.eta)
+              theta=args.theta, eta=args.eta, arms_wanted=tuple(args.arms.split(",")))
     else:
         learned(args.n or 4194304, args.steps or 500, args.seed, order=args.order,
                 theta=args.theta, eta=args.eta)
