@@ -21,11 +21,14 @@
 // two-float (hi + lo) split of the FP64 offsets, so a pair separation keeps
 // ~1e-7 relative accuracy even for the closest e-i pairs.  Chunk sums of 32
 // terms are added into Kahan-compensated per-lane accumulators.
-// Far field: net monopole, dipole and trace-free quadrupole (and octupole at
-// order 3) about the centroid -- the Coulomb expansion of tree.f90:744-779
-// carried to full subtree moments and one order further, for cells whose net
-// charge nearly cancels.  Near field: erf-Kelbg (or the reference laws) for
-// every particle pair.
+// Far field: net monopole, dipole and trace-free quadrupole (octupole at order
+// 3, hexadecapole at order 4) about the centroid -- the Coulomb expansion of
+// tree.f90:744-779 carried to full subtree moments and further, for cells
+// whose net charge nearly cancels; accepted cells far from the group go into
+// the group's fourth-order local expansion (local.cuh), evaluated once per
+// target.  Near field: erf-Kelbg (or the reference laws) for every particle
+// pair.  With a trained model, cells the fixed test opens may be accepted by
+// the learned criterion (mac.cuh, mac_batch below).
 #include <cstdio>
 #include "local.cuh"
 #include "mac.cuh"
