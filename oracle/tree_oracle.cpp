@@ -41,7 +41,8 @@
 //      (tree.f90:128-273).  Here insertion stops at ORACLE_MAX_DEPTH and the
 //      call returns ORACLE_ERR_DEPTH.
 //
-// Additional physics mode (no reference code; the north-star pair law):
+// Additional physics mode (no reference code; the erf-Kelbg pair law the
+// device paths also carry):
 //   KELBG: every leaf pair uses V = q_i q_j eps / r [1 - exp(-x^2) + sqrt(pi)
 //   x erfc(x)], x = r / lambda_ij, F = q_i q_j eps (1 - exp(-x^2)) rhat / r^2;
 //   self pairs are excluded by index; the far field is the reference's
@@ -316,7 +317,7 @@ inline void rdf_add(int64_t* hist, double r, double dxbin) {
   if (id >= 0 && id <= kNdist) hist[id]++;
 }
 
-// North-star Kelbg leaf law (no reference code): adds force and 0.5*V.
+// erf-Kelbg leaf law (no reference code): adds force and 0.5*V.
 inline void kelbg_pair(const double* xr, double r2, double qq, double lam,
                        Acc& a) {
   double pref = qq * kEps;
