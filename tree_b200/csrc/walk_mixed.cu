@@ -1021,9 +1021,9 @@ __global__ void __launch_bounds__(RDF ? 32 * kRdfWarps : kMxThreads,
         __syncwarp();
         bool cand = false;  // queued for the learned MAC
         if (node >= 0) {
-          // the particle range and (learned criterion) the cell geometry
-          // depend on the node index alone: issued with node_c, so a batch
-          // waits for one round of loads instead of two or three
+          // the particle range and (learned criterion) the cell's pre-filter
+          // record depend on the node index alone: issued with node_c, so a
+          // batch waits for one round of loads instead of two or three
           const double4 c = ldg_d4(&a.node_c[node]);
           const int cnt = __ldg(&a.count[node]);
           const int fst = __ldg(&a.first[node]);
