@@ -53,10 +53,12 @@ class Trial:
 
 
 def default_space(learned=True):
+    # grids of 2 and 3 blocks per SM: the learned criterion's build holds at
+    # most 2 (more are clamped), the fixed test's 80-register build 3
     thetas = (0.26, 0.28, 0.30, 0.32, 0.35)
     etas = (0.0, 1e-5, 3e-5, 1e-4) if learned else (0.0,)
     return [Candidate(t, e, b, 3, g) for t, e, b, g in
-            itertools.product(thetas, etas, (6, 8), (3, 4))]
+            itertools.product(thetas, etas, (6, 8), (2, 3))]
 
 
 def select(trials, target, margin=0.9):
