@@ -857,7 +857,8 @@ def run_ensemble(args, rank, world, dist):
         "method": {"setting": rec["setting"], "tuned": rec["tuned_in_this_run"]},
         "clocks": rec["clocks"], "gpu_launches": rec["gpu_launches"],
         "phases_ms_per_step": rec["phases_ms_per_step"], "accuracy": rec["accuracy"],
-        "e2e": rec["e2e"], "separate_handles_ms_per_step": rec["separate_handles_ms_per_step"],
+        "e2e": rec["e2e"], "fixed_theta_same_setting": rec["fixed_theta_same_setting"],
+        "separate_handles_ms_per_step": rec["separate_handles_ms_per_step"],
         "one_launch_speedup": rec["one_launch_speedup"],
     }
     print(json.dumps(line), flush=True)

@@ -49,3 +49,29 @@ def test_both_arms_describe_the_same_workload():
 def test_whole_job_rate():
     assert bench.whole_job_rate(1000, 2, 10, 20.0) == pytest.approx(1e6)
     assert np.isfinite(bench.whole_job_rate(1, 1, 1, 1e-3))
+
+
+class _FakeEnsemble:
+    """Two clouds whose forces differ from their direct sums by known
+    relative errors: cloud 0 by 1e-4 on every particle, cloud 1 by 3e-4."""
+
+    def __init__(self):
+        self.offsets = np.array([0, 5000, 11000])
+        rng = np.random.default_rng(3)
+        self.fd = rng.standard_normal((11000, 3)) + 2.0
+        scale = np.where(np.arange(11000) < 5000, 1e-4, 3e-4)[:, None]
+        unit = rng.standard_normal((11000, 3))
+        unit /= np.linalg.norm(unit, axis=1)[:, None]
+        self.f = self.fd + scale * np.linalg.norm(self.fd, axis=1)[:, None] * unit
+
+    def get_state(self):
+        return {"f": self.f}
+
+    def direct(self, cloud, targets):
+        a = int(self.offsets[cloud])
+        return self.fd[a + np.asarray(targets)], None
+
+
+def test_ensemble_rms_is_per_cloud():
+    rms = bench.ensemble_rms(_FakeEnsemble(), 2)
+    assert rms == pytest.approx([1e-4, 3e-4], rel=1e-9)
